@@ -1,0 +1,285 @@
+"""Benchmark of the GeoSWE fused finite-volume step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gsw|reference] [--n 8192]
+
+Workload (the rain-on-terrain pluvial case, dense grid): 8192 x 8192 cells, dx = 3 m,
+seeded fractal bed (power ~ k^-3, 0-40 m, 0.2 % slope), 4 Manning classes
+(0.025/0.04/0.06/0.1) on 256 seeded Voronoi cells, dry start, uniform rain 50 mm/h,
+x+ edge open ('fall'), other edges walls, CFL 0.5, fp32. A step is one time step of the
+solver (ghost fill + fused SRM-HLLC/rain/Euler/Manning/wet-dry step + device dt).
+The state (3 x 268 MB) is far larger than L2, so no flush is needed between steps.
+
+Prints one JSON line. Under torchrun each rank runs an independent replica (the
+single-GPU step does not shard here), timed on the device, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s on 1 B200: plain vs batched; adjoint/forward cost ratio"
+UNIT = "cell-updates/s"
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (SM MHz, throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_case(n, dtype="float32", seed=0):
+    """Host arrays of the rain-on-terrain case (the bed and classes are computed once and
+    cached under _bench_cache/ as .npy, keyed by size and seed)."""
+    from geoswe_b200.synthetic import fractal_bed, voronoi_classes_fast
+    cache = ROOT / "_bench_cache"
+    cache.mkdir(exist_ok=True)
+    fz, fc = cache / f"bed_{n}_{seed}.npy", cache / f"cls_{n}_{seed}.npy"
+    if fz.exists() and fc.exists():
+        z, cls = np.load(fz), np.load(fc)
+    else:
+        z = fractal_bed(n, n, 3.0, seed=seed).astype(np.float32)
+        cls = voronoi_classes_fast(n, n, seed=seed)
+        np.save(fz, z)
+        np.save(fc, cls)
+    return z, cls
+
+
+def make_solver(z, cls, n, dtype="float32"):
+    from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
+    from geoswe_b200.synthetic import MANNING_CLASSES
+    mesh = Mesh2D(nx=n, ny=n, dx=3.0, dy=3.0, ngh=2)
+    cfg = Config(bc_x="wall", bc_y="wall", bc={"x+": "fall"}, cfl=0.5, dtype=dtype,
+                 friction="manning",
+                 rainfall_forcing=RainfallForcing(time_s=[0.0, 1e9], rate_mm_h=[50.0, 50.0]))
+    q0 = np.zeros((3, n, n), np.float32)
+    s = Solver2D(mesh, cfg, q0, z)
+    ngh = mesh.ngh
+    clsp = np.pad(cls, ngh, mode="edge")
+    s.set_manning_table(clsp, MANNING_CLASSES)
+    return s
+
+
+def bytes_per_cell(track_max=True):
+    # read h, hu, hv, z (16 B) + class id (1 B); write h, hu, hv (12 B); running max 8 B
+    return 16 + 1 + 12 + (8 if track_max else 0)
+
+
+def run_gsw(args, rank, world):
+    import torch
+    from geoswe_b200 import _lib
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    n = args.n
+    z, cls = build_case(n)
+    cells = n * n
+    # ---------------- device-resident throughput (value) ----------------
+    s = make_solver(z, cls, n)
+    s.run(t_end=1e12, max_steps=args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = Clocks(int(os.environ.get("LOCAL_RANK", 0)))
+    clk.start()
+    l0 = _lib.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    steps = s.run(t_end=1e12, max_steps=args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    launches = _lib.launch_count() - l0
+    assert steps == args.steps, (steps, args.steps)
+    # ---------------- dominant kernel alone (roofline) ----------------
+    kern_ms = time_step_kernel(s, reps=args.kernel_reps)
+    # ---------------- end to end through the public API ----------------
+    e2e = run_e2e(args, z, cls, n)
+    del s
+    torch.cuda.empty_cache()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = cells * args.steps * world / (ms / 1e3)
+    peak, peak_kind = _peaks()
+    bpc = bytes_per_cell(True)
+    achieved = bpc * cells / (kern_ms / 1e3) / 1e9
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"rain-on-terrain dense {n}x{n}, dx=3 m, fractal bed, 4-class Voronoi "
+                               f"Manning, dry start, 50 mm/h uniform rain, x+ open, walls elsewhere, "
+                               f"CFL 0.5, fp32", "cells": cells, "l2": "inputs larger than L2 (no flush)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "dense_march_kernel<float,true>", "kernel_ms": kern_ms,
+                     "bytes_per_cell": bpc, "peak_source": peak_kind},
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(args)
+    return out
+
+
+def time_step_kernel(s, reps=20):
+    """Average duration of the fused dense step kernel alone (CUDA events on its stream)."""
+    import ctypes as C
+    import torch
+    from geoswe_b200 import _lib as L
+    from geoswe_b200.solver import _ptr, _stream
+    T = s._tables()
+    st = L.GswLoopState()
+    st.t = s.t
+    st.dt = s.last_dt
+    st.dt_f32 = float(np.float32(s.last_dt))
+    s._state_host.copy_(torch.frombuffer(bytearray(bytes(st) + bytes(128 - C.sizeof(st))), dtype=torch.uint8))
+    s._state.copy_(s._state_host)
+    args = [s._dense_args(s._buf[k], s._buf[1 - k], T) for k in (0, 1)]
+    for k in range(4):
+        L.call("gsw_dense_step", C.byref(args[k % 2]), _stream())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(reps):
+        L.call("gsw_dense_step", C.byref(args[k % 2]), _stream())
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_e2e(args, z, cls, n):
+    """Public API from pinned host buffers: construct (H2D of state, bed, classes),
+    run the timed steps, read the depth back (D2H), all inside the timed region."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    t0 = time.perf_counter()
+    s = make_solver(z, cls, n)
+    s.run(t_end=1e12, max_steps=args.steps)
+    h = s.depth()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    h2d = 3 * n * n * 4 + (n + 4) * (n + 4) * 4 + (n + 4) * (n + 4)
+    d2h = h.nbytes
+    del s
+    return {"value": n * n * args.steps / (ms / 1e3), "unit": UNIT,
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+            "what": "Solver2D(host arrays) + run(steps) + depth(); bytes per step = total / steps"}
+
+
+def cpu_baseline(args):
+    """The reference's CPU path (its NumPy solver, restated in oracle/numpy_ref.py) on a
+    bounded sample of the same workload, on this host's cores."""
+    try:
+        from oracle import numpy_ref
+    except Exception as e:                      # pragma: no cover
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "port", "sample": f"unavailable: {e}"}
+    return numpy_ref.time_rain_on_terrain(n=args.cpu_n, steps=args.cpu_steps)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="gsw", choices=["gsw", "reference"])
+    ap.add_argument("--n", type=int, default=8192)
+    ap.add_argument("--kernel-reps", type=int, default=20)
+    ap.add_argument("--cpu-n", type=int, default=512)
+    ap.add_argument("--cpu-steps", type=int, default=20)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        from oracle import numpy_ref
+        out = numpy_ref.reference_arm(args, METRIC, UNIT)
+        print(json.dumps(out), flush=True)
+        return 0
+    if world > 1:
+        import torch
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    out = run_gsw(args, rank, world)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,142 @@
+"""ctypes binding of libgsw.so (include/gsw.h).
+
+The library is the product's only compute path: if it is missing or fails to load,
+importing a solver raises. There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libgsw.so"
+
+ABI_VERSION = 1
+
+OK = 0
+ERR_INVALID, ERR_CUDA, ERR_ABI, ERR_NONFINITE, ERR_RANGE, ERR_TIMEOUT = -1, -2, -3, -4, -5, -6
+
+F32, F64 = 0, 1
+BC_EXTRAPOLATE, BC_WALL, BC_FALL, BC_PERIODIC, BC_NONE = 0, 1, 2, 3, 4
+BC_CODES = {"extrapolate": BC_EXTRAPOLATE, "wall": BC_WALL, "fall": BC_FALL,
+            "periodic": BC_PERIODIC, "none": BC_NONE}
+RAIN_NONE, RAIN_UNIFORM, RAIN_GRIDDED, RAIN_LOOKUP = 0, 1, 2, 3
+FRICTION_NONE, FRICTION_TABLE, FRICTION_FIELD = 0, 1, 2
+NORM_LINF, NORM_L2 = 0, 1
+BRICK_W, BRICK_PITCH = 30, 32
+
+vp = C.c_void_p
+i32, i64, u32, u64, f64 = C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_double
+
+
+class GswLoopState(C.Structure):
+    _fields_ = [("t", f64), ("dt", f64), ("t_new", f64), ("steps", i64), ("lam_bits", u64),
+                ("lam_used", f64), ("dt_f32", C.c_float), ("rain_idx", i32), ("done", i32),
+                ("error", i32), ("pending", i32), ("reserved", i32 * 3)]
+
+
+class GswDtParams(C.Structure):
+    _fields_ = [("abi_version", u32), ("mode", i32), ("cfl_dmin", f64), ("lam_floor", f64),
+                ("t_end", f64), ("eps_end", f64), ("dt_max", f64), ("fixed_dt", f64),
+                ("max_steps", i64), ("rain_t", vp), ("rain_lim", vp), ("n_rain", i32),
+                ("reserved", i32)]
+
+
+class GswDenseArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("dtype", i32), ("nxp", i32), ("nyp", i32), ("ngh", i32),
+                ("pitch", i64),
+                ("q0", vp), ("q1", vp), ("q2", vp), ("qn0", vp), ("qn1", vp), ("qn2", vp),
+                ("bed", vp), ("inside_mask", vp), ("mask_pitch", i64),
+                ("inv_dx", f64), ("inv_dy", f64), ("g", f64), ("h_min", f64),
+                ("state", vp), ("lam_target", vp), ("rain_kind", i32), ("rain", vp),
+                ("friction_kind", i32), ("n_cls", vp), ("n_cls_pitch", i64), ("n_tab", vp),
+                ("n_tab_len", i32), ("n_field", vp), ("vcap", f64), ("quadratic", i32),
+                ("keep_h", i32), ("max_h", vp), ("cfl_skip", vp), ("h_cfl", f64),
+                ("tile_rows", i32), ("warps", i32)]
+
+
+class GswBcArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("dtype", i32), ("nxp", i32), ("nyp", i32), ("ngh", i32),
+                ("pitch", i64), ("q0", vp), ("q1", vp), ("q2", vp), ("kinds", i32 * 4),
+                ("state", vp)]
+
+
+class GswStageArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("dtype", i32), ("pitch", i64), ("q0", vp), ("q1", vp),
+                ("q2", vp), ("cell_off", vp), ("bed64", vp), ("bed_is_f32", i32), ("n_cells", i32),
+                ("time_s", vp), ("stage_m", vp), ("n_knots", i32), ("state", vp),
+                ("lam_target", vp), ("cfl_ghost", vp), ("g", f64), ("h_cfl", f64)]
+
+
+class GswInflowArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("dtype", i32), ("pitch", i64), ("q0", vp), ("q1", vp),
+                ("q2", vp), ("bed", vp), ("inlet_off", vp), ("n", i32), ("ngh", i32),
+                ("step_off", i64), ("nx_n", f64), ("ny_n", f64), ("ds", f64), ("dry_frac", f64),
+                ("t_knots", vp), ("q_knots", vp), ("n_knots", i32), ("state", vp)]
+
+
+# entry point -> (argtypes, doc)
+_PROTOS = {
+    "gsw_dense_step": [C.POINTER(GswDenseArgs), vp],
+    "gsw_dense_rhs": [C.POINTER(GswDenseArgs), vp],
+    "gsw_dense_lammax": [C.POINTER(GswDenseArgs), vp, vp],
+    "gsw_bc_fill": [C.POINTER(GswBcArgs), vp],
+    "gsw_stage_apply": [C.POINTER(GswStageArgs), vp],
+    "gsw_lam_cells": [C.POINTER(GswStageArgs), vp],
+    "gsw_inflow_apply": [C.POINTER(GswInflowArgs), vp],
+    "gsw_dt_finalize": [C.POINTER(GswDtParams), vp, vp],
+    "gsw_loop_commit": [vp, vp],
+}
+
+
+class GswError(RuntimeError):
+    """A libgsw entry point returned a non-zero status."""
+
+    def __init__(self, fn, code, msg):
+        super().__init__(f"{fn} failed ({code}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libgsw.so (once). Raises ImportError if it is missing or unloadable."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m geoswe_b200.build` "
+            f"(nvcc, sm_100a). geoswe_b200 has no CPU fallback.")
+    L = C.CDLL(str(LIB_PATH))
+    for name, argt in _PROTOS.items():
+        fn = getattr(L, name)
+        fn.argtypes = argt
+        fn.restype = C.c_int
+    L.gsw_last_error.restype = C.c_char_p
+    L.gsw_last_error.argtypes = []
+    L.gsw_abi_version.restype = C.c_uint32
+    L.gsw_launch_count.restype = C.c_uint64
+    if L.gsw_abi_version() != ABI_VERSION:
+        raise ImportError(f"libgsw ABI {L.gsw_abi_version()} != {ABI_VERSION}; rebuild it")
+    _lib = L
+    return L
+
+
+def call(name, *args):
+    L = lib()
+    rc = getattr(L, name)(*args)
+    if rc != OK:
+        raise GswError(name, rc, L.gsw_last_error().decode(errors="replace"))
+    return rc
+
+
+def launch_count() -> int:
+    return int(lib().gsw_launch_count())
+
+
+def exported_symbols():
+    """Names the header declares (used by the load test)."""
+    return list(_PROTOS) + ["gsw_last_error", "gsw_abi_version", "gsw_launch_count"]

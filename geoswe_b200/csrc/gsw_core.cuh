@@ -1,0 +1,311 @@
+// gsw_core.cuh -- per-face and per-cell arithmetic of GeoSWE's SRM-HLLC step.
+//
+// Every expression follows the operand order of the reference kernel text
+// (geoswe/rhs_cuda.py:900-1207 for the residual, :1757-1796 for the update tail) and
+// is evaluated with separately rounded IEEE operations: the library is compiled with
+// --fmad=false and uses no fast-math intrinsics, so the C oracle (oracle/gsw_oracle.c)
+// reproduces every value.
+//
+// Face sharing. The reference evaluates the four faces of every cell, so each
+// interior face is computed twice, once from each side. From the right-hand cell
+// every input of the face is the exact negation or the same value as from the
+// left-hand cell (dz_clip and dz flip sign exactly, deta_L/deta_R swap), so the
+// flux is bit-identical from both sides; only the bed source differs per side.
+// The kernels here compute each face once and hand it to both cells.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gsw {
+
+template <typename T> struct Real;
+template <> struct Real<float>  { static __device__ __forceinline__ float  zero() { return 0.0f; } };
+template <> struct Real<double> { static __device__ __forceinline__ double zero() { return 0.0; } };
+
+// The reference's max()/min() device calls on floating point (fmaxf/fminf).
+__device__ __forceinline__ float  gmax(float a, float b)   { return fmaxf(a, b); }
+__device__ __forceinline__ float  gmin(float a, float b)   { return fminf(a, b); }
+__device__ __forceinline__ double gmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ double gmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float  gsqrt(float a)  { return sqrtf(a); }
+__device__ __forceinline__ double gsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ float  gabs(float a)   { return fabsf(a); }
+__device__ __forceinline__ double gabs(double a)  { return fabs(a); }
+
+// Primitive state of one cell (PRIMS macro, rhs_cuda.py:931-938) plus what the
+// faces need: free surface and the central bed gradients.
+template <typename T>
+struct Cell {
+    T h, hu, hv;   // conserved state (the update needs hu, hv)
+    T u, v;        // velocities, 0 when h <= h_min
+    T eta, b;      // free surface h + b and bed
+    T gx, gy;      // central bed gradients 0.5*(b+ - b-)*inv_d (rhs_cuda.py:1644-1651)
+};
+
+template <typename T>
+__device__ __forceinline__ void make_prims(Cell<T>& c, T h_min) {
+    const T hs = (c.h > h_min) ? c.h : h_min;
+    c.u = (c.h > h_min) ? c.hu / hs : Real<T>::zero();
+    c.v = (c.h > h_min) ? c.hv / hs : Real<T>::zero();
+    c.eta = c.h + c.b;
+}
+
+// x^(-4/3) for the Manning coefficient, x >= h_min > 0.
+// r = x^(-1/3) from an exponent-splitting first guess (bits(r) ~ (4/3)(127-s)2^23 -
+// bits(x)/3 with s = 0.0450466, the log-linear offset of IEEE binary32) refined by
+// three Newton steps r <- r + r*(1 - x r^3)/3 on f(r) = r^-3 - x, then x^(-4/3) = r/x.
+// Only IEEE +,-,*,/ and integer ops, so C and CUDA give the same bits. Accuracy
+// <= 1.85 ulp of the exact x^(-4/3) over [1e-7, 1e3] (the reference's powf evaluates
+// x^fl32(-4/3), within ~9 ulp of the exact power).
+__device__ __forceinline__ float pow_m43(float x) {
+    const uint32_t ix = __float_as_uint(x);
+    float r = __uint_as_float(0x54a2fa8du - ix / 3u);
+    const float third = 0.333333343267440796f;
+#pragma unroll
+    for (int it = 0; it < 3; ++it) {
+        float t = r * r;
+        t = t * r;
+        t = x * t;
+        t = 1.0f - t;
+        t = r * t;
+        t = t * third;
+        r = r + t;
+    }
+    return r / x;
+}
+// fp64: same iteration in double with two more steps (quadratic convergence from
+// the binary32 guess), r/x correctly rounded to well below one double ulp's worth
+// of the model.
+__device__ __forceinline__ double pow_m43(double x) {
+    const float xf = (float)x;
+    const uint32_t ix = __float_as_uint(xf);
+    double r = (double)__uint_as_float(0x54a2fa8du - ix / 3u);
+    const double third = 0.333333333333333315;
+#pragma unroll
+    for (int it = 0; it < 6; ++it) {
+        double t = r * r;
+        t = t * r;
+        t = x * t;
+        t = 1.0 - t;
+        t = r * t;
+        t = t * third;
+        r = r + t;
+    }
+    return r / x;
+}
+
+// HLLC flux in the face frame (rhs_cuda.py:986-1036) with Sigma = 0 (the no-sigma
+// build, rhs_cuda.py:1717-1722): uN normal, uT transverse velocity.
+template <typename T>
+__device__ __forceinline__ void hllc(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
+                                     T g, T h_min, T& Fh, T& FN, T& FT) {
+    const T z = Real<T>::zero();
+    const T half = (T)0.5, quarter = (T)0.25, two = (T)2.0;
+    const T aL = gsqrt(g * (hL > z ? hL : z));
+    const T aR = gsqrt(g * (hR > z ? hR : z));
+    const T u_st = half * (uNL + uNR) + aL - aR;
+    const T h_rt = half * (aL + aR) + quarter * (uNL - uNR);
+    const T h_st = (h_rt > z) ? (h_rt * h_rt) / g : z;
+    const T a_st = gsqrt(g * (h_st > z ? h_st : z));
+    const T SL_w = gmin(uNL - aL, u_st - a_st);
+    const T SR_w = gmax(uNR + aR, u_st + a_st);
+    const bool dryL = (hL <= h_min);
+    const bool dryR = (hR <= h_min);
+    T SL = dryL ? (uNR - two * aR) : SL_w;
+    T SR = dryR ? (uNL + two * aL) : SR_w;
+    if (dryL && dryR) { SL = z; SR = z; }
+    const T denom = hR * (uNR - SR) - hL * (uNL - SL);
+    T SM;
+    if (gabs(denom) > (T)1.0e-14) {
+        SM = (SL * hR * (uNR - SR) - SR * hL * (uNL - SL)) / denom;
+    } else {
+        SM = half * (uNL + uNR);
+    }
+    const T huNL = hL * uNL, huNR = hR * uNR;
+    const T huTL = hL * uTL, huTR = hR * uTR;
+    const T pL = half * g * hL * hL;
+    const T pR = half * g * hR * hR;
+    const T FL_h = huNL;
+    const T FL_N = huNL * uNL + pL;
+    const T FL_T = huNL * uTL;
+    const T FR_h = huNR;
+    const T FR_N = huNR * uNR + pR;
+    const T FR_T = huNR * uTR;
+    if (SL >= z) { Fh = FL_h; FN = FL_N; FT = FL_T; return; }
+    if (SM >= z) {
+        const T facL = (SL - uNL) / (SL - SM + (T)1.0e-30);
+        const T hLs = hL * facL;
+        const T huNLs = hLs * SM;
+        const T huTLs = hLs * uTL;
+        Fh = FL_h + SL * (hLs - hL);
+        FN = FL_N + SL * (huNLs - huNL);
+        FT = FL_T + SL * (huTLs - huTL);
+        return;
+    }
+    if (SR >= z) {
+        const T facR = (SR - uNR) / (SR - SM + (T)1.0e-30);
+        const T hRs = hR * facR;
+        const T huNRs = hRs * SM;
+        const T huTRs = hRs * uTR;
+        Fh = FR_h + SR * (hRs - hR);
+        FN = FR_N + SR * (huNRs - huNR);
+        FT = FR_T + SR * (huTRs - huTR);
+        return;
+    }
+    Fh = FR_h; FN = FR_N; FT = FR_T;
+}
+
+// One face between cell L (lower index) and cell R (upper index) along one axis.
+// Outputs are already scaled by 1/d, as the reference accumulates F*inv_d:
+//   Fh, Fn, Ft : mass, normal-momentum, transverse-momentum flux * inv_d
+//   srcL       : SRM bed source of the face for cell L (its +side), * inv_d
+//   srcR       : SRM bed source of the face for cell R (its -side), * inv_d
+//   wet        : false when both cells are below h_min (the face is skipped)
+template <typename T>
+struct Face { T Fh, Fn, Ft, srcL, srcR; bool wet; };
+
+template <typename T, bool XAXIS>
+__device__ __forceinline__ void srm_face(const Cell<T>& L, const Cell<T>& R,
+                                         T half_d, T inv_d, T g, T h_min, Face<T>& F) {
+    const T z = Real<T>::zero();
+    F.wet = !(L.h < h_min && R.h < h_min);
+    if (!F.wet) { F.Fh = z; F.Fn = z; F.Ft = z; F.srcL = z; F.srcR = z; return; }
+    const T gL = XAXIS ? L.gx : L.gy;
+    const T gR = XAXIS ? R.gx : R.gy;
+    // rhs_cuda.py:1044-1054 (cell L's frame; cell R's frame is the exact mirror)
+    const T zL = L.b + half_d * gL;
+    const T zR = R.b - half_d * gR;
+    const T zf0 = (L.b > R.b) ? L.b : R.b;
+    const T dz_clip = zR - zL;
+    const T dz = R.b - L.b - dz_clip;
+    const T deta_L = gmax(z, gmin(dz, R.eta - L.eta));
+    const T deta_R = gmax(z, gmin(-dz, L.eta - R.eta));
+    const T eta_Lf = L.eta + deta_L;
+    const T eta_Rf = R.eta + deta_R;
+    const T h_Lf = gmax(z, eta_Lf - zf0);
+    const T h_Rf = gmax(z, eta_Rf - zf0);
+    T Fh, FN, FT;
+    if (XAXIS) hllc<T>(h_Lf, L.u, L.v, h_Rf, R.u, R.v, g, h_min, Fh, FN, FT);
+    else       hllc<T>(h_Lf, L.v, L.u, h_Rf, R.v, R.u, g, h_min, Fh, FN, FT);
+    F.Fh = Fh * inv_d;
+    F.Fn = FN * inv_d;
+    F.Ft = FT * inv_d;
+    // bed source, cell L (rhs_cuda.py:1062-1072)
+    {
+        T dzb;
+        if (R.h < h_min) dzb = gmax(z, zf0 - L.eta);
+        else             dzb = gmax(z, gmin(dz_clip, zf0 - L.eta));
+        const T zf = zf0 - dzb;
+        const T src = (T)0.5 * g * (h_Lf + L.h) * (zf - L.b);
+        F.srcL = src * inv_d;
+    }
+    // bed source, cell R: its frame has dz_clip' = -dz_clip (rhs_cuda.py:1092-1104)
+    {
+        T dzb;
+        if (L.h < h_min) dzb = gmax(z, zf0 - R.eta);
+        else             dzb = gmax(z, gmin(-dz_clip, zf0 - R.eta));
+        const T zf = zf0 - dzb;
+        const T src = (T)0.5 * g * (h_Rf + R.h) * (zf - R.b);
+        F.srcR = src * inv_d;
+    }
+}
+
+// Residual of one cell from its four faces, accumulated in the reference order:
+// x-face i+1/2 (E), x-face i-1/2 (W), y-face j+1/2 (N), y-face j-1/2 (S).
+// E and N have this cell on their L side, W and S on their R side.
+template <typename T>
+__device__ __forceinline__ void accumulate(const Face<T>& E, const Face<T>& W,
+                                           const Face<T>& N, const Face<T>& S,
+                                           T& rh, T& rhu, T& rhv) {
+    rh = Real<T>::zero(); rhu = Real<T>::zero(); rhv = Real<T>::zero();
+    if (E.wet) { rh = rh - E.Fh; rhu = rhu - E.Fn; rhv = rhv - E.Ft; rhu = rhu - E.srcL; }
+    if (W.wet) { rh = rh + W.Fh; rhu = rhu + W.Fn; rhv = rhv + W.Ft; rhu = rhu + W.srcR; }
+    if (N.wet) { rh = rh - N.Fh; rhu = rhu - N.Ft; rhv = rhv - N.Fn; rhv = rhv - N.srcL; }
+    if (S.wet) { rh = rh + S.Fh; rhu = rhu + S.Ft; rhv = rhv + S.Fn; rhv = rhv + S.srcR; }
+}
+
+// Wet/dry floor and point-implicit Manning friction on an updated cell
+// (rhs_cuda.py:1765-1790; solver.py:233-307). friction == false applies the wet/dry
+// floor alone, as the reference does when Config.friction is None (solver.py:2952-2962).
+template <typename T>
+__device__ __forceinline__ void wetdry_friction(T& h, T& hu, T& hv, bool friction, T n,
+                                                T dt, T g, T h_min, T vcap,
+                                                bool quadratic, bool keep_h) {
+    const T z = Real<T>::zero();
+    if (h < h_min) {
+        h = keep_h ? (h > z ? h : z) : z;
+        hu = z; hv = z;
+        return;
+    }
+    if (!friction) return;
+    const T hs = (h > h_min) ? h : h_min;
+    const T u = hu / hs;
+    const T v = hv / hs;
+    const T modU = gsqrt(u * u + v * v);
+    const T h43 = pow_m43(hs);
+    if (modU > vcap) {
+        const T n_cri = gsqrt((T)1.0 / (((T)1.0e-10 + dt) * g * h43 * (modU + (T)1.0e-30)));
+        if (n_cri > n) n = n_cri;
+    }
+    const T Cf = g * n * n * h43;
+    T alpha;
+    if (quadratic) {
+        const T twodtCfU = (T)2.0 * dt * Cf * modU;
+        alpha = (T)2.0 / (gsqrt((T)1.0 + (T)2.0 * twodtCfU) + (T)1.0);
+    } else {
+        alpha = (T)1.0 / ((T)1.0 + dt * Cf * modU);
+    }
+    hu = hu * alpha;
+    hv = hv * alpha;
+}
+
+// Wave speeds are reduced as the IEEE bits of a non-negative double (unsigned order
+// is the float order for non-negative values, and NaN/Inf sit above every finite
+// value), so fp32 and fp64 runs share one 64-bit atomicMax target.
+//
+// Dense loop, fp32 (lammax_fp32_lean, solver.py:152-205): cells with h < h_cfl give
+// 0, u = hu/h, non-finite -> +Inf.
+__device__ __forceinline__ unsigned long long lam_dense_bits(float h, float hu, float hv,
+                                                             float g, float h_cfl) {
+    if (h < h_cfl) return 0ull;
+    const float u = hu / h;
+    const float v = hv / h;
+    const float au = fabsf(u), av = fabsf(v);
+    const float lam = ((au > av) ? au : av) + sqrtf(g * h);
+    const bool fin = (lam <= 3.0e38f) && (au <= 3.0e38f) && (av <= 3.0e38f);
+    return fin ? (unsigned long long)__double_as_longlong((double)lam) : 0x7ff0000000000000ull;
+}
+// Dense loop, fp64 (the generic path, solver.py:2668-2693 with swe.max_wave_speed_2d):
+// every cell counts, u = 0 where h <= h_cfl else hu/max(h, h_cfl), c = sqrt(g max(h,0)).
+// The all-dry floor sqrt(g h_cfl) is applied by gsw_dt_finalize, so whether cells below
+// h_cfl contribute sqrt(g h) < floor or nothing gives the same dt.
+__device__ __forceinline__ unsigned long long lam_dense_bits(double h, double hu, double hv,
+                                                             double g, double h_cfl) {
+    const bool dry = h <= h_cfl;
+    const double hs = h > h_cfl ? h : h_cfl;
+    const double u = dry ? 0.0 : hu / hs;
+    const double v = dry ? 0.0 : hv / hs;
+    const double c = sqrt(g * (h > 0.0 ? h : 0.0));
+    const double au = fabs(u), av = fabs(v);
+    const double lam = ((au > av) ? au : av) + c;
+    if (!(lam <= 1.0e308)) return 0x7ff0000000000000ull;   // NaN or Inf
+    return (unsigned long long)__double_as_longlong(lam);
+}
+
+// Flat loop (cfl_lammax_flat_blk_ns, compressed_solver.py:209-244, and the fused
+// _LAM_BLOCK, compressed_rhs.py:1027-1039), fp32: NaN depth -> quiet NaN; h < h_min
+// -> 0; divisor floored at h_min_cfl; L2 norm, or Linf with cfl_linf.
+__device__ __forceinline__ unsigned long long lam_flat_bits(float h, float hu, float hv, float g,
+                                                            float h_min, float h_min_cfl,
+                                                            bool linf) {
+    if (h != h) return 0x7ff8000000000000ull;
+    if (h < h_min) return 0ull;
+    const float hs = h > h_min_cfl ? h : h_min_cfl;
+    const float u = hu / hs, v = hv / hs;
+    const float c = sqrtf(g * (h > 0.0f ? h : 0.0f));
+    const float speed = linf ? fmaxf(fabsf(u), fabsf(v)) : sqrtf(u * u + v * v);
+    const float l = speed + c;
+    return (unsigned long long)__double_as_longlong((double)l);
+}
+
+}  // namespace gsw

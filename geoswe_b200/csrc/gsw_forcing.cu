@@ -1,0 +1,145 @@
+// gsw_forcing.cu -- discharge inflow through ghost cells, on the device.
+//
+// The reference evaluates each inlet on the host every step: np.interp for Q(t), a
+// NumPy sum of the inlet depths (a device sync on the GPU path) and fancy-index writes
+// (geoswe/solver.py:1944-1971, geoswe/bc.py:175-235). This kernel performs the same
+// arithmetic in one block per inlet, inside the captured step, including NumPy's
+// pairwise float summation order so the depth weights are bit-identical.
+#include "gsw_common.cuh"
+
+namespace gsw {
+
+// numpy's pairwise sum (add.reduce over a contiguous run): < 8 terms sequential;
+// <= 128 terms in eight interleaved partial sums combined as ((0+1)+(2+3))+((4+5)+(6+7))
+// plus a sequential tail; longer runs split at n/2 rounded down to a multiple of 8.
+template <typename T>
+__device__ T pairwise_sum(const T* q0, const int64_t* off, int64_t a, int64_t n) {
+    if (n < 8) {
+        T res = (T)0;
+        for (int64_t i = 0; i < n; ++i) res = res + q0[off[a + i]];
+        return res;
+    }
+    if (n <= 128) {
+        T r[8];
+        for (int k = 0; k < 8; ++k) r[k] = q0[off[a + k]];
+        int64_t i = 8;
+        for (; i < n - (n % 8); i += 8)
+            for (int k = 0; k < 8; ++k) r[k] = r[k] + q0[off[a + i + k]];
+        T res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+        for (; i < n; ++i) res = res + q0[off[a + i]];
+        return res;
+    }
+    int64_t n2 = n / 2;
+    n2 -= n2 % 8;
+    return pairwise_sum(q0, off, a, n2) + pairwise_sum(q0, off, a + n2, n - n2);
+}
+
+// np.interp(x, xp, fp) for one scalar x (numpy/_core/src/multiarray/compiled_base.c).
+__device__ double np_interp(double x, const double* xp, const double* fp, int n) {
+    if (n == 1) return fp[0];
+    if (x != x) return x;
+    if (x < xp[0]) return fp[0];
+    if (x > xp[n - 1]) return fp[n - 1];
+    int lo = 0, hi = n;                               // last j with xp[j] <= x
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (xp[mid] <= x) lo = mid + 1; else hi = mid; }
+    const int j = lo - 1;
+    if (j >= n - 1) return fp[n - 1];
+    if (xp[j] == x) return fp[j];
+    const double slope = __ddiv_rn(__dsub_rn(fp[j + 1], fp[j]), __dsub_rn(xp[j + 1], xp[j]));
+    double r = __dadd_rn(__dmul_rn(slope, __dsub_rn(x, xp[j])), fp[j]);
+    if (r != r) {
+        r = __dadd_rn(__dmul_rn(slope, __dsub_rn(x, xp[j + 1])), fp[j + 1]);
+        if (r != r && fp[j] == fp[j + 1]) r = fp[j];
+    }
+    return r;
+}
+
+template <typename T>
+__global__ void inflow_kernel(GswInflowArgs a) {
+    if (a.state->done) return;
+    T* q0 = (T*)a.q0; T* q1 = (T*)a.q1; T* q2 = (T*)a.q2;
+    const T* bed = (const T*)a.bed;
+    __shared__ double s_Q, s_sum, s_add;
+    __shared__ T s_zmin, s_zmax;
+    __shared__ int s_wet, s_nlow, s_flat;
+    if (threadIdx.x == 0) {
+        s_Q = np_interp(a.state->t, a.t_knots, a.q_knots, a.n_knots);
+        const T sum = pairwise_sum<T>(q0, a.inlet_off, 0, a.n);
+        s_sum = (double)sum;
+        s_wet = s_sum > 0.0;
+        if (!s_wet) {
+            T zmin = bed[a.inlet_off[0]], zmax = zmin;
+            for (int k = 1; k < a.n; ++k) {
+                const T z = bed[a.inlet_off[k]];
+                zmin = z < zmin ? z : zmin;        // np.min / np.max of finite values
+                zmax = z > zmax ? z : zmax;
+            }
+            s_zmin = zmin; s_zmax = zmax;
+            int nlow = 0;
+            T hmax = (T)0;
+            const T frac = (T)a.dry_frac;
+            for (int k = 0; k < a.n; ++k) {
+                const T z = bed[a.inlet_off[k]];
+                nlow += (z <= zmin);
+                T hf = zmin + frac * (zmax - zmin) - z;
+                hf = hf > (T)0 ? hf : (T)0;
+                hmax = (k == 0 || hf > hmax) ? hf : hmax;
+            }
+            s_nlow = nlow;
+            s_flat = !((double)hmax > 0.0);
+            s_add = 0.0;
+            if (s_flat) {
+                const double nl = nlow > 1 ? (double)nlow : 1.0;
+                const double qc = __ddiv_rn(fabs(s_Q), __dmul_rn(nl, a.ds));
+                s_add = pow(__ddiv_rn(__dmul_rn(qc, qc), 9.80665), 1.0 / 3.0);
+            }
+        }
+    }
+    __syncthreads();
+    const double Q = s_Q;
+    const int64_t total = (int64_t)a.n * a.ngh;
+    for (int64_t t = threadIdx.x; t < total; t += blockDim.x) {
+        const int k = (int)(t % a.n);
+        const int gk = (int)(t / a.n) + 1;                       // ghost layer 1..ngh
+        const int64_t src = a.inlet_off[k];
+        const int64_t go = src + (int64_t)gk * a.step_off;
+        const T h = q0[src];
+        T hf, hu, hv;
+        if (s_wet) {
+            const T w = h / (T)s_sum;                            // h / s in the array dtype
+            const T qn = (T)__ddiv_rn(Q, a.ds) * w;              // (Q/ds) * w
+            hf = h;
+            hu = qn * (T)a.nx_n;
+            hv = qn * (T)a.ny_n;
+        } else {
+            const T z = bed[src];
+            T f = s_zmin + (T)a.dry_frac * (s_zmax - s_zmin) - z;
+            f = f > (T)0 ? f : (T)0;
+            if (s_flat) f = f + (T)s_add;
+            const double nl = s_nlow > 1 ? (double)s_nlow : 1.0;
+            const double w = (z <= s_zmin) ? __ddiv_rn(1.0, nl) : 0.0;   // float64 weights
+            const double qn = __dmul_rn(__ddiv_rn(Q, a.ds), w);
+            hf = f;
+            hu = (T)__dmul_rn(qn, a.nx_n);
+            hv = (T)__dmul_rn(qn, a.ny_n);
+        }
+        q0[go] = hf; q1[go] = hu; q2[go] = hv;
+    }
+}
+
+}  // namespace gsw
+
+using namespace gsw;
+
+extern "C" int gsw_inflow_apply(const GswInflowArgs* a, void* stream) {
+    GSW_CHECK_ABI(a);
+    if (a->n <= 0) return GSW_OK;
+    if (!a->inlet_off || !a->q0 || !a->q1 || !a->q2 || !a->bed || !a->t_knots || !a->q_knots ||
+        a->n_knots < 1 || !a->state || a->ngh < 1)
+        return set_error(GSW_ERR_INVALID, "inflow: null pointer or empty hydrograph");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (a->dtype == GSW_F32) inflow_kernel<float><<<1, 256, 0, s>>>(*a);
+    else if (a->dtype == GSW_F64) inflow_kernel<double><<<1, 256, 0, s>>>(*a);
+    else return set_error(GSW_ERR_INVALID, "inflow: bad dtype");
+    return check_launch("inflow");
+}

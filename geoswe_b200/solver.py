@@ -1,0 +1,701 @@
+"""Dense-grid solver: the reference's Solver2D (geoswe/solver.py:1273-3032) on libgsw.
+
+The state lives on the GPU in two pitched buffers (ping-pong). One step is
+
+    ghost fill -> inflow ghosts -> fused SRM-HLLC step -> t += dt -> stage boundary
+
+exactly the order of Solver2D.step (solver.py:2695-2973), and `run` keeps dt, t, the
+rain frame and the loop condition on the device (gsw_dt_finalize), capturing windows
+of steps in CUDA graphs so the host only polls a done flag once per window.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+import warnings
+from typing import Callable, Optional
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .config import Config
+from .forcing import RainfallForcing, StageBoundary
+from .mesh import Mesh2D
+
+
+def _pitch(n, itemsize):
+    per = 128 // itemsize
+    return ((n + per - 1) // per) * per
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def _require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError("geoswe_b200 solvers run on a CUDA device (sm_100a); none is visible. "
+                           "There is no CPU fallback; the CPU oracle under oracle/ is a test checker.")
+    L.lib()
+
+
+class _Tables:
+    """Device copies of the forcing tables, in the solver's dtype."""
+
+
+class Solver2D:
+    """Two-dimensional shallow-water solver on the dense padded grid.
+
+    ``q0`` has shape (3, nx, ny) and ``b`` (nx, ny), host or device arrays. The padded
+    state is exposed as ``q`` (a (3, nx+2ngh, ny+2ngh) CUDA tensor view) and the depth
+    as ``depth()`` (NumPy). ``run``/``step``/``cfl_dt`` follow the reference.
+    """
+
+    def __init__(self, mesh: Mesh2D, cfg: Config, q0, b, comm=None, dims=None, *,
+                 device=None, track_max_depth: bool = True, use_graphs: bool = True,
+                 tile_rows: int = 0, warps: int = 0):
+        _require_cuda()
+        if comm is not None and getattr(comm, "size", 1) > 1:
+            raise NotImplementedError("Solver2D: multi-rank runs are not part of this package "
+                                      "(one GPU per solver)")
+        cfg.require_production_scheme("Solver2D")
+        if "dirichlet" in (cfg.bc_x, cfg.bc_y):
+            raise ValueError("bc 'dirichlet' exists for Solver1D only; in 2D impose a water "
+                             "level with a StageBoundary (Config.stage_boundary)")
+        self.mesh, self.cfg = mesh, cfg
+        self.t = 0.0
+        self.nsteps = 0
+        self.diagnostics = {"rhs_calls": 0, "wallclock": 0.0}
+        ngh = mesh.ngh
+        if ngh < 2:
+            raise ValueError(f"ngh={ngh} is too small: the fused SRM-HLLC step reads two cells "
+                             f"beyond every interior cell. Construct Mesh2D with ngh >= 2.")
+        q0 = np.asarray(q0.detach().cpu() if torch.is_tensor(q0) else q0)
+        b = np.asarray(b.detach().cpu() if torch.is_tensor(b) else b)
+        if tuple(q0.shape) != (3, mesh.nx, mesh.ny):
+            raise ValueError(f"q0 must have shape (3, nx, ny) = (3, {mesh.nx}, {mesh.ny}); "
+                             f"got {tuple(q0.shape)}")
+        if tuple(b.shape) != (mesh.nx, mesh.ny):
+            raise ValueError(f"the bed must have shape (nx, ny) = ({mesh.nx}, {mesh.ny}); "
+                             f"got {tuple(b.shape)}")
+        for what, arr in (("the bed", b), ("the initial state q0", q0)):
+            if not np.isfinite(arr).all():
+                raise ValueError(f"Solver2D: {what} holds non-finite values (NaN or inf)")
+        rate = getattr(getattr(cfg, "rainfall_forcing", None), "rate_mm_h", None)
+        if rate is not None and int(getattr(rate, "ndim", 1)) == 3 and tuple(rate.shape[1:]) != (mesh.nx, mesh.ny):
+            raise ValueError(f"Config.rainfall_forcing.rate_mm_h has shape {tuple(rate.shape)}; gridded "
+                             f"rain must be (nt, nx, ny) = (nt, {mesh.nx}, {mesh.ny})")
+        if cfg.manning_field is not None:
+            mf = np.asarray(cfg.manning_field.detach().cpu() if torch.is_tensor(cfg.manning_field)
+                            else cfg.manning_field)
+            if tuple(mf.shape) != mesh.padded_shape:
+                raise ValueError(f"Config.manning_field must be the padded (nx+2*ngh, ny+2*ngh) = "
+                                 f"{mesh.padded_shape} array, got {tuple(mf.shape)}")
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.np_dtype = np.dtype(cfg.dtype)
+        self.t_dtype = torch.float32 if self.np_dtype == np.float32 else torch.float64
+        self.code = L.F32 if self.np_dtype == np.float32 else L.F64
+        self.nxp, self.nyp = mesh.padded_shape
+        self.pitch = _pitch(self.nyp, self.np_dtype.itemsize)
+        self._tile_rows, self._warps = int(tile_rows), int(warps)
+        self._use_graphs = bool(use_graphs)
+        dev, td = self.device, self.t_dtype
+        self._buf = [torch.zeros((3, self.nxp, self.pitch), dtype=td, device=dev) for _ in range(2)]
+        self._cur = 0
+        qpad = np.zeros((3, self.nxp, self.nyp), dtype=self.np_dtype)
+        qpad[:, ngh:ngh + mesh.nx, ngh:ngh + mesh.ny] = q0.astype(self.np_dtype, copy=False)
+        self._buf[0][:, :, :self.nyp].copy_(torch.from_numpy(qpad))
+        bpad = np.zeros((self.nxp, self.nyp), dtype=self.np_dtype)
+        bpad[ngh:ngh + mesh.nx, ngh:ngh + mesh.ny] = b.astype(self.np_dtype, copy=False)
+        self._pad_bed(bpad)
+        self._b = torch.zeros((self.nxp, self.pitch), dtype=td, device=dev)
+        self._b[:, :self.nyp].copy_(torch.from_numpy(bpad))
+        self._b_host = bpad
+        self._mask = None
+        self.inside_mask_interior = None
+        self._ncls = None
+        self._ntab = None
+        self._nfield = None
+        self._ghost = None             # interior cfl ghost mask (host bool)
+        self._skip = None              # device uint8 (nx*ny): ghost | stage cells
+        self._max_h = torch.zeros((self.nxp, self.pitch), dtype=td, device=dev) if track_max_depth else None
+        self._stepped = False
+        self._inflows = []
+        self._state = torch.zeros(128, dtype=torch.uint8, device=dev)
+        self._state_host = torch.zeros(128, dtype=torch.uint8).pin_memory()
+        self._lam_scratch = torch.zeros(1, dtype=torch.int64, device=dev)
+        self._graph_cache = {}
+        self._dev_tables = None
+        self._tables_key = None
+        if cfg.manning_field is not None and cfg.friction is not None:
+            self._nfield = torch.zeros((self.nxp, self.pitch), dtype=td, device=dev)
+            self._nfield[:, :self.nyp].copy_(torch.from_numpy(np.ascontiguousarray(mf, dtype=self.np_dtype)))
+
+    # ------------------------------------------------------------------ layout
+    def _pad_bed(self, bpad):
+        """Ghost bed as the ghost state is filled (solver.py:1466-1484)."""
+        ngh = self.mesh.ngh
+        if self.cfg.bc_x == "periodic":
+            bpad[:ngh, :] = bpad[-2 * ngh:-ngh, :]
+            bpad[-ngh:, :] = bpad[ngh:2 * ngh, :]
+        else:
+            bpad[:ngh, :] = bpad[ngh:ngh + 1, :]
+            bpad[-ngh:, :] = bpad[-ngh - 1:-ngh, :]
+        if self.cfg.bc_y == "periodic":
+            bpad[:, :ngh] = bpad[:, -2 * ngh:-ngh]
+            bpad[:, -ngh:] = bpad[:, ngh:2 * ngh]
+        else:
+            bpad[:, :ngh] = bpad[:, ngh:ngh + 1]
+            bpad[:, -ngh:] = bpad[:, -ngh - 1:-ngh]
+
+    @property
+    def q(self):
+        """Padded conserved state (3, nxp, nyp): a CUDA tensor view of the current buffer."""
+        return self._buf[self._cur][:, :, :self.nyp]
+
+    @q.setter
+    def q(self, value):
+        v = value if torch.is_tensor(value) else torch.from_numpy(np.asarray(value))
+        self._buf[self._cur][:, :, :self.nyp].copy_(v.to(self.t_dtype))
+        self._invalidate()
+
+    @property
+    def b(self):
+        return self._b[:, :self.nyp]
+
+    @property
+    def q_interior(self):
+        g = self.mesh.ngh
+        return self.q[:, g:-g, g:-g]
+
+    def depth(self):
+        """Water depth (nx, ny) as a NumPy array, ghost cells removed."""
+        return self.q_interior[0].detach().cpu().numpy()
+
+    def max_depth(self):
+        """Running maximum depth after any step so far; depth() before the first step."""
+        if self._max_h is None or not self._stepped:
+            return self.depth()
+        g = self.mesh.ngh
+        return self._max_h[g:-g, g:self.nyp - g].detach().cpu().numpy()
+
+    # ------------------------------------------------------------- set-up API
+    def set_inside_mask(self, mask, cfl_robust_pct=None):
+        """Active set (nx, ny) bool: cells outside get a zero residual and no rain."""
+        if cfl_robust_pct is not None:
+            raise NotImplementedError("cfl_robust_pct (a percentile dt limit) is not implemented; "
+                                      "use set_cfl_ghost_mask to exclude cells from the dt limit")
+        if mask is None:
+            self._mask = None
+            self.inside_mask_interior = None
+            self._invalidate()
+            return
+        m = np.asarray(mask.detach().cpu() if torch.is_tensor(mask) else mask)
+        if m.shape != (self.mesh.nx, self.mesh.ny):
+            raise ValueError(f"inside_mask must have shape ({self.mesh.nx}, {self.mesh.ny}); got {m.shape}")
+        ngh = self.mesh.ngh
+        pad = np.zeros((self.nxp, self.pitch), dtype=np.uint8)
+        pad[ngh:ngh + self.mesh.nx, ngh:ngh + self.mesh.ny] = m.astype(np.uint8)
+        self._mask = torch.from_numpy(pad).to(self.device)
+        self.inside_mask_interior = m.astype(bool)
+        self._invalidate()
+
+    @property
+    def inside_mask(self):
+        return None if self._mask is None else self._mask[:, :self.nyp]
+
+    def set_manning_table(self, cls_padded, table):
+        cls_padded = np.asarray(cls_padded.detach().cpu() if torch.is_tensor(cls_padded) else cls_padded)
+        table = np.asarray(table.detach().cpu() if torch.is_tensor(table) else table, dtype=np.float64)
+        if tuple(cls_padded.shape) != (self.nxp, self.nyp):
+            raise ValueError(f"set_manning_table expects a PADDED (nxp, nyp)={(self.nxp, self.nyp)} class "
+                             f"array; got {tuple(cls_padded.shape)}")
+        if cls_padded.dtype != np.uint8:
+            raise ValueError(f"set_manning_table: cls_padded must be uint8; got {cls_padded.dtype}")
+        if table.ndim != 1 or table.size < 1 or table.size > 256:
+            raise ValueError("set_manning_table: table must be 1-D with 1..256 entries")
+        if int(cls_padded.max()) >= int(table.size):
+            raise ValueError(f"set_manning_table: class id {int(cls_padded.max())} out of range for a "
+                             f"{int(table.size)}-entry table")
+        if self.cfg.friction is None:
+            warnings.warn("set_manning_table: friction is off (Config.friction is None), so this "
+                          "roughness table will not be applied", stacklevel=2)
+        pad = np.zeros((self.nxp, self.pitch), dtype=np.uint8)
+        pad[:, :self.nyp] = cls_padded
+        self._ncls = torch.from_numpy(pad).to(self.device)
+        self._ntab = torch.from_numpy(table.astype(np.float32).astype(self.np_dtype)).to(self.device)
+        self._nfield = None
+        self._invalidate()
+
+    def set_manning(self, n):
+        """Manning's n from a scalar or an (nx, ny) array; friction is switched on."""
+        nx, ny, ngh = self.mesh.nx, self.mesh.ny, self.mesh.ngh
+        n_host = np.asarray(n.detach().cpu() if torch.is_tensor(n) else n, dtype=np.float64)
+        if n_host.ndim == 0:
+            n_host = np.full((nx, ny), float(n_host))
+        if n_host.shape != (nx, ny):
+            raise ValueError(f"set_manning expects a scalar or an unpadded ({nx}, {ny}) array; got "
+                             f"shape {n_host.shape}")
+        if not np.all(np.isfinite(n_host)) or float(n_host.min()) < 0.0:
+            raise ValueError("set_manning: Manning's n must be finite and non-negative")
+        padded = np.pad(n_host, ngh, mode="edge")
+        if self.cfg.friction is None:
+            self.cfg.friction = "manning_implicit"
+        self.cfg.manning_field = None
+        vals, inv = np.unique(padded, return_inverse=True)
+        if vals.size <= 256:
+            self.set_manning_table(inv.reshape(padded.shape).astype(np.uint8), vals.astype(np.float32))
+            return
+        self._ncls = None
+        self._ntab = None
+        self._nfield = torch.zeros((self.nxp, self.pitch), dtype=self.t_dtype, device=self.device)
+        self._nfield[:, :self.nyp].copy_(torch.from_numpy(padded.astype(self.np_dtype)))
+        self._invalidate()
+
+    def set_cfl_ghost_mask(self, mask):
+        """Interior cells (nx, ny) excluded from the CFL wave speed."""
+        if mask is None:
+            self._ghost = None
+        else:
+            m = np.asarray(mask.detach().cpu() if torch.is_tensor(mask) else mask)
+            if m.shape != (self.mesh.nx, self.mesh.ny):
+                raise ValueError(f"cfl_ghost_mask must have shape ({self.mesh.nx}, {self.mesh.ny}); "
+                                 f"got {m.shape}")
+            self._ghost = m.astype(bool)
+        self._invalidate()
+
+    def add_inflow(self, idx_i, idx_j, normal, ds, t_series, q_series, dry_frac=0.10):
+        """One discharge inlet on padded cells (idx_i, idx_j) along a physical edge;
+        ``normal`` is the inward unit normal (axis-aligned)."""
+        ii = np.asarray(idx_i, dtype=np.int64).ravel()
+        jj = np.asarray(idx_j, dtype=np.int64).ravel()
+        if ii.shape != jj.shape:
+            raise ValueError("add_inflow: idx_i and idx_j must have the same length")
+        si, sj = int(round(float(normal[0]))), int(round(float(normal[1])))
+        if abs(si) + abs(sj) != 1:
+            raise ValueError("add_inflow: the inward normal must be axis-aligned, one of (+-1, 0), (0, +-1)")
+        ngh = self.mesh.ngh
+        gi = ii[:, None] - np.arange(1, ngh + 1)[None, :] * si
+        gj = jj[:, None] - np.arange(1, ngh + 1)[None, :] * sj
+        if ii.size and (gi.min() < 0 or gi.max() >= self.nxp or gj.min() < 0 or gj.max() >= self.nyp):
+            raise ValueError("add_inflow: the ghost cells outward of the inlet leave the padded grid")
+        t = np.asarray(t_series, dtype=np.float64)
+        qv = np.asarray(q_series, dtype=np.float64)
+        if t.shape != qv.shape or t.ndim != 1 or t.size < 1:
+            raise ValueError("add_inflow: t_series and q_series must be 1-D and of equal length")
+        self._inflows.append(dict(i=ii, j=jj, nx=float(normal[0]), ny=float(normal[1]), ds=float(ds),
+                                  t=t, q=qv, dry_frac=float(dry_frac), si=si, sj=sj))
+        self._invalidate()
+
+    def set_inflow(self, *a, **k):
+        self._inflows = []
+        self.add_inflow(*a, **k)
+
+    def _invalidate(self):
+        self._graph_cache.clear()
+        self._dev_tables = None
+
+    # --------------------------------------------------------------- tables
+    def _h_cfl(self):
+        cfg = self.cfg
+        h = cfg.h_min_cfl if cfg.h_min_cfl > 0.0 else cfg.h_min
+        if self.np_dtype == np.float32 and h < 1.0e-6:
+            h = 1.0e-6
+        return h
+
+    def _stage_list(self):
+        sb = self.cfg.stage_boundary
+        if sb is None:
+            return []
+        return list(sb) if isinstance(sb, (list, tuple)) else [sb]
+
+    def _tables(self):
+        """Device tables for rain, stage, inflow and the CFL skip mask (built once)."""
+        if self._dev_tables is not None:
+            return self._dev_tables
+        T = _Tables()
+        dev, cfg = self.device, self.cfg
+        nx, ny, ngh = self.mesh.nx, self.mesh.ny, self.mesh.ngh
+        dmin = min(self.mesh.dx, self.mesh.dy)
+        # rain (solver.py:1903-1914, forcing.py:170-216; rain limit solver.py:3005-3027)
+        T.rain_kind = L.RAIN_NONE
+        T.rain = T.rain_t = T.rain_lim = None
+        rf = cfg.rainfall_forcing
+        if rf is not None:
+            frames = rf.frames(self.np_dtype)
+            T.rain_kind = L.RAIN_GRIDDED if rf.gridded else L.RAIN_UNIFORM
+            T.rain = torch.from_numpy(np.ascontiguousarray(frames)).to(dev)
+            times = np.asarray(rf.time_s, dtype=np.float64)
+            if rf.gridded:
+                rmax = [float(frames[k].max()) for k in range(frames.shape[0])]
+            else:
+                rmax = [float(rf.rate_mm_h[k]) / 3.6e6 for k in range(len(times))]
+        elif cfg.rainfall > 0.0:
+            T.rain_kind = L.RAIN_UNIFORM
+            T.rain = torch.tensor([cfg.rainfall], dtype=self.t_dtype, device=dev)
+            times = np.array([0.0])
+            rmax = [float(cfg.rainfall)]
+        if T.rain_kind != L.RAIN_NONE:
+            lim = [((cfg.cfl * dmin) ** (2.0 / 3.0) / (cfg.g * r) ** (1.0 / 3.0)) if r > 0.0 else 0.0
+                   for r in rmax]
+            T.rain_t = torch.from_numpy(times.copy()).to(dev)
+            T.rain_lim = torch.tensor(lim, dtype=torch.float64, device=dev)
+            T.n_rain = len(times)
+        else:
+            T.n_rain = 0
+        # stage boundaries (forcing.py:315-377)
+        T.stages = []
+        skip = np.zeros((nx, ny), dtype=bool)
+        if self._ghost is not None:
+            skip |= self._ghost
+        all_cells = []
+        for sb in self._stage_list():
+            cells = np.asarray(sb.cells, dtype=np.int64)
+            if cells.size and (cells[:, 0].min() < ngh or cells[:, 0].max() >= ngh + nx or
+                               cells[:, 1].min() < ngh or cells[:, 1].max() >= ngh + ny):
+                raise ValueError("StageBoundary.cells must index the padded grid (unpadded index + "
+                                 f"mesh.ngh = {ngh}); some cells lie in the ghost layers")
+            off = cells[:, 0] * self.pitch + cells[:, 1]
+            bed = np.asarray(sb.bed_b)
+            d = dict(off=torch.from_numpy(off.astype(np.int64)).to(dev),
+                     bed=torch.from_numpy(bed.astype(np.float64)).to(dev),
+                     bed_f32=int(bed.dtype == np.float32), n=int(len(off)),
+                     t=torch.from_numpy(np.asarray(sb.time_s, dtype=np.float64).copy()).to(dev),
+                     s=torch.from_numpy(np.asarray(sb.stage_m, dtype=np.float64).copy()).to(dev),
+                     nk=int(len(sb.time_s)))
+            T.stages.append(d)
+            skip[cells[:, 0] - ngh, cells[:, 1] - ngh] = True
+            all_cells.append(cells)
+        if all_cells:
+            u = np.unique(np.concatenate(all_cells), axis=0)
+            T.stage_union = torch.from_numpy((u[:, 0] * self.pitch + u[:, 1]).astype(np.int64)).to(dev)
+            excl = np.zeros(len(u), dtype=np.uint8)
+            if self._ghost is not None:
+                excl = self._ghost[u[:, 0] - ngh, u[:, 1] - ngh].astype(np.uint8)
+            T.stage_excl = torch.from_numpy(excl).to(dev)
+        else:
+            T.stage_union = None
+        T.skip = torch.from_numpy(skip.astype(np.uint8).ravel()).to(dev) if skip.any() else None
+        T.ghost_skip = (torch.from_numpy(self._ghost.astype(np.uint8).ravel()).to(dev)
+                        if self._ghost is not None else None)
+        # inflow inlets (solver.py:1916-1971)
+        T.inflows = []
+        for f in self._inflows:
+            off = f["i"] * self.pitch + f["j"]
+            T.inflows.append(dict(off=torch.from_numpy(off.astype(np.int64)).to(dev), n=int(len(off)),
+                                  step=-(f["si"] * self.pitch + f["sj"]),
+                                  t=torch.from_numpy(f["t"].copy()).to(dev),
+                                  q=torch.from_numpy(f["q"].copy()).to(dev), nk=int(len(f["t"])), f=f))
+        # friction
+        if cfg.friction is None:
+            T.fkind, T.ntab, T.ncls, T.nfield = L.FRICTION_NONE, None, None, None
+        elif self._ncls is not None:
+            T.fkind, T.ntab, T.ncls, T.nfield = L.FRICTION_TABLE, self._ntab, self._ncls, None
+        elif self._nfield is not None:
+            T.fkind, T.ntab, T.ncls, T.nfield = L.FRICTION_FIELD, None, None, self._nfield
+        else:
+            T.fkind, T.ncls, T.nfield = L.FRICTION_TABLE, None, None
+            T.ntab = torch.tensor([float(self.np_dtype.type(cfg.manning_n))], dtype=self.t_dtype, device=dev)
+        self._dev_tables = T
+        return T
+
+    # ---------------------------------------------------------- kernel calls
+    def _dense_args(self, src, dst, T=None, step=True):
+        cfg = self.cfg
+        a = L.GswDenseArgs()
+        a.abi_version = L.ABI_VERSION
+        a.dtype = self.code
+        a.nxp, a.nyp, a.ngh = self.nxp, self.nyp, self.mesh.ngh
+        a.pitch = self.pitch
+        a.q0, a.q1, a.q2 = _ptr(src[0]), _ptr(src[1]), _ptr(src[2])
+        a.qn0, a.qn1, a.qn2 = _ptr(dst[0]), _ptr(dst[1]), _ptr(dst[2])
+        a.bed = _ptr(self._b)
+        a.inside_mask = _ptr(self._mask)
+        a.mask_pitch = self.pitch
+        a.inv_dx, a.inv_dy = 1.0 / self.mesh.dx, 1.0 / self.mesh.dy
+        a.g, a.h_min = cfg.g, cfg.h_min
+        a.h_cfl = self._h_cfl()
+        a.tile_rows, a.warps = self._tile_rows, self._warps
+        if step:
+            T = T or self._tables()
+            a.state = _ptr(self._state)
+            a.lam_target = C.c_void_p(self._state.data_ptr() + L.GswLoopState.lam_bits.offset)
+            a.rain_kind = T.rain_kind
+            a.rain = _ptr(T.rain)
+            a.friction_kind = T.fkind
+            a.n_cls = _ptr(T.ncls)
+            a.n_cls_pitch = self.pitch
+            a.n_tab = _ptr(T.ntab)
+            a.n_tab_len = int(T.ntab.numel()) if T.ntab is not None else 0
+            a.n_field = _ptr(T.nfield)
+            a.vcap = float(cfg.friction_velocity_cap_ms)
+            a.quadratic = int(bool(cfg.friction_quadratic_alpha))
+            a.keep_h = int(bool(cfg.wetdry_keep_h))
+            a.max_h = _ptr(self._max_h)
+            a.cfl_skip = _ptr(T.skip)
+        return a
+
+    def _bc_args(self, buf):
+        a = L.GswBcArgs()
+        a.abi_version = L.ABI_VERSION
+        a.dtype = self.code
+        a.nxp, a.nyp, a.ngh, a.pitch = self.nxp, self.nyp, self.mesh.ngh, self.pitch
+        a.q0, a.q1, a.q2 = _ptr(buf[0]), _ptr(buf[1]), _ptr(buf[2])
+        kinds = [L.BC_CODES[k] for k in self.cfg.face_kinds()]
+        for f in range(4):
+            a.kinds[f] = kinds[f]
+        a.state = _ptr(self._state)
+        return a
+
+    def _launch_inflow(self, inl, src, s):
+        f = inl["f"]
+        a = L.GswInflowArgs()
+        a.abi_version = L.ABI_VERSION
+        a.dtype = self.code
+        a.pitch = self.pitch
+        a.q0, a.q1, a.q2 = _ptr(src[0]), _ptr(src[1]), _ptr(src[2])
+        a.bed = _ptr(self._b)
+        a.inlet_off = _ptr(inl["off"])
+        a.n, a.ngh = inl["n"], self.mesh.ngh
+        a.step_off = inl["step"]
+        a.nx_n, a.ny_n, a.ds, a.dry_frac = f["nx"], f["ny"], f["ds"], f["dry_frac"]
+        a.t_knots, a.q_knots, a.n_knots = _ptr(inl["t"]), _ptr(inl["q"]), inl["nk"]
+        a.state = _ptr(self._state)
+        L.call("gsw_inflow_apply", C.byref(a), s)
+
+    def _launch_step(self, k_parity: int, T):
+        """Ghost fill, inflow, fused step and stage for the buffer pair (k, 1-k)."""
+        src, dst = self._buf[k_parity], self._buf[1 - k_parity]
+        s = _stream()
+        L.call("gsw_bc_fill", C.byref(self._bc_args(src)), s)
+        for inl in T.inflows:
+            self._launch_inflow(inl, src, s)
+        L.call("gsw_dense_step", C.byref(self._dense_args(src, dst, T)), s)
+        multi = len(T.stages) > 1
+        for st in T.stages:
+            a = L.GswStageArgs()
+            a.abi_version = L.ABI_VERSION
+            a.dtype = self.code
+            a.pitch = self.pitch
+            a.q0, a.q1, a.q2 = _ptr(dst[0]), _ptr(dst[1]), _ptr(dst[2])
+            a.cell_off, a.bed64, a.bed_is_f32, a.n_cells = _ptr(st["off"]), _ptr(st["bed"]), st["bed_f32"], st["n"]
+            a.time_s, a.stage_m, a.n_knots = _ptr(st["t"]), _ptr(st["s"]), st["nk"]
+            a.state = _ptr(self._state)
+            a.g, a.h_cfl = self.cfg.g, self._h_cfl()
+            if not multi:
+                a.lam_target = C.c_void_p(self._state.data_ptr() + L.GswLoopState.lam_bits.offset)
+                a.cfl_ghost = _ptr(T.stage_excl)
+            L.call("gsw_stage_apply", C.byref(a), s)
+        if multi:   # fold the union of stage cells once, after every stage write
+            a = L.GswStageArgs()
+            a.abi_version = L.ABI_VERSION
+            a.dtype = self.code
+            a.pitch = self.pitch
+            a.q0, a.q1, a.q2 = _ptr(dst[0]), _ptr(dst[1]), _ptr(dst[2])
+            a.cell_off, a.n_cells = _ptr(T.stage_union), int(T.stage_union.numel())
+            a.state = _ptr(self._state)
+            a.lam_target = C.c_void_p(self._state.data_ptr() + L.GswLoopState.lam_bits.offset)
+            a.cfl_ghost = _ptr(T.stage_excl)
+            a.g, a.h_cfl = self.cfg.g, self._h_cfl()
+            L.call("gsw_lam_cells", C.byref(a), s)
+        self.diagnostics["rhs_calls"] += 1
+
+    def _dt_params(self, t_end, dt_max=None, max_steps=0, fixed_dt=None):
+        T = self._tables()
+        cfg = self.cfg
+        p = L.GswDtParams()
+        p.abi_version = L.ABI_VERSION
+        p.mode = 1 if fixed_dt is not None else 0
+        p.cfl_dmin = cfg.cfl * min(self.mesh.dx, self.mesh.dy)
+        p.lam_floor = (cfg.g * self._h_cfl()) ** 0.5
+        p.t_end = float(t_end)
+        p.eps_end = 1.0e-12
+        p.dt_max = float(dt_max) if dt_max is not None else 0.0
+        p.fixed_dt = float(fixed_dt) if fixed_dt is not None else 0.0
+        p.max_steps = int(max_steps)
+        if fixed_dt is None and T.n_rain:
+            p.rain_t, p.rain_lim, p.n_rain = _ptr(T.rain_t), _ptr(T.rain_lim), T.n_rain
+        elif T.n_rain:
+            p.rain_t, p.rain_lim, p.n_rain = _ptr(T.rain_t), C.c_void_p(0), T.n_rain
+        return p
+
+    def _write_state(self, **kw):
+        st = L.GswLoopState()
+        st.t = float(kw.get("t", self.t))
+        self._state_host.copy_(torch.frombuffer(bytearray(bytes(st) + bytes(128 - C.sizeof(st))),
+                                                dtype=torch.uint8))
+        self._state.copy_(self._state_host, non_blocking=False)
+
+    def _read_state(self) -> L.GswLoopState:
+        self._state_host.copy_(self._state, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return L.GswLoopState.from_buffer_copy(bytes(self._state_host.numpy()[:C.sizeof(L.GswLoopState)]))
+
+    def _lammax_into_state(self, skip):
+        """Wave speed of the current state into state.lam_bits (the reference's cfl_dt pass)."""
+        a = self._dense_args(self._buf[self._cur], self._buf[self._cur], step=False)
+        a.cfl_skip = _ptr(skip)
+        L.call("gsw_dense_lammax", C.byref(a),
+               C.c_void_p(self._state.data_ptr() + L.GswLoopState.lam_bits.offset), _stream())
+
+    # --------------------------------------------------------------- public
+    def apply_bc(self):
+        """Fill the ghost cells of the current state: face kinds, then inflow ghosts at
+        the current time (the reference's _apply_bc, solver.py:1750-1780)."""
+        T = self._tables()
+        self._write_state()
+        src = self._buf[self._cur]
+        s = _stream()
+        L.call("gsw_bc_fill", C.byref(self._bc_args(src)), s)
+        for inl in T.inflows:
+            self._launch_inflow(inl, src, s)
+
+    def residual(self):
+        """SRM-HLLC residual (3, nxp, nyp) of the current state on cells [2, n-3]^2, zero
+        elsewhere and outside the inside mask -- the fused residual kernel of the
+        reference (rhs_cuda.py:900-1207) without rain. Ghosts are used as they are;
+        call apply_bc() first to refresh them."""
+        out = torch.zeros((3, self.nxp, self.pitch), dtype=self.t_dtype, device=self.device)
+        a = self._dense_args(self._buf[self._cur], out, step=False)
+        L.call("gsw_dense_rhs", C.byref(a), _stream())
+        return out[:, :, :self.nyp]
+
+    def cfl_dt(self):
+        """Global CFL time step (solver.py:2569-2693)."""
+        T = self._tables()
+        self._write_state()
+        self._lammax_into_state(T.ghost_skip)
+        lam_max = self._read_state().lam_bits
+        lam_max = float(np.array([lam_max], dtype=np.uint64).view(np.float64)[0])
+        if not math.isfinite(lam_max):
+            raise FloatingPointError(f"cfl_dt: non-finite max wave speed {lam_max} at t={self.t:.3f}s "
+                                     f"-- NaN/Inf in hu/hv; check forcing/inputs")
+        lam_floor = (self.cfg.g * self._h_cfl()) ** 0.5
+        if lam_max < lam_floor:
+            lam_max = lam_floor
+        return self.cfg.cfl * min(self.mesh.dx, self.mesh.dy) / (lam_max + 1.0e-12)
+
+    def step(self, dt: Optional[float] = None):
+        """Advance one step of size dt (the CFL step when None); returns dt."""
+        if dt is None:
+            dt = self.cfl_dt()
+        dt = float(dt)
+        T = self._tables()
+        self._write_state()
+        p = self._dt_params(t_end=math.inf, fixed_dt=dt)
+        s = _stream()
+        L.call("gsw_dt_finalize", C.byref(p), _ptr(self._state), s)
+        self._launch_step(self._cur, T)
+        L.call("gsw_loop_commit", _ptr(self._state), s)
+        self._cur = 1 - self._cur
+        self._stepped = True
+        self.t += dt
+        self.nsteps += 1
+        self.last_dt = dt
+        return dt
+
+    def _rain_step_limit(self, dt):
+        cfg = self.cfg
+        if cfg.rainfall_forcing is not None:
+            rate = cfg.rainfall_forcing.rate_at_time(self.t, self.np_dtype if cfg.rainfall_forcing.gridded else None)
+        elif cfg.rainfall > 0.0:
+            rate = cfg.rainfall
+        else:
+            return dt
+        rmax = float(rate.max()) if getattr(rate, "ndim", 0) else float(rate)
+        if rmax <= 0.0:
+            return dt
+        dmin = min(self.mesh.dx, self.mesh.dy)
+        return min(dt, (cfg.cfl * dmin) ** (2.0 / 3.0) / (cfg.g * rmax) ** (1.0 / 3.0))
+
+    def run(self, t_end: float, max_steps: int = 10 ** 7, callback: Optional[Callable] = None,
+            dt_max: Optional[float] = None, window: int = 0):
+        """Step to ``t_end`` with CFL steps (the rain film limit and ``dt_max`` applied,
+        the last step clipped onto ``t_end``); returns the number of steps taken.
+
+        Without a callback the loop runs on the device: dt, t and the rain frame are
+        computed by gsw_dt_finalize and ``window`` steps at a time are replayed from a
+        CUDA graph. With a callback each step returns to the host, as in the reference.
+        """
+        t0 = time.perf_counter()
+        for sb in self._stage_list():
+            sb.warn_if_uncovered(t_end)
+        if callback is not None:
+            steps = 0
+            while self.t < t_end - 1.0e-12 and steps < max_steps:
+                dt = self._rain_step_limit(self.cfl_dt())
+                if dt_max is not None and dt > dt_max:
+                    dt = dt_max
+                if self.t + dt > t_end:
+                    dt = t_end - self.t
+                self.step(dt)
+                steps += 1
+                callback(self, steps)
+            self.diagnostics["wallclock"] = time.perf_counter() - t0
+            self.diagnostics["steps"] = steps
+            return steps
+        steps = self._run_device(t_end, max_steps, dt_max, window)
+        self.diagnostics["wallclock"] = time.perf_counter() - t0
+        self.diagnostics["steps"] = steps
+        return steps
+
+    def _window_size(self):
+        n = self.mesh.nx * self.mesh.ny
+        return 256 if n <= 1 << 20 else (64 if n <= 1 << 24 else 16)
+
+    def _run_device(self, t_end, max_steps, dt_max, window=0):
+        T = self._tables()
+        K = int(window) if window else self._window_size()
+        K += K % 2
+        self._write_state()
+        self._lammax_into_state(T.ghost_skip)
+        p = self._dt_params(t_end=t_end, dt_max=dt_max, max_steps=max_steps)
+        start_cur = self._cur
+
+        def one_window():
+            s = _stream()
+            for k in range(K):
+                L.call("gsw_dt_finalize", C.byref(p), _ptr(self._state), s)
+                self._launch_step((start_cur + k) % 2, T)
+
+        if self._use_graphs:
+            key = (K, start_cur, float(t_end), None if dt_max is None else float(dt_max), int(max_steps))
+            g = self._graph_cache.get(key)
+            if g is None:
+                self._graph_cache.clear()
+                side = torch.cuda.Stream(device=self.device)
+                side.wait_stream(torch.cuda.current_stream())
+                g = torch.cuda.CUDAGraph()
+                # capture on a side stream; the captured kernels read `done` first, so a
+                # replay after the loop has finished is a no-op
+                with torch.cuda.graph(g, stream=side):
+                    one_window()
+                torch.cuda.current_stream().wait_stream(side)
+                self._graph_cache[key] = g
+            run_window = g.replay
+        else:
+            run_window = one_window
+        while True:
+            run_window()
+            st = self._read_state()
+            if st.done:
+                break
+        L.call("gsw_loop_commit", _ptr(self._state), _stream())
+        st = self._read_state()
+        steps = int(st.steps)
+        self._cur = (start_cur + steps) % 2
+        if steps:
+            self._stepped = True
+            self.last_dt = float(st.dt)
+        self.t = float(st.t)
+        self.nsteps += steps
+        if st.error == L.ERR_NONFINITE:
+            raise FloatingPointError(f"cfl_dt: non-finite max wave speed {st.lam_used} at t={self.t:.3f}s "
+                                     f"-- NaN/Inf in hu/hv; check forcing/inputs")
+        return steps

@@ -1,0 +1,109 @@
+"""Seeded synthetic inputs of the benchmark cases (no external data is used).
+
+* dam_break        -- circular dam on a flat bed (r = hypot(i-(n-1)/2, j-(n-1)/2)).
+* fractal_bed      -- Gaussian random-phase spectrum with power ~ k^-3 (amplitude
+                      k^-3/2, DC removed), real part rescaled to [0, zmax] m, plus a
+                      planar slope along x.
+* voronoi_classes  -- land-cover classes by nearest of `n_seeds` uniform seeds,
+                      one class per seed drawn with rng.integers(n_classes).
+* dilate_cross     -- binary dilation with the 4-neighbour cross, as
+                      scipy.ndimage.binary_dilation's default structure.
+* tidal_case       -- the everywhere-wet sinusoidal-bed case with a tidal stage.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+MANNING_CLASSES = np.array([0.025, 0.04, 0.06, 0.1], dtype=np.float64)
+
+
+def dam_break(n=512, radius=64.0, h_in=2.0, h_out=0.5, dtype=np.float64):
+    i = np.arange(n, dtype=np.float64)[:, None]
+    j = np.arange(n, dtype=np.float64)[None, :]
+    r = np.hypot(i - (n - 1) / 2.0, j - (n - 1) / 2.0)
+    q0 = np.zeros((3, n, n), dtype=dtype)
+    q0[0] = np.where(r < radius, h_in, h_out)
+    bed = np.zeros((n, n), dtype=dtype)
+    return q0, bed
+
+
+def fractal_bed(nx, ny, dx, seed=0, zmax=40.0, slope=0.002):
+    rng = np.random.default_rng(seed)
+    kx = np.fft.fftfreq(nx)[:, None]
+    ky = np.fft.fftfreq(ny)[None, :]
+    k = np.sqrt(kx * kx + ky * ky)
+    amp = np.zeros_like(k)
+    nz = k > 0
+    amp[nz] = k[nz] ** -1.5
+    noise = rng.standard_normal((nx, ny)) + 1j * rng.standard_normal((nx, ny))
+    z = np.real(np.fft.ifft2(noise * amp))
+    z = (z - z.min()) / (z.max() - z.min()) * zmax
+    x = (np.arange(nx, dtype=np.float64) + 0.5) * dx
+    return z + slope * x[:, None]
+
+
+def voronoi_classes(nx, ny, n_seeds=256, n_classes=4, seed=0, chunk=1 << 20):
+    rng = np.random.default_rng(seed + 7919)
+    pts = rng.random((n_seeds, 2)) * np.array([nx, ny], dtype=np.float64)
+    cls_of_seed = rng.integers(n_classes, size=n_seeds).astype(np.uint8)
+    out = np.empty(nx * ny, dtype=np.uint8)
+    ii, jj = np.divmod(np.arange(nx * ny, dtype=np.int64), ny)
+    for s0 in range(0, nx * ny, chunk):
+        ci = ii[s0:s0 + chunk, None] + 0.5
+        cj = jj[s0:s0 + chunk, None] + 0.5
+        d2 = (ci - pts[None, :, 0]) ** 2 + (cj - pts[None, :, 1]) ** 2
+        out[s0:s0 + chunk] = cls_of_seed[np.argmin(d2, axis=1)]
+    return out.reshape(nx, ny)
+
+
+def voronoi_classes_fast(nx, ny, n_seeds=256, n_classes=4, seed=0):
+    """Same classes as voronoi_classes, through a KD-tree (for large grids)."""
+    from scipy.spatial import cKDTree
+    rng = np.random.default_rng(seed + 7919)
+    pts = rng.random((n_seeds, 2)) * np.array([nx, ny], dtype=np.float64)
+    cls_of_seed = rng.integers(n_classes, size=n_seeds).astype(np.uint8)
+    tree = cKDTree(pts)
+    out = np.empty((nx, ny), dtype=np.uint8)
+    jj = np.arange(ny, dtype=np.float64) + 0.5
+    rows = max(1, (1 << 22) // ny)
+    for i0 in range(0, nx, rows):
+        i1 = min(nx, i0 + rows)
+        ci = np.repeat(np.arange(i0, i1, dtype=np.float64) + 0.5, ny)
+        cj = np.tile(jj, i1 - i0)
+        _, idx = tree.query(np.stack([ci, cj], axis=1))
+        out[i0:i1] = cls_of_seed[idx].reshape(i1 - i0, ny)
+    return out
+
+
+def dilate_cross(mask, iterations):
+    """scipy.ndimage.binary_dilation(mask, iterations=k) with the default cross."""
+    m = np.asarray(mask, dtype=bool).copy()
+    for _ in range(int(iterations)):
+        d = m.copy()
+        d[1:, :] |= m[:-1, :]
+        d[:-1, :] |= m[1:, :]
+        d[:, 1:] |= m[:, :-1]
+        d[:, :-1] |= m[:, 1:]
+        m = d
+    return m
+
+
+def rain_on_terrain(n=8192, dx=3.0, seed=0, pct=60.0, band=8):
+    """Rain-on-terrain pluvial case: fractal bed, Voronoi Manning classes, dry start,
+    active set z < pct-th percentile dilated `band` times."""
+    z = fractal_bed(n, n, dx, seed=seed)
+    cls = voronoi_classes_fast(n, n, seed=seed) if n * n > (1 << 22) else voronoi_classes(n, n, seed=seed)
+    active = dilate_cross(z < np.percentile(z, pct), band)
+    return z, cls, active
+
+
+def tidal_case(nx, ny, dx=1.0, seed=0, eta0=1.5, noise=0.01, dtype=np.float32):
+    """Everywhere-wet case: z = 0.5 sin(2 pi x / 2000) cos(2 pi y / 1500) at cell centres,
+    eta = 1.5 + N(0, noise^2), zero velocity."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(nx, dtype=np.float64) + 0.5) * dx
+    y = (np.arange(ny, dtype=np.float64) + 0.5) * dx
+    z = 0.5 * np.sin(2 * np.pi * x / 2000.0)[:, None] * np.cos(2 * np.pi * y / 1500.0)[None, :]
+    eta = eta0 + noise * rng.standard_normal((nx, ny))
+    h = np.maximum(eta - z, 0.0)
+    return h.astype(dtype), z.astype(dtype)

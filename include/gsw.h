@@ -1,0 +1,258 @@
+/*
+ * gsw.h -- C ABI of libgsw.so, the B200 (sm_100a) finite-volume step of GeoSWE.
+ *
+ * The reference launches its step kernels from Python as CuPy RawKernels with raw
+ * device pointers and scalars on CuPy's current stream, and checks nothing on the
+ * device side (geoswe/solver.py:2271-2290, geoswe/compressed_solver.py:880-905).
+ * Each entry point below replaces one of those launches, or one of the host-side
+ * loop pieces the reference keeps in Python, with a C function that
+ *   - takes plain device pointers (the caller owns every buffer: torch tensors,
+ *     cudaMalloc, anything) and an explicit cudaStream_t,
+ *   - never allocates on the step path,
+ *   - returns 0 on success or a negative GSW_ERR_* code, with a message in
+ *     gsw_last_error() (thread-local).
+ * Every argument struct starts with `abi_version`; pass GSW_ABI_VERSION.
+ *
+ * Layouts
+ *   Dense fields are the reference's padded (nx+2*ngh, ny+2*ngh) C-order arrays,
+ *   with an explicit row pitch (elements between rows, >= nyp) so rows can be
+ *   128-byte aligned. The pointer addresses padded cell (0, 0).
+ *   Flat (compressed-mesh) fields live in brick storage: bricks of
+ *   GSW_BRICK_W x brick_h cells, each stored as brick_h rows of
+ *   GSW_BRICK_PITCH elements, bricks ordered along a Hilbert curve. The canonical
+ *   row-major flat order of the reference (geoswe/compressed_mesh.py:135-160) maps
+ *   to brick slots through the permutation gsw_mesh_build returns.
+ */
+#ifndef GSW_H
+#define GSW_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define GSW_API __attribute__((visibility("default")))
+#else
+#define GSW_API
+#endif
+
+#define GSW_ABI_VERSION 1u
+
+/* return codes */
+#define GSW_OK               0
+#define GSW_ERR_INVALID     -1   /* bad argument (shape, null pointer, range) */
+#define GSW_ERR_CUDA        -2   /* a CUDA runtime call failed */
+#define GSW_ERR_ABI         -3   /* abi_version mismatch */
+#define GSW_ERR_NONFINITE   -4   /* non-finite wave speed (NaN/Inf in the state) */
+#define GSW_ERR_RANGE       -5   /* table/delta out of the representable range */
+#define GSW_ERR_TIMEOUT     -6   /* a bounded device wait gave up */
+
+/* element types */
+#define GSW_F32 0
+#define GSW_F64 1
+
+/* boundary kinds per face (geoswe/bc.py:50-172) */
+#define GSW_BC_EXTRAPOLATE 0
+#define GSW_BC_WALL        1
+#define GSW_BC_FALL        2
+#define GSW_BC_PERIODIC    3
+#define GSW_BC_NONE        4   /* leave this face's ghosts alone */
+
+/* rain kinds */
+#define GSW_RAIN_NONE     0
+#define GSW_RAIN_UNIFORM  1    /* rain[frame] is one rate (m/s) */
+#define GSW_RAIN_GRIDDED  2    /* rain + frame*nx*ny is an interior (nx, ny) frame (m/s) */
+#define GSW_RAIN_LOOKUP   3    /* flat: rate_table[frame*ncol + lookup[cell]] */
+
+/* friction kinds */
+#define GSW_FRICTION_NONE  0
+#define GSW_FRICTION_TABLE 1   /* n = n_tab[n_cls[cell]] */
+#define GSW_FRICTION_FIELD 2   /* n = n_field[cell] */
+
+/* CFL velocity norms */
+#define GSW_NORM_LINF 0        /* max(|u|,|v|): geoswe/solver.py:152-205 */
+#define GSW_NORM_L2   1        /* sqrt(u^2+v^2): geoswe/compressed_solver.py:209-244 */
+
+/* compressed-mesh brick geometry */
+#define GSW_BRICK_W      30
+#define GSW_BRICK_PITCH  32
+
+/* ------------------------------------------------------------------------- */
+/* Device-resident loop control.                                              */
+/* One per solver, in device memory, written only by the library's kernels.  */
+/* ------------------------------------------------------------------------- */
+typedef struct GswLoopState {
+    double   t;          /* simulated time (s), accumulated in fp64 as the reference host loop does */
+    double   dt;         /* this step's time step (s) */
+    double   t_new;      /* t + dt, committed by the next gsw_dt_finalize / gsw_loop_commit */
+    int64_t  steps;      /* steps taken */
+    uint64_t lam_bits;   /* max wave speed of the current state as IEEE double bits (atomicMax target) */
+    double   lam_used;   /* wave speed the last dt came from (diagnostic) */
+    float    dt_f32;     /* (float)dt, the value fp32 kernels read */
+    int32_t  rain_idx;   /* rain frame of the current step */
+    int32_t  done;       /* 1: loop condition false, step cap reached, or error */
+    int32_t  error;      /* 0 or a GSW_ERR_* code raised on the device */
+    int32_t  pending;    /* 1: t_new/steps not committed yet */
+    int32_t  reserved[3];
+} GswLoopState;
+
+/* Time-step rule (replaces the host arithmetic of Solver2D.run / cfl_dt /
+ * _rain_step_limit, geoswe/solver.py:2569-2693, 2975-3027, and of the flat loop,
+ * geoswe/compressed_solver.py:713-748, 2133-2235). All in fp64:
+ *   lam = max((double)lam_f32, lam_floor)
+ *   dt  = cfl_dmin / (lam + 1e-12)
+ *   dt  = min(dt, rain_lim[rain_idx])   when rain_lim != NULL and rain_lim[idx] > 0
+ *   dt  = min(dt, dt_max)               when dt_max > 0
+ *   dt  = t_end - t                     when t + dt > t_end   (dense form)
+ *   dt  = min(dt, t_end - t)            (flat form, same value)
+ * The loop stops (done = 1) when !(t < t_end - eps_end) or steps >= max_steps. */
+typedef struct GswDtParams {
+    uint32_t abi_version;
+    int32_t  mode;        /* 0: CFL rule above; 1: fixed dt (fixed_dt) */
+    double   cfl_dmin;    /* cfl * min(dx, dy), computed by the caller in fp64 */
+    double   lam_floor;   /* sqrt(g * h_floor), computed by the caller */
+    double   t_end;
+    double   eps_end;     /* 1e-12 (dense loop) or 1e-9 (flat loop) */
+    double   dt_max;      /* <= 0: none */
+    double   fixed_dt;
+    int64_t  max_steps;
+    const double* rain_t;   /* device, n_rain knot times (bisect_right - 1, clamped) or NULL */
+    const double* rain_lim; /* device, per-frame rain step limit (<= 0: none) or NULL */
+    int32_t  n_rain;
+    int32_t  reserved;
+} GswDtParams;
+
+/* ------------------------------------------------------------------------- */
+/* Dense fused step.                                                          */
+/* ------------------------------------------------------------------------- */
+typedef struct GswDenseArgs {
+    uint32_t abi_version;
+    int32_t  dtype;            /* GSW_F32 or GSW_F64 */
+    int32_t  nxp, nyp, ngh;    /* padded extents; ngh >= 2 */
+    int64_t  pitch;            /* row pitch of every float field, elements */
+    const void* q0; const void* q1; const void* q2;   /* state in */
+    void* qn0; void* qn1; void* qn2;                  /* state out (step) / residual (rhs) */
+    const void* bed;
+    const uint8_t* inside_mask; /* padded, pitch `mask_pitch`; NULL: every cell inside */
+    int64_t  mask_pitch;
+    double   inv_dx, inv_dy, g, h_min;
+    /* step only */
+    const GswLoopState* state; /* dt, rain frame and done flag are read from here */
+    uint64_t* lam_target;     /* atomicMax target (double bits) of the new state's wave speed, or NULL */
+    int32_t  rain_kind;        /* GSW_RAIN_NONE / UNIFORM / GRIDDED */
+    const void* rain;          /* uniform: rates[n_frames]; gridded: frames[n_frames][nx][ny] */
+    int32_t  friction_kind;    /* GSW_FRICTION_* */
+    const uint8_t* n_cls; int64_t n_cls_pitch;
+    const void* n_tab; int32_t n_tab_len;
+    const void* n_field;       /* pitch = pitch */
+    double   vcap;             /* velocity cap (inf disables) */
+    int32_t  quadratic;        /* 1: quadratic alpha (default), 0: linearised */
+    int32_t  keep_h;           /* 1: dry cells keep max(h,0) (default), 0: h = 0 */
+    void*    max_h;            /* running max depth, pitch = pitch, or NULL */
+    const uint8_t* cfl_skip;   /* interior (nx, ny) C-order: 1 = excluded from the wave speed */
+    double   h_cfl;            /* wave-speed wet threshold (and divisor) */
+    int32_t  tile_rows;        /* rows per warp strip (0: default) */
+    int32_t  warps;            /* warps per block (0: default) */
+} GswDenseArgs;
+
+/* One fused step over the interior: SRM-HLLC residual, rain, forward Euler,
+ * wet/dry floor, point-implicit Manning, running max and the new state's wave
+ * speed. Replaces the fused-step launch (geoswe/rhs_cuda.py:1738-1796, 2095-2192;
+ * geoswe/solver.py:2166-2322) and the split path it equals (solver.py:2735-2771). */
+GSW_API int gsw_dense_step(const GswDenseArgs* a, void* stream);
+
+/* Residual only, written to qn0..qn2 (rhs0..rhs2) on cells [2, n-3]^2 with the
+ * inside mask honoured; other cells are set to 0. Replaces
+ * fused_rhs_linear2_lf_2d(recon="wb_srm", flux="hllc") (geoswe/rhs_cuda.py:2411-2556). */
+GSW_API int gsw_dense_rhs(const GswDenseArgs* a, void* stream);
+
+/* Wave speed of the current dense state into *lam_bits (atomicMax; caller zeroes it):
+ * max over interior cells of max(|u|,|v|) + sqrt(g h), cells with h < h_cfl or
+ * cfl_skip set skipped, non-finite -> +Inf. Replaces lammax_fp32_lean
+ * (geoswe/solver.py:152-205). */
+GSW_API int gsw_dense_lammax(const GswDenseArgs* a, uint64_t* lam_bits, void* stream);
+
+/* Ghost fill of one dense state. kinds[4] = x-, x+, y-, y+ (GSW_BC_*).
+ * Writes the non-corner ghost cells (the stencil reads no corner).
+ * Replaces apply_bc_2d / apply_bc_2d_face (geoswe/bc.py:50-172). */
+typedef struct GswBcArgs {
+    uint32_t abi_version;
+    int32_t  dtype;
+    int32_t  nxp, nyp, ngh;
+    int64_t  pitch;
+    void* q0; void* q1; void* q2;
+    int32_t  kinds[4];
+    const GswLoopState* state;   /* skip when state->done; may be NULL */
+} GswBcArgs;
+GSW_API int gsw_bc_fill(const GswBcArgs* a, void* stream);
+
+/* Stage (Dirichlet eta) boundary applied after the step: eta(t_new) by linear
+ * interpolation of (time_s, stage_m) clamped at the ends, h = max(eta - bed, 0),
+ * hu = hv = 0 on the listed cells; the wave speed of those cells is folded into
+ * lam_target. Replaces StageBoundary.apply (geoswe/forcing.py:315-377). */
+typedef struct GswStageArgs {
+    uint32_t abi_version;
+    int32_t  dtype;
+    int64_t  pitch;
+    void* q0; void* q1; void* q2;
+    const int64_t* cell_off;   /* n_cells element offsets (i*pitch + j) */
+    const double*  bed64;      /* n_cells bed values (fp64 copy) */
+    int32_t  bed_is_f32;       /* 1: eta - bed evaluated in fp32 (bed given as float32) */
+    int32_t  n_cells;
+    const double* time_s; const double* stage_m; int32_t n_knots;
+    const GswLoopState* state; /* eta is taken at state->t_new */
+    uint64_t* lam_target;      /* NULL: no wave-speed fold */
+    const uint8_t* cfl_ghost;  /* per stage cell: 1 = excluded from the wave speed, or NULL */
+    double g, h_cfl;
+} GswStageArgs;
+GSW_API int gsw_stage_apply(const GswStageArgs* a, void* stream);
+/* Fold the wave speed of the listed cells (cell_off, n_cells; cfl_ghost excludes) into
+ * lam_target, after several stage boundaries have written overlapping cells. Only the
+ * q*, cell_off, n_cells, cfl_ghost, state, lam_target, g and h_cfl fields are read. */
+GSW_API int gsw_lam_cells(const GswStageArgs* a, void* stream);
+
+/* Discharge inflow through ghost cells (one inlet): Q(t) = interp(t, knots),
+ * depth-weighted split w = h/sum(h) with numpy's pairwise float32 sum, dry
+ * inlet seeded from the bed relief or the critical depth. Replaces
+ * Solver2D._fill_inflow_ghosts / apply_inflow_discharge
+ * (geoswe/solver.py:1944-1971, geoswe/bc.py:175-235). */
+typedef struct GswInflowArgs {
+    uint32_t abi_version;
+    int32_t  dtype;
+    int64_t  pitch;
+    void* q0; void* q1; void* q2;
+    const void* bed;
+    const int64_t* inlet_off;   /* n element offsets of the inlet cells */
+    int32_t  n;
+    int32_t  ngh;
+    int64_t  step_off;          /* offset of one cell outward along the inward normal (-(si*pitch + sj)) */
+    double   nx_n, ny_n, ds, dry_frac;
+    const double* t_knots; const double* q_knots; int32_t n_knots;
+    const GswLoopState* state;  /* Q is taken at state->t (pre-step) */
+} GswInflowArgs;
+GSW_API int gsw_inflow_apply(const GswInflowArgs* a, void* stream);
+
+/* ------------------------------------------------------------------------- */
+/* Loop control.                                                              */
+/* ------------------------------------------------------------------------- */
+/* Commit the pending t/steps, test the loop condition, and compute this step's dt
+ * and rain frame from state->lam_bits (then zeroed for the step's reduction). */
+GSW_API int gsw_dt_finalize(const GswDtParams* p, GswLoopState* state, void* stream);
+/* Commit a pending t_new/steps (call once after the last step). */
+GSW_API int gsw_loop_commit(GswLoopState* state, void* stream);
+
+/* ------------------------------------------------------------------------- */
+/* Library                                                                    */
+/* ------------------------------------------------------------------------- */
+GSW_API const char* gsw_last_error(void);
+GSW_API uint32_t    gsw_abi_version(void);
+/* Number of this library's kernels launched since load (all entry points). */
+GSW_API uint64_t    gsw_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GSW_H */

@@ -1,0 +1,309 @@
+"""CPU oracle for the GeoSWE finite-volume step -- TEST INFRASTRUCTURE ONLY.
+
+This package is the checker: tests/, __graft_entry__.smoke() and the CPU-baseline
+leg of bench.py use it to compute what the GPU kernels must produce. The product
+(geoswe_b200) never imports it.
+
+  * liboracle.so (gsw_oracle.c): per-cell C restatement of the reference's fused
+    SRM-HLLC kernel text, CFL reductions and ghost fills, fp32 and fp64.
+  * OracleSolver2D: the reference's dense time loop (geoswe/solver.py:2569-3027)
+    driving those kernels, with dt/t arithmetic in Python floats as the reference
+    host loop does, plus the stage boundary (geoswe/forcing.py:315-377) and the
+    discharge inflow (geoswe/bc.py:175-235) restated in NumPy.
+  * numpy_ref: a NumPy restatement of the reference's CPU path (Solver2D with the
+    NumPy backend), the reference CPU implementation timed as the CPU baseline.
+"""
+from __future__ import annotations
+
+import bisect
+import ctypes as C
+import math
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+SRC = [HERE / "gsw_oracle.c", HERE / "gsw_oracle_body.h"]
+
+
+def build(force=False):
+    """Compile liboracle.so with gcc (no fused multiply-add, no fast-math, OpenMP)."""
+    if not force and LIB.exists() and all(LIB.stat().st_mtime >= p.stat().st_mtime for p in SRC):
+        return LIB
+    tmp = LIB.with_suffix(".so.tmp")
+    subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
+                    "-shared", "-o", str(tmp), str(HERE / "gsw_oracle.c"), "-lm"], check=True)
+    tmp.replace(LIB)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        _lib = C.CDLL(str(LIB))
+        for sfx in ("f32", "f64"):
+            getattr(_lib, f"gswo_dense_step_{sfx}").restype = C.c_double
+            getattr(_lib, f"gswo_dense_lammax_{sfx}").restype = C.c_double
+        _lib.gswo_pow_m43_f32.restype = C.c_double
+        _lib.gswo_pow_m43_f32.argtypes = [C.c_float]
+        _lib.gswo_pow_m43_f64.restype = C.c_double
+        _lib.gswo_pow_m43_f64.argtypes = [C.c_double]
+    return _lib
+
+
+def _sfx(dtype):
+    return "f32" if np.dtype(dtype) == np.float32 else "f64"
+
+
+def _R(dtype):
+    return C.c_float if np.dtype(dtype) == np.float32 else C.c_double
+
+
+def _p(a):
+    return C.c_void_p(0) if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+BC = {"extrapolate": 0, "wall": 1, "fall": 2, "periodic": 3, "none": 4}
+
+
+def dense_rhs(q, b, dx, dy, g, h_min, mask=None):
+    """Residual (3, nxp, nyp) of the padded state q on cells [2, n-3]^2."""
+    dt = q.dtype
+    q = np.ascontiguousarray(q)
+    b = np.ascontiguousarray(b, dtype=dt)
+    nxp, nyp = q.shape[1:]
+    r = np.zeros_like(q)
+    R = _R(dt)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    getattr(lib(), f"gswo_dense_rhs_{_sfx(dt)}")(
+        _p(q[0]), _p(q[1]), _p(q[2]), _p(b), C.c_int(nxp), C.c_int(nyp), C.c_int64(nyp),
+        R(1.0 / dx), R(1.0 / dy), R(g), R(h_min), _p(m), _p(r[0]), _p(r[1]), _p(r[2]))
+    return r
+
+
+def dense_step(q, b, ngh, dx, dy, g, h_min, dt, *, mask=None, rain=None, rain_kind=0,
+               friction_kind=0, ncls=None, ntab=None, nfield=None, vcap=15.0, quad=True,
+               keep_h=True, max_h=None, skip=None, h_cfl=None):
+    """One fused step; returns (qn, lam_new)."""
+    dtp = q.dtype
+    q = np.ascontiguousarray(q)
+    nxp, nyp = q.shape[1:]
+    qn = np.empty_like(q)
+    R = _R(dtp)
+    conv = lambda a, d=dtp: None if a is None else np.ascontiguousarray(a, dtype=d)
+    lam = getattr(lib(), f"gswo_dense_step_{_sfx(dtp)}")(
+        _p(q[0]), _p(q[1]), _p(q[2]), _p(conv(b)), C.c_int(nxp), C.c_int(nyp), C.c_int(ngh),
+        C.c_int64(nyp), R(1.0 / dx), R(1.0 / dy), R(g), R(h_min), R(dt),
+        _p(conv(mask, np.uint8)), C.c_int(rain_kind), _p(conv(rain)), C.c_int(friction_kind),
+        _p(conv(ncls, np.uint8)), _p(conv(ntab)), _p(conv(nfield)), R(vcap), C.c_int(int(quad)),
+        C.c_int(int(keep_h)), _p(qn[0]), _p(qn[1]), _p(qn[2]), _p(max_h), _p(conv(skip, np.uint8)),
+        R(h_cfl if h_cfl is not None else h_min))
+    return qn, float(lam)
+
+
+def dense_lammax(q, ngh, g, h_cfl, skip=None):
+    dtp = q.dtype
+    q = np.ascontiguousarray(q)
+    nxp, nyp = q.shape[1:]
+    R = _R(dtp)
+    s = None if skip is None else np.ascontiguousarray(skip, dtype=np.uint8)
+    return float(getattr(lib(), f"gswo_dense_lammax_{_sfx(dtp)}")(
+        _p(q[0]), _p(q[1]), _p(q[2]), C.c_int(nxp), C.c_int(nyp), C.c_int(ngh), C.c_int64(nyp),
+        R(g), R(h_cfl), _p(s)))
+
+
+def bc_fill(q, ngh, kinds):
+    """In-place ghost fill of the padded state (kinds for x-, x+, y-, y+)."""
+    assert q.flags.c_contiguous
+    nxp, nyp = q.shape[1:]
+    k = (C.c_int * 4)(*[BC[x] for x in kinds])
+    getattr(lib(), f"gswo_bc_{_sfx(q.dtype)}")(_p(q[0]), _p(q[1]), _p(q[2]), C.c_int(nxp),
+                                                C.c_int(nyp), C.c_int(ngh), C.c_int64(nyp), k)
+
+
+def pow_m43(x, dtype=np.float32):
+    L = lib()
+    return L.gswo_pow_m43_f32(float(x)) if np.dtype(dtype) == np.float32 else L.gswo_pow_m43_f64(float(x))
+
+
+# ---------------------------------------------------------------------------
+# Host-side pieces of the reference loop, restated.
+# ---------------------------------------------------------------------------
+def rain_index(time_s, t):
+    """bisect_right(time_s, t) - 1, clamped (geoswe/forcing.py:191-193)."""
+    tl = list(np.asarray(time_s, dtype=np.float64).tolist())
+    idx = max(0, bisect.bisect_right(tl, float(t)) - 1)
+    return min(idx, len(tl) - 1)
+
+
+def stage_eta(time_s, stage_m, t):
+    """Clamped linear interpolation (geoswe/forcing.py:283-313)."""
+    tl = list(np.asarray(time_s, dtype=np.float64).tolist())
+    sl = list(np.asarray(stage_m, dtype=np.float64).tolist())
+    t = float(t)
+    if t <= tl[0]:
+        return sl[0]
+    if t >= tl[-1]:
+        return sl[-1]
+    i = bisect.bisect_left(tl, t)
+    w = (t - tl[i - 1]) / (tl[i] - tl[i - 1])
+    return sl[i - 1] + w * (sl[i] - sl[i - 1])
+
+
+def inflow_apply(q, bed, idx_i, idx_j, nx_n, ny_n, ds, Q, ngh, dry_frac=0.10):
+    """Discharge inflow through the ghost cells (geoswe/bc.py:175-235), NumPy."""
+    if len(idx_i) == 0:
+        return
+    h = q[0][idx_i, idx_j]
+    z = bed[idx_i, idx_j]
+    s = float(h.sum())
+    if s > 0.0:
+        w = h / s
+        h_face = h
+    else:
+        zmin = z.min(); zmax = z.max()
+        h_face = np.maximum(zmin + dry_frac * (zmax - zmin) - z, 0.0)
+        low = (z <= zmin)
+        n_low = float(low.sum())
+        if float(h_face.max()) <= 0.0:
+            q_cell = abs(Q) / (max(n_low, 1.0) * ds)
+            h_face = h_face + (q_cell * q_cell / 9.80665) ** (1.0 / 3.0)
+        w = np.where(low, 1.0 / max(n_low, 1.0), 0.0)
+    qn = (Q / ds) * w
+    si, sj = int(round(nx_n)), int(round(ny_n))
+    for k in range(1, int(ngh) + 1):
+        gi = idx_i - k * si
+        gj = idx_j - k * sj
+        q[0][gi, gj] = h_face
+        q[1][gi, gj] = qn * nx_n
+        q[2][gi, gj] = qn * ny_n
+
+
+class OracleSolver2D:
+    """The reference dense loop on the C oracle kernels (fp32 or fp64).
+
+    Parameters mirror geoswe_b200.Solver2D: padded state (3, nxp, nyp) and bed, the
+    face BC kinds, Manning (none / table / field / scalar), rain (none / uniform table /
+    gridded frames with their times), stage boundaries and inflow inlets.
+    """
+
+    def __init__(self, q_pad, b_pad, ngh, dx, dy, *, g=9.81, h_min=1e-6, h_cfl=None, cfl=0.5,
+                 kinds=("extrapolate",) * 4, mask=None, friction=None, ncls=None, ntab=None,
+                 nfield=None, manning_n=0.0, vcap=15.0, quad=True, keep_h=True,
+                 rain_times=None, rain_frames=None, rain_gridded=False, rain_rmax=None,
+                 stages=(), inflows=(), ghost=None, track_max=True):
+        self.q = np.ascontiguousarray(q_pad).copy()
+        self.dtype = self.q.dtype
+        self.b = np.ascontiguousarray(b_pad, dtype=self.dtype)
+        self.ngh, self.dx, self.dy = ngh, dx, dy
+        self.g, self.h_min, self.cfl = g, h_min, cfl
+        hc = h_cfl if h_cfl is not None else h_min
+        if self.dtype == np.float32 and hc < 1e-6:
+            hc = 1e-6
+        self.h_cfl = hc
+        self.kinds = list(kinds)
+        self.mask = mask
+        self.vcap, self.quad, self.keep_h = vcap, quad, keep_h
+        if friction is None:
+            self.fk, self.ncls, self.ntab, self.nfield = 0, None, None, None
+        elif ncls is not None:
+            self.fk, self.ncls, self.ntab, self.nfield = 1, ncls, np.asarray(ntab, np.float32).astype(self.dtype), None
+        elif nfield is not None:
+            self.fk, self.ncls, self.ntab, self.nfield = 2, None, None, nfield
+        else:   # scalar n: a one-entry table read for every cell
+            self.fk = 1
+            self.ncls = np.zeros(self.q.shape[1:], np.uint8)
+            self.ntab = np.array([manning_n], dtype=self.dtype)
+            self.nfield = None
+        self.rain_times = None if rain_times is None else np.asarray(rain_times, np.float64)
+        self.rain_frames = rain_frames
+        self.rain_gridded = rain_gridded
+        self.rain_rmax = rain_rmax
+        self.stages = list(stages)
+        self.inflows = list(inflows)
+        nx, ny = self.q.shape[1] - 2 * ngh, self.q.shape[2] - 2 * ngh
+        self.ghost = ghost
+        skip = np.zeros((nx, ny), bool) if (ghost is not None or self.stages) else None
+        if ghost is not None:
+            skip |= ghost
+        for s in self.stages:
+            skip[np.asarray(s["cells"])[:, 0] - ngh, np.asarray(s["cells"])[:, 1] - ngh] = True
+        self.skip = skip
+        self.max_h = np.zeros(self.q.shape[1:], dtype=self.dtype) if track_max else None
+        self.t = 0.0
+        self.nsteps = 0
+        self.dts = []
+
+    def cfl_dt(self):
+        lam = dense_lammax(self.q, self.ngh, self.g, self.h_cfl, self.ghost)
+        if not math.isfinite(lam):
+            raise FloatingPointError(f"non-finite max wave speed at t={self.t}")
+        floor = (self.g * self.h_cfl) ** 0.5
+        if lam < floor:
+            lam = floor
+        return self.cfl * min(self.dx, self.dy) / (lam + 1.0e-12)
+
+    def _rain_now(self):
+        if self.rain_times is None:
+            return 0, None, 0.0
+        k = rain_index(self.rain_times, self.t)
+        return k, self.rain_frames[k], self.rain_rmax[k]
+
+    def rain_step_limit(self, dt):
+        if self.rain_times is None:
+            return dt
+        _, _, rmax = self._rain_now()
+        if rmax <= 0.0:
+            return dt
+        dmin = min(self.dx, self.dy)
+        return min(dt, (self.cfl * dmin) ** (2.0 / 3.0) / (self.g * rmax) ** (1.0 / 3.0))
+
+    def step(self, dt):
+        bc_fill(self.q, self.ngh, self.kinds)
+        for f in self.inflows:
+            Q = float(np.interp(self.t, f["t"], f["q"]))
+            inflow_apply(self.q, self.b, f["i"], f["j"], f["nx"], f["ny"], f["ds"], Q, self.ngh,
+                         f.get("dry_frac", 0.10))
+        rk, rain = 0, None
+        if self.rain_times is not None:
+            _, frame, _ = self._rain_now()
+            rk = 2 if self.rain_gridded else 1
+            rain = np.asarray(frame, dtype=self.dtype).reshape(-1) if self.rain_gridded else \
+                np.array([frame], dtype=self.dtype)
+        qn, _ = dense_step(self.q, self.b, self.ngh, self.dx, self.dy, self.g, self.h_min,
+                           self.dtype.type(dt), mask=self.mask, rain=rain, rain_kind=rk,
+                           friction_kind=self.fk, ncls=self.ncls, ntab=self.ntab, nfield=self.nfield,
+                           vcap=self.vcap, quad=self.quad, keep_h=self.keep_h, max_h=self.max_h,
+                           skip=self.skip, h_cfl=self.h_cfl)
+        self.q = qn
+        self.t += dt
+        for s in self.stages:
+            eta = stage_eta(s["time_s"], s["stage_m"], self.t)
+            bed = np.asarray(s["bed"])
+            hn = np.maximum(eta - bed, 0.0)
+            c = np.asarray(s["cells"])
+            self.q[0][c[:, 0], c[:, 1]] = hn
+            self.q[1][c[:, 0], c[:, 1]] = 0.0
+            self.q[2][c[:, 0], c[:, 1]] = 0.0
+        self.nsteps += 1
+        self.dts.append(dt)
+        return dt
+
+    def run(self, t_end, max_steps=10 ** 7, dt_max=None):
+        steps = 0
+        while self.t < t_end - 1.0e-12 and steps < max_steps:
+            dt = self.rain_step_limit(self.cfl_dt())
+            if dt_max is not None and dt > dt_max:
+                dt = dt_max
+            if self.t + dt > t_end:
+                dt = t_end - self.t
+            self.step(dt)
+            steps += 1
+        return steps

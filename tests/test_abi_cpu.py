@@ -1,0 +1,69 @@
+"""The C ABI library loads here (no GPU) and exports every entry point include/gsw.h
+declares; the ctypes layouts match the C structs."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _declared():
+    txt = (ROOT / "include" / "gsw.h").read_text()
+    return sorted(set(re.findall(r"GSW_API\s+[\w\s\*]+?\b(gsw_\w+)\s*\(", txt)))
+
+
+def test_header_declares_entry_points():
+    names = _declared()
+    assert "gsw_dense_step" in names and "gsw_dt_finalize" in names and len(names) >= 10
+
+
+def test_library_loads_and_exports_all_declared():
+    from geoswe_b200 import _lib
+    L = _lib.lib()
+    for n in _declared():
+        assert hasattr(L, n), n
+    assert L.gsw_abi_version() == _lib.ABI_VERSION
+    assert set(_declared()) == set(_lib.exported_symbols())
+
+
+def test_struct_layouts_match_c(tmp_path):
+    from geoswe_b200 import _lib
+    src = tmp_path / "abi.c"
+    checks = {"GswLoopState": ["lam_bits", "dt_f32", "done", "reserved"],
+              "GswDtParams": ["cfl_dmin", "max_steps", "rain_lim", "n_rain"],
+              "GswDenseArgs": ["pitch", "state", "lam_target", "rain", "n_cls_pitch", "n_field", "vcap",
+                               "max_h", "cfl_skip", "h_cfl", "warps"],
+              "GswBcArgs": ["pitch", "kinds", "state"],
+              "GswStageArgs": ["pitch", "bed_is_f32", "time_s", "lam_target", "g", "h_cfl"],
+              "GswInflowArgs": ["pitch", "step_off", "nx_n", "t_knots", "state"]}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{ROOT}/include/gsw.h"', "int main(){"]
+    for s, fs in checks.items():
+        lines.append(f'printf("{s} %zu\\n", sizeof({s}));')
+        for f in fs:
+            lines.append(f'printf("{s}.{f} %zu\\n", offsetof({s}, {f}));')
+    lines.append("return 0;}")
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "abi"
+    subprocess.run(["gcc", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    for line in out.strip().splitlines():
+        key, val = line.rsplit(" ", 1)
+        if "." in key:
+            cls, f = key.split(".")
+            got = getattr(getattr(_lib, cls), f).offset
+        else:
+            got = C.sizeof(getattr(_lib, key))
+        assert got == int(val), (key, got, val)
+
+
+def test_solver_refuses_without_cuda():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("CUDA present")
+    import numpy as np
+    from geoswe_b200 import Config, Mesh2D, Solver2D
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        Solver2D(Mesh2D(8, 8, 1.0, 1.0, ngh=2), Config(), np.zeros((3, 8, 8)), np.zeros((8, 8)))
