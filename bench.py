@@ -143,7 +143,7 @@ def run_gsw(args, rank, world):
         torch.distributed.barrier()
     clk = Clocks(int(os.environ.get("LOCAL_RANK", 0)))
     clk.start()
-    l0 = _lib.launch_count()
+    l0 = s.kernel_launches
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record()
@@ -152,7 +152,7 @@ def run_gsw(args, rank, world):
     torch.cuda.synchronize()
     clocks = clk.stop()
     ms = e0.elapsed_time(e1)
-    launches = _lib.launch_count() - l0
+    launches = s.kernel_launches - l0
     assert steps == args.steps, (steps, args.steps)
     # ---------------- dominant kernel alone (roofline) ----------------
     kern_ms = time_step_kernel(s, reps=args.kernel_reps)

@@ -73,9 +73,8 @@ __device__ __forceinline__ float pow_m43(float x) {
     }
     return r / x;
 }
-// fp64: same iteration in double with two more steps (quadratic convergence from
-// the binary32 guess), r/x correctly rounded to well below one double ulp's worth
-// of the model.
+// fp64: the same iteration in double, six steps from the binary32 guess; r/x is within
+// ~6 double ulp of x^(-4/3).
 __device__ __forceinline__ double pow_m43(double x) {
     const float xf = (float)x;
     const uint32_t ix = __float_as_uint(xf);
@@ -131,28 +130,24 @@ __device__ __forceinline__ void hllc(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
     const T FR_h = huNR;
     const T FR_N = huNR * uNR + pR;
     const T FR_T = huNR * uTR;
-    if (SL >= z) { Fh = FL_h; FN = FL_N; FT = FL_T; return; }
-    if (SM >= z) {
-        const T facL = (SL - uNL) / (SL - SM + (T)1.0e-30);
-        const T hLs = hL * facL;
-        const T huNLs = hLs * SM;
-        const T huTLs = hLs * uTL;
-        Fh = FL_h + SL * (hLs - hL);
-        FN = FL_N + SL * (huNLs - huNL);
-        FT = FL_T + SL * (huTLs - huTL);
-        return;
-    }
-    if (SR >= z) {
-        const T facR = (SR - uNR) / (SR - SM + (T)1.0e-30);
-        const T hRs = hR * facR;
-        const T huNRs = hRs * SM;
-        const T huTRs = hRs * uTR;
-        Fh = FR_h + SR * (hRs - hR);
-        FN = FR_N + SR * (huNRs - huNR);
-        FT = FR_T + SR * (huTRs - huTR);
-        return;
-    }
-    Fh = FR_h; FN = FR_N; FT = FR_T;
+    // One star state, on the side of the contact the reference selects (SM >= 0: left),
+    // with the reference's own expressions for that side: a single division and no
+    // divergent branches, and the same values where the reference's select uses them.
+    const bool left = SM >= z;
+    const T S = left ? SL : SR;
+    const T hK = left ? hL : hR, uNK = left ? uNL : uNR, uTK = left ? uTL : uTR;
+    const T huNK = left ? huNL : huNR, huTK = left ? huTL : huTR;
+    const T FK_h = left ? FL_h : FR_h, FK_N = left ? FL_N : FR_N, FK_T = left ? FL_T : FR_T;
+    const T fac = (S - uNK) / (S - SM + (T)1.0e-30);
+    const T hKs = hK * fac;
+    const T huNKs = hKs * SM;
+    const T huTKs = hKs * uTK;
+    const T Fs_h = FK_h + S * (hKs - hK);
+    const T Fs_N = FK_N + S * (huNKs - huNK);
+    const T Fs_T = FK_T + S * (huTKs - huTK);
+    if (SL >= z)           { Fh = FL_h; FN = FL_N; FT = FL_T; }
+    else if (left || SR >= z) { Fh = Fs_h; FN = Fs_N; FT = Fs_T; }
+    else                   { Fh = FR_h; FN = FR_N; FT = FR_T; }
 }
 
 // One face between cell L (lower index) and cell R (upper index) along one axis.

@@ -208,61 +208,87 @@ __global__ void __launch_bounds__(256) dense_lammax_kernel(DenseK<T> p, unsigned
     block_max_to(lam, out);
 }
 
-// Ghost fill (bc.py:50-172), non-corner ghosts: x-ghost rows over interior columns,
-// y-ghost columns over interior rows.
+// Ghost fill (bc.py:50-172). apply_bc_2d fills the x faces over all columns, then the
+// y faces over all rows, so a corner ends up as the y rule applied to the x-filled cell
+// of its row. One launch computes every ghost directly from interior cells: x-ghost
+// rows over interior columns, y-ghost columns over interior rows, and the corners by
+// composing the two rules, which is what the two passes produce.
+__device__ __forceinline__ int bc_src(int kind, int g, int n, int ngh) {
+    // source index of ghost g along an axis of length n, for EXTRAPOLATE/WALL/PERIODIC
+    if (g < ngh) {
+        const int k = g;
+        return kind == GSW_BC_WALL ? (2 * ngh - 1 - k) : kind == GSW_BC_PERIODIC ? (n - 2 * ngh + k) : ngh;
+    }
+    const int k = g - (n - ngh);
+    return kind == GSW_BC_WALL ? (n - ngh - 1 - k) : kind == GSW_BC_PERIODIC ? (ngh + k) : (n - ngh - 1);
+}
+
 template <typename T>
 __global__ void bc_fill_kernel(T* q0, T* q1, T* q2, int nxp, int nyp, int ngh, int64_t pitch,
                                int kxm, int kxp, int kym, int kyp, const GswLoopState* st) {
     if (st != nullptr && st->done) return;
     const int nyi = nyp - 2 * ngh, nxi = nxp - 2 * ngh;
-    const int64_t nX = (int64_t)2 * ngh * nyi;      // x-ghost cells
-    const int64_t nY = (int64_t)2 * ngh * nxi;      // y-ghost cells
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nX + nY;
+    const int64_t nX = (int64_t)2 * ngh * nyi;      // x-ghost cells at interior columns
+    const int64_t nY = (int64_t)2 * ngh * nxi;      // y-ghost cells at interior rows
+    const int64_t nC = (int64_t)4 * ngh * ngh;      // corners
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nX + nY + nC;
          t += (int64_t)gridDim.x * blockDim.x) {
-        int gi, gj, si, sj, kind;
-        bool flip_u = false, flip_v = false;
+        int gi, gj, kx = GSW_BC_NONE, ky = GSW_BC_NONE;
         if (t < nX) {
             const int side = (int)(t / ((int64_t)ngh * nyi));
             const int64_t rem = t - (int64_t)side * ngh * nyi;
             const int k = (int)(rem / nyi);
             gj = ngh + (int)(rem - (int64_t)k * nyi);
-            sj = gj;
-            if (side == 0) {             // x-: ghost row k
-                kind = kxm; gi = k;
-                si = (kind == GSW_BC_WALL) ? (2 * ngh - 1 - k)
-                   : (kind == GSW_BC_PERIODIC) ? (nxp - 2 * ngh + k) : ngh;
-            } else {                     // x+: ghost row nxp-ngh+k
-                kind = kxp; gi = nxp - ngh + k;
-                si = (kind == GSW_BC_WALL) ? (nxp - ngh - 1 - k)
-                   : (kind == GSW_BC_PERIODIC) ? (ngh + k) : (nxp - ngh - 1);
-            }
-            flip_u = (kind == GSW_BC_WALL);
-        } else {
+            gi = side == 0 ? k : nxp - ngh + k;
+            kx = side == 0 ? kxm : kxp;
+        } else if (t < nX + nY) {
             const int64_t u = t - nX;
             const int side = (int)(u / ((int64_t)ngh * nxi));
             const int64_t rem = u - (int64_t)side * ngh * nxi;
             const int k = (int)(rem / nxi);
             gi = ngh + (int)(rem - (int64_t)k * nxi);
-            si = gi;
-            if (side == 0) {             // y-: ghost column k
-                kind = kym; gj = k;
-                sj = (kind == GSW_BC_WALL) ? (2 * ngh - 1 - k)
-                   : (kind == GSW_BC_PERIODIC) ? (nyp - 2 * ngh + k) : ngh;
-            } else {                     // y+: ghost column nyp-ngh+k
-                kind = kyp; gj = nyp - ngh + k;
-                sj = (kind == GSW_BC_WALL) ? (nyp - ngh - 1 - k)
-                   : (kind == GSW_BC_PERIODIC) ? (ngh + k) : (nyp - ngh - 1);
-            }
-            flip_v = (kind == GSW_BC_WALL);
+            gj = side == 0 ? k : nyp - ngh + k;
+            ky = side == 0 ? kym : kyp;
+            if (ky == GSW_BC_NONE) continue;
+        } else {
+            const int64_t u = t - nX - nY;
+            const int c = (int)(u / ((int64_t)ngh * ngh));
+            const int rem = (int)(u - (int64_t)c * ngh * ngh);
+            const int a = rem / ngh, bb = rem - a * ngh;
+            gi = (c & 1) ? nxp - ngh + a : a;
+            gj = (c & 2) ? nyp - ngh + bb : bb;
+            kx = (c & 1) ? kxp : kxm;
+            ky = (c & 2) ? kyp : kym;
+            if (ky == GSW_BC_NONE && kx == GSW_BC_NONE) continue;
         }
-        if (kind == GSW_BC_NONE) continue;
         const int64_t go = (int64_t)gi * pitch + gj;
-        if (kind == GSW_BC_FALL) { q0[go] = (T)0; q1[go] = (T)0; q2[go] = (T)0; continue; }
-        const int64_t so = (int64_t)si * pitch + sj;
-        const T a = q0[so], bu = q1[so], bv = q2[so];
-        q0[go] = a;
-        q1[go] = flip_u ? -bu : bu;
-        q2[go] = flip_v ? -bv : bv;
+        // value of the x pass at (row gi, column cj)
+        auto xval = [&](int cj, T& a, T& u, T& v) {
+            if (kx == GSW_BC_NONE) { const int64_t o = (int64_t)gi * pitch + cj; a = q0[o]; u = q1[o]; v = q2[o]; return; }
+            if (kx == GSW_BC_FALL) { a = (T)0; u = (T)0; v = (T)0; return; }
+            const int64_t o = (int64_t)bc_src(kx, gi, nxp, ngh) * pitch + cj;
+            a = q0[o]; u = q1[o]; v = q2[o];
+            if (kx == GSW_BC_WALL) u = -u;
+        };
+        T a, u, v;
+        if (t < nX) {
+            xval(gj, a, u, v);
+            if (kx == GSW_BC_NONE) continue;
+        } else if (ky == GSW_BC_NONE) {            // corner left to the x pass
+            xval(gj, a, u, v);
+        } else if (ky == GSW_BC_FALL) {
+            a = (T)0; u = (T)0; v = (T)0;
+        } else {
+            const int sj = bc_src(ky, gj, nyp, ngh);
+            if (t < nX + nY) {
+                const int64_t o = (int64_t)gi * pitch + sj;
+                a = q0[o]; u = q1[o]; v = q2[o];
+            } else {
+                xval(sj, a, u, v);
+            }
+            if (ky == GSW_BC_WALL) v = -v;
+        }
+        q0[go] = a; q1[go] = u; q2[go] = v;
     }
 }
 
@@ -427,7 +453,8 @@ extern "C" int gsw_bc_fill(const GswBcArgs* a, void* stream) {
         return set_error(GSW_ERR_INVALID, "bc: bad extents");
     for (int f = 0; f < 4; ++f)
         if (a->kinds[f] < 0 || a->kinds[f] > GSW_BC_NONE) return set_error(GSW_ERR_INVALID, "bc: bad kind %d", a->kinds[f]);
-    const int64_t n = (int64_t)2 * a->ngh * (a->nyp - 2 * a->ngh) + (int64_t)2 * a->ngh * (a->nxp - 2 * a->ngh);
+    const int64_t n = (int64_t)2 * a->ngh * (a->nyp - 2 * a->ngh) + (int64_t)2 * a->ngh * (a->nxp - 2 * a->ngh) +
+                      (int64_t)4 * a->ngh * a->ngh;
     const int grid = (int)std::min<int64_t>(sm_count() * 4, (n + 255) / 256);
     cudaStream_t s = (cudaStream_t)stream;
     if (a->dtype == GSW_F32)

@@ -133,6 +133,7 @@ class Solver2D:
         self._graph_cache = {}
         self._dev_tables = None
         self._tables_key = None
+        self.kernel_launches = 0        # libgsw kernels enqueued or replayed by this solver
         if cfg.manning_field is not None and cfg.friction is not None:
             self._nfield = torch.zeros((self.nxp, self.pitch), dtype=td, device=dev)
             self._nfield[:, :self.nyp].copy_(torch.from_numpy(np.ascontiguousarray(mf, dtype=self.np_dtype)))
@@ -476,6 +477,8 @@ class Solver2D:
         L.call("gsw_bc_fill", C.byref(self._bc_args(src)), s)
         for inl in T.inflows:
             self._launch_inflow(inl, src, s)
+        n = 2 + len(T.inflows) + 2 * len(T.stages) + (1 if len(T.stages) > 1 else 0)
+        self._counting += n
         L.call("gsw_dense_step", C.byref(self._dense_args(src, dst, T)), s)
         multi = len(T.stages) > 1
         for st in T.stages:
@@ -505,6 +508,8 @@ class Solver2D:
             a.g, a.h_cfl = self.cfg.g, self._h_cfl()
             L.call("gsw_lam_cells", C.byref(a), s)
         self.diagnostics["rhs_calls"] += 1
+
+    _counting = 0
 
     def _dt_params(self, t_end, dt_max=None, max_steps=0, fixed_dt=None):
         T = self._tables()
@@ -590,9 +595,11 @@ class Solver2D:
         self._write_state()
         p = self._dt_params(t_end=math.inf, fixed_dt=dt)
         s = _stream()
+        self._counting = 0
         L.call("gsw_dt_finalize", C.byref(p), _ptr(self._state), s)
         self._launch_step(self._cur, T)
         L.call("gsw_loop_commit", _ptr(self._state), s)
+        self.kernel_launches += self._counting + 2
         self._cur = 1 - self._cur
         self._stepped = True
         self.t += dt
@@ -660,14 +667,16 @@ class Solver2D:
 
         def one_window():
             s = _stream()
+            self._counting = 0
             for k in range(K):
                 L.call("gsw_dt_finalize", C.byref(p), _ptr(self._state), s)
+                self._counting += 1
                 self._launch_step((start_cur + k) % 2, T)
+            return self._counting
 
         if self._use_graphs:
             key = (K, start_cur, float(t_end), None if dt_max is None else float(dt_max), int(max_steps))
-            g = self._graph_cache.get(key)
-            if g is None:
+            if key not in self._graph_cache:
                 self._graph_cache.clear()
                 side = torch.cuda.Stream(device=self.device)
                 side.wait_stream(torch.cuda.current_stream())
@@ -675,18 +684,24 @@ class Solver2D:
                 # capture on a side stream; the captured kernels read `done` first, so a
                 # replay after the loop has finished is a no-op
                 with torch.cuda.graph(g, stream=side):
-                    one_window()
+                    per = one_window()
                 torch.cuda.current_stream().wait_stream(side)
-                self._graph_cache[key] = g
-            run_window = g.replay
+                self._graph_cache[key] = (g, per)
+            g, per = self._graph_cache[key]
+
+            def run_window():
+                g.replay()
+                return per
         else:
             run_window = one_window
+        self.kernel_launches += 1            # the initial wave-speed pass
         while True:
-            run_window()
+            self.kernel_launches += run_window()
             st = self._read_state()
             if st.done:
                 break
         L.call("gsw_loop_commit", _ptr(self._state), _stream())
+        self.kernel_launches += 1
         st = self._read_state()
         steps = int(st.steps)
         self._cur = (start_cur + steps) % 2

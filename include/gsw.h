@@ -176,7 +176,7 @@ GSW_API int gsw_dense_rhs(const GswDenseArgs* a, void* stream);
 GSW_API int gsw_dense_lammax(const GswDenseArgs* a, uint64_t* lam_bits, void* stream);
 
 /* Ghost fill of one dense state. kinds[4] = x-, x+, y-, y+ (GSW_BC_*).
- * Writes the non-corner ghost cells (the stencil reads no corner).
+ * Writes every ghost cell; corners come out as apply_bc_2d's x-then-y passes leave them.
  * Replaces apply_bc_2d / apply_bc_2d_face (geoswe/bc.py:50-172). */
 typedef struct GswBcArgs {
     uint32_t abi_version;

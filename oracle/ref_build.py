@@ -1,0 +1,152 @@
+"""Compile the reference's own dense-step CUDA kernels for sm_100a -- TEST INFRASTRUCTURE.
+
+    python oracle/ref_build.py [--ref /root/reference/src]
+
+The reference keeps its GPU kernels as CUDA C text inside Python and assembles the
+production variants at import (geoswe/rhs_cuda.py:1698-2192, geoswe/solver.py:152-205).
+This recipe imports the reference package with a recording stand-in for CuPy, so the
+exact text the reference would hand to NVRTC is captured, and compiles it with nvcc:
+
+  oracle/_ref/ref_kernels.cu          the captured reference text + C launch wrappers
+  oracle/_ref/libref_fma.so           nvcc defaults (FMA contraction on, as NVRTC)
+  oracle/_ref/libref_strict.so        --fmad=false (every operation rounded separately)
+
+oracle/_ref/ is git-ignored (the reference's source is not committed) but travels to
+the GPU box with the other built libraries; oracle/ref_runner.py drives the kernels
+there as the reference's dense solver does. Nothing in the product uses them.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+
+
+class _Recorded:
+    def __init__(self, code=None, name=None, options=()):
+        self.code, self.name, self.options = code, name, tuple(options)
+
+    def __call__(self, *a, **k):
+        raise RuntimeError("recorded kernel: not runnable on the build host")
+
+
+def _fake_cupy():
+    cp = types.ModuleType("cupy")
+    for n in dir(np):
+        if not n.startswith("__"):
+            try:
+                setattr(cp, n, getattr(np, n))
+            except Exception:
+                pass
+    cp.ndarray = np.ndarray
+    cp.asnumpy = lambda a: np.asarray(a)
+    cp.RawKernel = lambda code, name, options=(), **k: _Recorded(code, name, options)
+    cp.RawModule = lambda code=None, options=(), **k: _Recorded(code, "module", options)
+    cp.ElementwiseKernel = lambda *a, **k: _Recorded(None, k.get("name", "elementwise"))
+    cp.ReductionKernel = lambda *a, **k: _Recorded(None, "reduction")
+    cp.get_default_memory_pool = lambda: types.SimpleNamespace(free_all_blocks=lambda: None)
+    cuda = types.ModuleType("cupy.cuda")
+    cuda.runtime = types.SimpleNamespace(getDeviceCount=lambda: 1, is_hip=False,
+                                         memGetInfo=lambda: (0, 0))
+    cuda.Device = lambda *a: types.SimpleNamespace(compute_capability="100", id=0)
+    cp.cuda = cuda
+    sys.modules["cupy"] = cp
+    sys.modules["cupy.cuda"] = cuda
+    return cp
+
+
+def capture(ref_src):
+    """Return {kernel_name: source} of the production dense kernels of the reference."""
+    os.environ["GEOSWE_BACKEND"] = "cupy"
+    for k in ("SWE_DENSE_XY", "SWE_BED_GRAD_LIMITER", "SWE_DRY_SKIP", "SWE_WETDRY_ZERO_H",
+              "SWE_DENSE_MAXRREG"):
+        os.environ.pop(k, None)
+    _fake_cupy()
+    sys.path.insert(0, str(ref_src))
+    from geoswe import rhs_cuda as R
+    from geoswe import solver as S
+    k2d = R.build_dense_fstep2d_kernel(True, 1)                         # no sigma, keep-h
+    kres = R._build_srm_hllc_ns("float", "fused_rhs_wb_srm_hllc_2d_ns_fp32")
+    kres64 = R._build_srm_hllc_ns("double", "fused_rhs_wb_srm_hllc_2d_ns_fp64")
+    return {k2d.name: k2d.code, kres.name: kres.code, kres64.name: kres64.code,
+            "lammax_fp32_lean": S._CFL_LAMMAX_SRC_LEAN}
+
+
+# C launch wrappers around the captured kernels (signatures of the reference text:
+# rhs_cuda.py:900-914 + 2159-2162 for the 2-D fused step, solver.py:152-165 for lammax).
+_WRAPPERS = r"""
+#include <cuda_runtime.h>
+extern "C" int ref_fstep2d(const float* q0, const float* q1, const float* q2, const float* b,
+    float* qn0, float* qn1, float* qn2, int nxp, int nyp, float inv_dx, float inv_dy, float g,
+    float h_min, const float* rain, int have_rain, const unsigned char* n_cls, const float* n_tab,
+    const float* n_field, int use_tab, float* max_h, int have_max, int ngh, float dt, float vcap,
+    int use_quadratic, const unsigned char* dummy_mask, const float* dummy_sigma, void* stream) {
+    dim3 block(16, 16), grid((nxp + 15) / 16, (nyp + 15) / 16);
+    fused_rhs_wb_srm_hllc_fstep2d_ns_fp32<<<grid, block, 0, (cudaStream_t)stream>>>(
+        q0, q1, q2, dummy_sigma, b, qn0, qn1, qn2, nxp, nyp, inv_dx, inv_dy, g, h_min,
+        dummy_mask, 0, qn0, qn1, qn2, rain, have_rain, n_field, n_cls, n_tab, use_tab,
+        max_h, have_max, ngh, dt, vcap, use_quadratic);
+    return (int)cudaGetLastError();
+}
+extern "C" int ref_rhs_f32(const float* q0, const float* q1, const float* q2, const float* b,
+    float* r0, float* r1, float* r2, int nxp, int nyp, float inv_dx, float inv_dy, float g,
+    float h_min, const unsigned char* mask, const float* dummy_sigma, void* stream) {
+    dim3 block(16, 16), grid((nxp + 15) / 16, (nyp + 15) / 16);
+    fused_rhs_wb_srm_hllc_2d_ns_fp32<<<grid, block, 0, (cudaStream_t)stream>>>(
+        q0, q1, q2, dummy_sigma, b, r0, r1, r2, nxp, nyp, inv_dx, inv_dy, g, h_min, mask);
+    return (int)cudaGetLastError();
+}
+extern "C" int ref_rhs_f64(const double* q0, const double* q1, const double* q2, const double* b,
+    double* r0, double* r1, double* r2, int nxp, int nyp, double inv_dx, double inv_dy, double g,
+    double h_min, const unsigned char* mask, const double* dummy_sigma, void* stream) {
+    dim3 block(16, 16), grid((nxp + 15) / 16, (nyp + 15) / 16);
+    fused_rhs_wb_srm_hllc_2d_ns_fp64<<<grid, block, 0, (cudaStream_t)stream>>>(
+        q0, q1, q2, dummy_sigma, b, r0, r1, r2, nxp, nyp, inv_dx, inv_dy, g, h_min, mask);
+    return (int)cudaGetLastError();
+}
+extern "C" int ref_lammax(const float* q0, const float* q1, const float* q2, int nx, int ny,
+    int nyp, int ngh, float g, float h_cfl, unsigned int* out_bits, const unsigned char* ghost,
+    void* stream) {
+    const int N = nx * ny;
+    int grid = (N + 255) / 256; if (grid > 2048) grid = 2048;
+    lammax_fp32_lean<<<grid, 256, 0, (cudaStream_t)stream>>>(q0, q1, q2, N, nx, ny, nyp, ngh, g,
+                                                               h_cfl, out_bits, ghost);
+    return (int)cudaGetLastError();
+}
+"""
+
+
+def build(ref_src="/root/reference/src"):
+    if not Path(ref_src).exists():
+        raise FileNotFoundError(f"reference tree {ref_src} not found (the recipe runs where it is)")
+    srcs = capture(ref_src)
+    OUT.mkdir(exist_ok=True)
+    parts = []
+    for name, code in srcs.items():
+        parts.append(f"// ---- {name} (captured from the reference) ----\n")
+        # each captured text defines its own macros (WETDRY_KEEP_H); keep them per kernel
+        parts.append(code)
+        parts.append("\n#undef WETDRY_KEEP_H\n#undef BSIZE\n")
+    cu = OUT / "ref_kernels.cu"
+    cu.write_text("".join(parts) + _WRAPPERS)
+    nvcc = "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc"
+    for tag, extra in (("fma", []), ("strict", ["--fmad=false"])):
+        out = OUT / f"libref_{tag}.so"
+        subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", *extra,
+                        "-Xcompiler", "-fPIC", "-shared", "-o", str(out), str(cu)], check=True)
+    return OUT
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference/src")
+    a = ap.parse_args()
+    print(build(a.ref))

@@ -1,0 +1,177 @@
+"""The reference's dense GPU solver loop on its own kernels -- TEST INFRASTRUCTURE ONLY.
+
+Drives oracle/_ref/libref_{fma,strict}.so (the reference's kernel text compiled by
+oracle/ref_build.py) the way the reference's Solver2D drives them on CuPy:
+apply_bc_2d (geoswe/bc.py:50-172) -> 2-D fused step (rhs_cuda.py:2151-2192, launched
+as solver.py:2283-2296) -> swap -> t += dt, with cfl_dt from lammax_fp32_lean and the
+host fp64 arithmetic of solver.py:2569-2666 and the run loop of solver.py:2975-3027.
+Uniform rain is given to the fused kernel as a constant frame, which the reference
+itself checks equals the uniform-rain split path bit for bit.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF = HERE / "_ref"
+
+
+def available(variant="fma"):
+    return (REF / f"libref_{variant}.so").exists()
+
+
+def _lib(variant):
+    L = C.CDLL(str(REF / f"libref_{variant}.so"))
+    for n in ("ref_fstep2d", "ref_rhs_f32", "ref_rhs_f64", "ref_lammax"):
+        getattr(L, n).restype = C.c_int
+    return L
+
+
+def _p(t):
+    return C.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _stream():
+    import torch
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def ref_residual(q_pad, b_pad, dx, dy, g, h_min, variant="fma", mask=None):
+    """Residual of the reference's 2-D SRM-HLLC kernel on a padded state (numpy in/out)."""
+    import torch
+    L = _lib(variant)
+    dt = q_pad.dtype
+    q = torch.from_numpy(np.ascontiguousarray(q_pad)).cuda()
+    b = torch.from_numpy(np.ascontiguousarray(b_pad, dtype=dt)).cuda()
+    r = torch.zeros_like(q)
+    m = torch.from_numpy(np.ascontiguousarray(mask if mask is not None else
+                                              np.ones(q_pad.shape[1:], np.uint8))).cuda()
+    sig = torch.zeros(1, dtype=q.dtype, device="cuda")
+    nxp, nyp = q_pad.shape[1:]
+    if dt == np.float32:
+        rc = L.ref_rhs_f32(_p(q[0]), _p(q[1]), _p(q[2]), _p(b), _p(r[0]), _p(r[1]), _p(r[2]), nxp, nyp,
+                           C.c_float(1.0 / dx), C.c_float(1.0 / dy), C.c_float(g), C.c_float(h_min),
+                           _p(m), _p(sig), _stream())
+    else:
+        rc = L.ref_rhs_f64(_p(q[0]), _p(q[1]), _p(q[2]), _p(b), _p(r[0]), _p(r[1]), _p(r[2]), nxp, nyp,
+                           C.c_double(1.0 / dx), C.c_double(1.0 / dy), C.c_double(g), C.c_double(h_min),
+                           _p(m), _p(sig), _stream())
+    assert rc == 0, rc
+    torch.cuda.synchronize()
+    return r.cpu().numpy()
+
+
+class RefDenseGPU:
+    """fp32 dense run of the reference GPU path (its fused 2-D step kernel)."""
+
+    def __init__(self, q_pad, b_pad, ngh, dx, dy, *, kinds=("extrapolate",) * 4, g=9.81, h_min=1e-6,
+                 h_min_cfl=0.0, cfl=0.5, ncls=None, ntab=None, friction=False, vcap=15.0, quad=True,
+                 rain_rate=None, variant="fma"):
+        import torch
+        self.L = _lib(variant)
+        self.q = torch.from_numpy(np.ascontiguousarray(q_pad, dtype=np.float32)).cuda()
+        self.qn = self.q.clone()
+        self.b = torch.from_numpy(np.ascontiguousarray(b_pad, dtype=np.float32)).cuda()
+        self.ngh, self.dx, self.dy, self.g, self.h_min, self.cfl = ngh, dx, dy, g, h_min, cfl
+        hc = h_min_cfl if h_min_cfl > 0.0 else h_min
+        self.h_cfl = max(hc, 1.0e-6)
+        self.kinds = list(kinds)
+        self.nxp, self.nyp = q_pad.shape[1:]
+        nx, ny = self.nxp - 2 * ngh, self.nyp - 2 * ngh
+        self.friction = friction
+        if ncls is None:
+            # friction off: the fused kernel always applies its friction block, so give it
+            # n = 0 (alpha = 1 exactly while |U| stays under the velocity cap)
+            ncls, ntab = np.zeros((self.nxp, self.nyp), np.uint8), [0.0]
+        self.ncls = torch.from_numpy(np.ascontiguousarray(ncls, np.uint8)).cuda()
+        self.ntab = torch.from_numpy(np.asarray(ntab, np.float32)).cuda()
+        self.vcap, self.quad = vcap, quad
+        self.rain_rate = rain_rate
+        self.rain = None if rain_rate is None else torch.full((nx, ny), float(np.float32(rain_rate)),
+                                                              dtype=torch.float32, device="cuda")
+        self.max_h = torch.zeros((self.nxp, self.nyp), dtype=torch.float32, device="cuda")
+        self.bits = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self.ghost = torch.zeros(nx * ny, dtype=torch.uint8, device="cuda")
+        self.dmask = torch.zeros(1, dtype=torch.uint8, device="cuda")
+        self.dsig = torch.zeros(1, dtype=torch.float32, device="cuda")
+        self.dfl = torch.zeros(1, dtype=torch.float32, device="cuda")
+        self.t = 0.0
+        self.nsteps = 0
+
+    def apply_bc(self):
+        q, n = self.q, self.ngh
+        for face, kind in zip(("x-", "x+", "y-", "y+"), self.kinds):
+            ax = 1 if face[0] == "x" else 2
+            lo = face[1] == "-"
+            N = q.shape[ax]
+            for k in range(n):
+                g = k if lo else N - 1 - k
+                if kind == "extrapolate":
+                    s = n if lo else N - n - 1
+                elif kind == "wall":
+                    s = 2 * n - 1 - k if lo else N - 2 * n + k
+                elif kind == "periodic":
+                    s = N - 2 * n + k if lo else 2 * n - 1 - k
+                else:
+                    s = None
+                dst = q[:, g, :] if ax == 1 else q[:, :, g]
+                if kind == "fall":
+                    dst.zero_()
+                    continue
+                src = q[:, s, :] if ax == 1 else q[:, :, s]
+                dst.copy_(src)
+                if kind == "wall":
+                    dst[ax].neg_()
+
+    def cfl_dt(self):
+        nx, ny = self.nxp - 2 * self.ngh, self.nyp - 2 * self.ngh
+        self.bits.zero_()
+        rc = self.L.ref_lammax(_p(self.q[0]), _p(self.q[1]), _p(self.q[2]), nx, ny, self.nyp, self.ngh,
+                               C.c_float(self.g), C.c_float(self.h_cfl), _p(self.bits), _p(self.ghost), _stream())
+        assert rc == 0
+        lam = float(self.bits.cpu().numpy().view(np.float32)[0])
+        if not math.isfinite(lam):
+            raise FloatingPointError("non-finite max wave speed")
+        floor = (self.g * self.h_cfl) ** 0.5
+        if lam < floor:
+            lam = floor
+        return self.cfl * min(self.dx, self.dy) / (lam + 1.0e-12)
+
+    def rain_step_limit(self, dt):
+        if self.rain_rate is None or self.rain_rate <= 0.0:
+            return dt
+        dmin = min(self.dx, self.dy)
+        return min(dt, (self.cfl * dmin) ** (2.0 / 3.0) / (self.g * float(self.rain_rate)) ** (1.0 / 3.0))
+
+    def step(self, dt):
+        self.apply_bc()
+        use_tab = 1 if self.ncls is not None else 0
+        rc = self.L.ref_fstep2d(
+            _p(self.q[0]), _p(self.q[1]), _p(self.q[2]), _p(self.b), _p(self.qn[0]), _p(self.qn[1]),
+            _p(self.qn[2]), self.nxp, self.nyp, C.c_float(1.0 / self.dx), C.c_float(1.0 / self.dy),
+            C.c_float(self.g), C.c_float(self.h_min), _p(self.rain if self.rain is not None else self.dfl),
+            1 if self.rain is not None else 0, _p(self.ncls if self.ncls is not None else self.dmask),
+            _p(self.ntab if self.ntab is not None else self.dfl), _p(self.dfl), use_tab, _p(self.max_h), 1,
+            self.ngh, C.c_float(dt), C.c_float(self.vcap), int(self.quad), _p(self.dmask), _p(self.dsig),
+            _stream())
+        assert rc == 0, rc
+        self.q, self.qn = self.qn, self.q
+        self.t += dt
+        self.nsteps += 1
+        return dt
+
+    def run(self, t_end, max_steps=10 ** 7, dt_max=None):
+        steps = 0
+        while self.t < t_end - 1.0e-12 and steps < max_steps:
+            dt = self.rain_step_limit(self.cfl_dt())
+            if dt_max is not None and dt > dt_max:
+                dt = dt_max
+            if self.t + dt > t_end:
+                dt = t_end - self.t
+            self.step(dt)
+            steps += 1
+        return steps
