@@ -138,6 +138,13 @@ def run_gsw(args, rank, world):
     # ---------------- device-resident throughput (value) ----------------
     s = make_solver(z, cls, n)
     s.run(t_end=1e12, max_steps=args.warmup)
+    tune = None
+    if not args.no_tune:
+        from geoswe_b200 import autotune
+        best, table = autotune.tune_dense(s, reps=4)
+        s._tile_rows, s._warps, s._min_blocks = best["tile_rows"], best["warps"], best["min_blocks"]
+        s._graph_cache.clear()
+        tune = {"best": best, "table": table}
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -156,6 +163,7 @@ def run_gsw(args, rank, world):
     assert steps == args.steps, (steps, args.steps)
     # ---------------- dominant kernel alone (roofline) ----------------
     kern_ms = time_step_kernel(s, reps=args.kernel_reps)
+    shape = {"tile_rows": s._tile_rows or 32, "warps": s._warps or 4, "min_blocks": s._min_blocks}
     # ---------------- end to end through the public API ----------------
     e2e = run_e2e(args, z, cls, n)
     del s
@@ -183,36 +191,21 @@ def run_gsw(args, rank, world):
                      "kernel": "dense_march_kernel<float,true>", "kernel_ms": kern_ms,
                      "bytes_per_cell": bpc, "peak_source": peak_kind},
         "clocks": clocks,
+        "launch_shape": shape,
     }
+    if tune is not None:
+        out["autotune"] = tune
     if rank == 0 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
 
 
 def time_step_kernel(s, reps=20):
-    """Average duration of the fused dense step kernel alone (CUDA events on its stream)."""
-    import ctypes as C
-    import torch
-    from geoswe_b200 import _lib as L
-    from geoswe_b200.solver import _ptr, _stream
-    T = s._tables()
-    st = L.GswLoopState()
-    st.t = s.t
-    st.dt = s.last_dt
-    st.dt_f32 = float(np.float32(s.last_dt))
-    s._state_host.copy_(torch.frombuffer(bytearray(bytes(st) + bytes(128 - C.sizeof(st))), dtype=torch.uint8))
-    s._state.copy_(s._state_host)
-    args = [s._dense_args(s._buf[k], s._buf[1 - k], T) for k in (0, 1)]
-    for k in range(4):
-        L.call("gsw_dense_step", C.byref(args[k % 2]), _stream())
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for k in range(reps):
-        L.call("gsw_dense_step", C.byref(args[k % 2]), _stream())
-    e1.record()
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) / reps
+    """Average duration of the fused dense step kernel alone (CUDA events on its stream),
+    on scratch copies of the state the timed run ended in, with the solver's launch shape."""
+    from geoswe_b200.autotune import time_dense_step
+    return time_dense_step(s, reps=reps, tile_rows=s._tile_rows, warps=s._warps,
+                           min_blocks=s._min_blocks, dt=s.last_dt)
 
 
 def run_e2e(args, z, cls, n):
@@ -258,6 +251,7 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=512)
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

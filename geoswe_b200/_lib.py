@@ -40,7 +40,7 @@ class GswDtParams(C.Structure):
     _fields_ = [("abi_version", u32), ("mode", i32), ("cfl_dmin", f64), ("lam_floor", f64),
                 ("t_end", f64), ("eps_end", f64), ("dt_max", f64), ("fixed_dt", f64),
                 ("max_steps", i64), ("rain_t", vp), ("rain_lim", vp), ("n_rain", i32),
-                ("reserved", i32)]
+                ("clip_flat", i32)]
 
 
 class GswDenseArgs(C.Structure):
@@ -53,7 +53,7 @@ class GswDenseArgs(C.Structure):
                 ("friction_kind", i32), ("n_cls", vp), ("n_cls_pitch", i64), ("n_tab", vp),
                 ("n_tab_len", i32), ("n_field", vp), ("vcap", f64), ("quadratic", i32),
                 ("keep_h", i32), ("max_h", vp), ("cfl_skip", vp), ("h_cfl", f64),
-                ("tile_rows", i32), ("warps", i32)]
+                ("tile_rows", i32), ("warps", i32), ("min_blocks", i32), ("reserved", i32)]
 
 
 class GswBcArgs(C.Structure):
@@ -76,7 +76,18 @@ class GswInflowArgs(C.Structure):
                 ("t_knots", vp), ("q_knots", vp), ("n_knots", i32), ("state", vp)]
 
 
-# entry point -> (argtypes, doc)
+class GswFlatArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("brick_h", i32), ("n_bricks", i64),
+                ("brick_ij", vp), ("brick_nbr", vp), ("flags", vp),
+                ("q0", vp), ("q1", vp), ("q2", vp), ("qn0", vp), ("qn1", vp), ("qn2", vp), ("bed", vp),
+                ("inv_dx", C.c_float), ("inv_dy", C.c_float), ("g", C.c_float), ("h_min", C.c_float),
+                ("h_min_cfl", C.c_float), ("linf", i32), ("state", vp), ("lam_target", vp),
+                ("rain_kind", i32), ("rain", vp), ("ngh", i32), ("nx", i32), ("ny", i32),
+                ("n_cls", vp), ("n_tab", vp), ("n_tab_len", i32), ("vcap", C.c_float),
+                ("quadratic", i32), ("keep_h", i32), ("max_h", vp), ("warps", i32)]
+
+
+# entry point -> argtypes
 _PROTOS = {
     "gsw_dense_step": [C.POINTER(GswDenseArgs), vp],
     "gsw_dense_rhs": [C.POINTER(GswDenseArgs), vp],
@@ -87,6 +98,12 @@ _PROTOS = {
     "gsw_inflow_apply": [C.POINTER(GswInflowArgs), vp],
     "gsw_dt_finalize": [C.POINTER(GswDtParams), vp, vp],
     "gsw_loop_commit": [vp, vp],
+    "gsw_flat_step": [C.POINTER(GswFlatArgs), vp],
+    "gsw_flat_rhs": [C.POINTER(GswFlatArgs), vp],
+    "gsw_flat_lammax": [C.POINTER(GswFlatArgs), vp, vp],
+    "gsw_mesh_count": [vp, C.c_int, C.c_int, C.c_int, vp, vp],
+    "gsw_mesh_build": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp],
+    "gsw_bricks_build": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp],
 }
 
 

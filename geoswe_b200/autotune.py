@@ -1,0 +1,120 @@
+"""Launch-shape autotuner for the fused step kernels.
+
+The dense step's speed depends on the rows a warp walks (tile_rows), the warps per
+block and the register cap (occupancy against spills); the best point depends on the
+device and on how wet the grid is. `tune_dense` times each candidate with CUDA events
+on scratch copies of a solver's current state (the solver itself is not advanced) and
+caches the winner as JSON keyed by device name, driver version and grid size class.
+
+Cache: $GSW_TUNE_CACHE, else ~/.cache/geoswe_b200/autotune.json.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import itertools
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+DENSE_SPACE = dict(tile_rows=(16, 32, 64), warps=(2, 4, 8), min_blocks=(0, 4, 5))
+
+
+def _cache_path() -> Path:
+    p = os.environ.get("GSW_TUNE_CACHE")
+    return Path(p) if p else Path.home() / ".cache" / "geoswe_b200" / "autotune.json"
+
+
+def _key(kind, cells):
+    dev = torch.cuda.get_device_name()
+    drv = torch.version.cuda or ""
+    try:
+        import ctypes
+        v = ctypes.c_int()
+        ctypes.CDLL("libcuda.so.1").cuDriverGetVersion(ctypes.byref(v))
+        drv = str(v.value)
+    except Exception:
+        pass
+    size = "small" if cells < 1 << 20 else ("medium" if cells < 1 << 24 else "large")
+    return f"{kind}|{dev}|{drv}|{size}"
+
+
+def load(kind, cells):
+    p = _cache_path()
+    if not p.exists():
+        return None
+    try:
+        return json.loads(p.read_text()).get(_key(kind, cells))
+    except Exception:
+        return None
+
+
+def _store(kind, cells, entry):
+    p = _cache_path()
+    p.parent.mkdir(parents=True, exist_ok=True)
+    data = {}
+    if p.exists():
+        try:
+            data = json.loads(p.read_text())
+        except Exception:
+            data = {}
+    data[_key(kind, cells)] = entry
+    tmp = p.with_suffix(".tmp")
+    tmp.write_text(json.dumps(data, indent=1))
+    tmp.replace(p)
+
+
+def time_dense_step(s, reps=10, tile_rows=0, warps=0, min_blocks=0, dt=None):
+    """Mean duration (ms) of one fused dense step launch of solver `s` on scratch copies
+    of its current state."""
+    from .solver import _ptr, _stream
+    T = s._tables()
+    if dt is None:
+        dt = s.cfl_dt()
+    st = L.GswLoopState()
+    st.t = s.t
+    st.dt = float(dt)
+    st.dt_f32 = float(np.float32(dt))
+    state = torch.zeros(128, dtype=torch.uint8, device=s.device)
+    state.copy_(torch.frombuffer(bytearray(bytes(st) + bytes(128 - C.sizeof(st))), dtype=torch.uint8))
+    bufs = [s._buf[s._cur].clone(), torch.empty_like(s._buf[s._cur])]
+    maxh = None if s._max_h is None else s._max_h.clone()
+    args = []
+    for k in (0, 1):
+        a = s._dense_args(bufs[k], bufs[1 - k], T)
+        a.state = _ptr(state)
+        a.lam_target = C.c_void_p(state.data_ptr() + L.GswLoopState.lam_bits.offset)
+        a.max_h = _ptr(maxh)
+        a.tile_rows, a.warps, a.min_blocks = int(tile_rows), int(warps), int(min_blocks)
+        args.append(a)
+    for k in range(2):
+        L.call("gsw_dense_step", C.byref(args[k % 2]), _stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(reps):
+        L.call("gsw_dense_step", C.byref(args[k % 2]), _stream())
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def tune_dense(s, reps=8, space=None, store=True, verbose=False):
+    """Time every launch shape of `space` on solver `s`; return (best, table) and cache
+    the best for this device and size class."""
+    space = space or DENSE_SPACE
+    dt = s.cfl_dt()
+    table = []
+    for tr, w, mb in itertools.product(space["tile_rows"], space["warps"], space["min_blocks"]):
+        ms = time_dense_step(s, reps=reps, tile_rows=tr, warps=w, min_blocks=mb, dt=dt)
+        table.append(dict(tile_rows=tr, warps=w, min_blocks=mb, ms=ms))
+        if verbose:
+            print(f"  tile_rows={tr:3d} warps={w} min_blocks={mb}: {ms:.4f} ms", flush=True)
+    best = min(table, key=lambda e: e["ms"])
+    cells = s.mesh.nx * s.mesh.ny
+    if store:
+        _store("dense", cells, best)
+    return best, table

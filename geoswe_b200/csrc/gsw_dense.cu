@@ -89,8 +89,8 @@ template <> __device__ __forceinline__ float  dt_of<float>(const GswLoopState* s
 template <> __device__ __forceinline__ double dt_of<double>(const GswLoopState* st) { return st->dt; }
 
 // STEP = false: residual into o0..o2. STEP = true: updated state into o0..o2.
-template <typename T, bool STEP>
-__global__ void __launch_bounds__(256) dense_march_kernel(DenseK<T> p) {
+template <typename T, bool STEP, int MINB>
+__global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
     if (STEP && p.st->done) return;                       // grid-uniform
     const int lane = threadIdx.x;
     const int strip = blockIdx.x * blockDim.y + threadIdx.y;
@@ -122,6 +122,11 @@ __global__ void __launch_bounds__(256) dense_march_kernel(DenseK<T> p) {
         load_cell(p, nx, i0, cl);
         nx.b = ldg_at(p.b, p.pitch, i0, cl);
         T b_next = ldg_at(p.b, p.pitch, i0 + 1, cl);
+        // prefetch of the row after next: its loads are in flight during this row's faces
+        T pf_h = ldg_at(p.q0, p.pitch, i0 + 1, cl);
+        T pf_hu = ldg_at(p.q1, p.pitch, i0 + 1, cl);
+        T pf_hv = ldg_at(p.q2, p.pitch, i0 + 1, cl);
+        T pf_b = ldg_at(p.b, p.pitch, i0 + 2, cl);
         make_prims(cur, p.h_min);
         make_prims(nx, p.h_min);
         cur.gx = (T)0.5 * (nx.b - b_m2) * p.inv_dx;
@@ -133,9 +138,15 @@ __global__ void __launch_bounds__(256) dense_march_kernel(DenseK<T> p) {
         cur = nx;
 
         for (int r = i0; r < i1; ++r) {
-            load_cell(p, nx, r + 1, cl);
+            nx.h = pf_h; nx.hu = pf_hu; nx.hv = pf_hv;
             nx.b = b_next;
-            const T b_p2 = ldg_at(p.b, p.pitch, r + 2, cl);
+            const T b_p2 = pf_b;
+            if (r + 1 < i1) {           // rows r+2 / r+3 exist: the strip ends at i1 <= nxp - lo
+                pf_h = ldg_at(p.q0, p.pitch, r + 2, cl);
+                pf_hu = ldg_at(p.q1, p.pitch, r + 2, cl);
+                pf_hv = ldg_at(p.q2, p.pitch, r + 2, cl);
+                pf_b = ldg_at(p.b, p.pitch, r + 3, cl);
+            }
             make_prims(nx, p.h_min);
             nx.gx = (T)0.5 * (b_p2 - cur.b) * p.inv_dx;
             nx.gy = grad_y(p, nx.b, r + 1, c, lane);
@@ -392,13 +403,17 @@ static int launch_march(const GswDenseArgs* a, cudaStream_t s) {
     int rc = fill_dense<T>(a, k, STEP);
     if (rc) return rc;
     const int W = a->warps > 0 ? a->warps : 4;
+    const int minb = a->min_blocks;
+    if (minb != 0 && minb != 4 && minb != 5) return set_error(GSW_ERR_INVALID, "dense: min_blocks must be 0, 4 or 5");
     if (W < 1 || W > 8) return set_error(GSW_ERR_INVALID, "dense: warps must be in [1, 8]");
     const int ncols = k.nyp - 2 * k.lo, nrows = k.nxp - 2 * k.lo;
     const int strips = (ncols + 29) / 30;
     dim3 block(32, W);
     dim3 grid((strips + W - 1) / W, (nrows + k.tile_rows - 1) / k.tile_rows);
     if (grid.y > 65535u) return set_error(GSW_ERR_INVALID, "dense: too many row tiles (%u); raise tile_rows", grid.y);
-    dense_march_kernel<T, STEP><<<grid, block, 0, s>>>(k);
+    if (minb == 0) dense_march_kernel<T, STEP, 1><<<grid, block, 0, s>>>(k);
+    else if (minb == 4) dense_march_kernel<T, STEP, 4><<<grid, block, 0, s>>>(k);
+    else dense_march_kernel<T, STEP, 5><<<grid, block, 0, s>>>(k);
     return check_launch("dense_march");
 }
 

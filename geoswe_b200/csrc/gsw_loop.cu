@@ -97,7 +97,12 @@ __global__ void dt_finalize_kernel(GswDtParams p, GswLoopState* s) {
         if (p.rain_lim != nullptr && p.rain_lim[idx] > 0.0 && p.rain_lim[idx] < dt) dt = p.rain_lim[idx];
         if (p.dt_max > 0.0 && dt > p.dt_max) dt = p.dt_max;
     }
-    if (__dadd_rn(t, dt) > p.t_end) dt = __dsub_rn(p.t_end, t);
+    if (p.clip_flat) {
+        const double rem = __dsub_rn(p.t_end, t);
+        if (rem < dt) dt = rem;
+    } else if (__dadd_rn(t, dt) > p.t_end) {
+        dt = __dsub_rn(p.t_end, t);
+    }
     s->dt = dt;
     s->dt_f32 = (float)dt;
     s->t_new = __dadd_rn(t, dt);

@@ -59,7 +59,7 @@ class Solver2D:
 
     def __init__(self, mesh: Mesh2D, cfg: Config, q0, b, comm=None, dims=None, *,
                  device=None, track_max_depth: bool = True, use_graphs: bool = True,
-                 tile_rows: int = 0, warps: int = 0):
+                 tile_rows: int = 0, warps: int = 0, min_blocks: int = 0, autotuned: bool = True):
         _require_cuda()
         if comm is not None and getattr(comm, "size", 1) > 1:
             raise NotImplementedError("Solver2D: multi-rank runs are not part of this package "
@@ -103,7 +103,13 @@ class Solver2D:
         self.code = L.F32 if self.np_dtype == np.float32 else L.F64
         self.nxp, self.nyp = mesh.padded_shape
         self.pitch = _pitch(self.nyp, self.np_dtype.itemsize)
-        self._tile_rows, self._warps = int(tile_rows), int(warps)
+        self._tile_rows, self._warps, self._min_blocks = int(tile_rows), int(warps), int(min_blocks)
+        if autotuned and not (tile_rows or warps or min_blocks):
+            from . import autotune
+            best = autotune.load("dense", mesh.nx * mesh.ny)
+            if best and self.np_dtype == np.float32:
+                self._tile_rows, self._warps = int(best["tile_rows"]), int(best["warps"])
+                self._min_blocks = int(best["min_blocks"])
         self._use_graphs = bool(use_graphs)
         dev, td = self.device, self.t_dtype
         self._buf = [torch.zeros((3, self.nxp, self.pitch), dtype=td, device=dev) for _ in range(2)]
@@ -422,7 +428,7 @@ class Solver2D:
         a.inv_dx, a.inv_dy = 1.0 / self.mesh.dx, 1.0 / self.mesh.dy
         a.g, a.h_min = cfg.g, cfg.h_min
         a.h_cfl = self._h_cfl()
-        a.tile_rows, a.warps = self._tile_rows, self._warps
+        a.tile_rows, a.warps, a.min_blocks = self._tile_rows, self._warps, self._min_blocks
         if step:
             T = T or self._tables()
             a.state = _ptr(self._state)
@@ -659,6 +665,8 @@ class Solver2D:
     def _run_device(self, t_end, max_steps, dt_max, window=0):
         T = self._tables()
         K = int(window) if window else self._window_size()
+        if max_steps and max_steps < K:
+            K = int(max_steps)
         K += K % 2
         self._write_state()
         self._lammax_into_state(T.ghost_skip)

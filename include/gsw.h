@@ -122,7 +122,7 @@ typedef struct GswDtParams {
     const double* rain_t;   /* device, n_rain knot times (bisect_right - 1, clamped) or NULL */
     const double* rain_lim; /* device, per-frame rain step limit (<= 0: none) or NULL */
     int32_t  n_rain;
-    int32_t  reserved;
+    int32_t  clip_flat;     /* 0: dense clip (t + dt > t_end -> t_end - t); 1: flat dt = min(dt, t_end - t) */
 } GswDtParams;
 
 /* ------------------------------------------------------------------------- */
@@ -154,8 +154,10 @@ typedef struct GswDenseArgs {
     void*    max_h;            /* running max depth, pitch = pitch, or NULL */
     const uint8_t* cfl_skip;   /* interior (nx, ny) C-order: 1 = excluded from the wave speed */
     double   h_cfl;            /* wave-speed wet threshold (and divisor) */
-    int32_t  tile_rows;        /* rows per warp strip (0: default) */
-    int32_t  warps;            /* warps per block (0: default) */
+    int32_t  tile_rows;        /* rows per warp strip (0: default 32) */
+    int32_t  warps;            /* warps per block (0: default 4) */
+    int32_t  min_blocks;       /* register cap: 0 (compiler's choice), 4 (64 regs) or 5 (51 regs) */
+    int32_t  reserved;
 } GswDenseArgs;
 
 /* One fused step over the interior: SRM-HLLC residual, rain, forward Euler,
@@ -234,6 +236,59 @@ typedef struct GswInflowArgs {
     const GswLoopState* state;  /* Q is taken at state->t (pre-step) */
 } GswInflowArgs;
 GSW_API int gsw_inflow_apply(const GswInflowArgs* a, void* stream);
+
+/* ------------------------------------------------------------------------- */
+/* Compressed (flat) mesh.                                                    */
+/* ------------------------------------------------------------------------- */
+/* Slot flags of the brick storage */
+#define GSW_SLOT_STORED 1u
+#define GSW_SLOT_ACTIVE 2u
+
+typedef struct GswFlatArgs {
+    uint32_t abi_version;
+    int32_t  brick_h;          /* rows per brick (>= 2) */
+    int64_t  n_bricks;         /* brick n_bricks is the all-zero brick (a missing neighbour) */
+    const int32_t* brick_ij;   /* (n_bricks, 2) brick row, brick column */
+    const int32_t* brick_nbr;  /* (n_bricks, 4) up, down, left, right */
+    const uint8_t* flags;      /* per slot: GSW_SLOT_STORED | GSW_SLOT_ACTIVE */
+    const float* q0; const float* q1; const float* q2;   /* state in, slot-indexed */
+    float* qn0; float* qn1; float* qn2;                  /* state out (step) / residual (rhs) */
+    const float* bed;
+    float    inv_dx, inv_dy, g, h_min, h_min_cfl;
+    int32_t  linf;             /* 1: CFL norm max(|u|,|v|); 0: sqrt(u^2+v^2) */
+    /* step only */
+    const GswLoopState* state;
+    uint64_t* lam_target;
+    int32_t  rain_kind;        /* GSW_RAIN_NONE / UNIFORM / GRIDDED */
+    const float* rain;         /* uniform: rates[n_frames]; gridded: frames[n_frames][nx][ny] */
+    int32_t  ngh, nx, ny;      /* dense padding and interior extents (gridded rain index) */
+    const uint8_t* n_cls; const float* n_tab; int32_t n_tab_len;
+    float    vcap;
+    int32_t  quadratic, keep_h;
+    float*   max_h;            /* slot-indexed, or NULL */
+    int32_t  warps;
+} GswFlatArgs;
+
+/* Fused step on the compressed mesh: active cells get the SRM-HLLC residual, rain,
+ * Euler, wet/dry and Manning (table); stored ring cells are carried unchanged.
+ * Replaces the flat fused step + CFL launch (geoswe/compressed_rhs.py:673-865, 990-1118;
+ * geoswe/compressed_solver.py:819-905). Residuals of active cells are bit-identical to
+ * the dense kernel's at the same state. */
+GSW_API int gsw_flat_step(const GswFlatArgs* a, void* stream);
+/* Residual of active cells into qn0..qn2 (0 at ring cells and empty slots). Replaces
+ * CompressedSWE.run_rhs / CompressedStepper.rhs (geoswe/compressed_rhs.py:355-369). */
+GSW_API int gsw_flat_rhs(const GswFlatArgs* a, void* stream);
+/* Wave speed of active cells of the current state into *lam_bits (atomicMax).
+ * Replaces cfl_lammax_flat_blk[_ns] (geoswe/compressed_solver.py:209-244). */
+GSW_API int gsw_flat_lammax(const GswFlatArgs* a, uint64_t* lam_bits, void* stream);
+
+/* Host-side compressed-mesh construction (gsw_mesh.cpp). */
+GSW_API int gsw_mesh_count(const uint8_t* inside, int nxp, int nyp, int ring,
+                           int64_t* n_stored, int64_t* n_active);
+GSW_API int gsw_mesh_build(const uint8_t* inside, int nxp, int nyp, int ring, int32_t* ij,
+                           int16_t* nbr16, uint8_t* is_active, int32_t* active_id, int32_t* covered);
+GSW_API int gsw_bricks_build(const uint8_t* stored, int nxp, int nyp, int brick_h,
+                             int64_t* n_bricks, int32_t* brick_ij, int32_t* brick_nbr);
 
 /* ------------------------------------------------------------------------- */
 /* Loop control.                                                              */

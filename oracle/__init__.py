@@ -307,3 +307,102 @@ class OracleSolver2D:
             self.step(dt)
             steps += 1
         return steps
+
+
+# ---------------------------------------------------------------------------
+# Compressed (flat) mesh: canonical order, int16 delta table (fp32).
+# ---------------------------------------------------------------------------
+def _flat_setup(L):
+    for n in ("gswo_flat_step_f32", "gswo_flat_lammax_f32"):
+        getattr(L, n).restype = C.c_double
+
+
+def flat_rhs(nbr, act, q, b, dx, g, h_min):
+    L = lib()
+    N = len(act)
+    q = [np.ascontiguousarray(x, np.float32) for x in q]
+    r = [np.zeros(N, np.float32) for _ in range(3)]
+    inv = C.c_float(np.float32(1.0 / dx))
+    L.gswo_flat_rhs_f32(C.c_int64(N), _p(np.ascontiguousarray(nbr, np.int16)), _p(np.ascontiguousarray(act, np.uint8)),
+                        _p(q[0]), _p(q[1]), _p(q[2]), _p(np.ascontiguousarray(b, np.float32)), inv, inv,
+                        C.c_float(g), C.c_float(h_min), _p(r[0]), _p(r[1]), _p(r[2]))
+    return np.stack(r)
+
+
+class OracleFlat:
+    """The reference's flat loop (geoswe/compressed_solver.py:713-748, 2133-2235) on the C
+    oracle: canonical flat arrays, int16 neighbour deltas, the fused step's semantics."""
+
+    def __init__(self, nbr, act, q, b, dx, *, g=9.81, h_min=1e-6, h_min_cfl=None, cfl=0.5, linf=False,
+                 ncls=None, ntab=(0.0,), vcap=15.0, quad=True, keep_h=True, rain_times=None,
+                 rain_table=None, rain_lookup=None, dt_max=None):
+        L = lib()
+        _flat_setup(L)
+        self.L = L
+        self.nbr = np.ascontiguousarray(nbr, np.int16)
+        self.act = np.ascontiguousarray(act, np.uint8)
+        self.q = [np.ascontiguousarray(x, np.float32).copy() for x in q]
+        self.b = np.ascontiguousarray(b, np.float32)
+        self.dx, self.g, self.cfl = dx, g, cfl
+        self.h_min = max(h_min, 1e-6)
+        self.h_min_cfl = max(self.h_min if h_min_cfl is None else h_min_cfl, 1e-6)
+        self.linf = int(linf)
+        self.ncls = None if ncls is None else np.ascontiguousarray(ncls, np.uint8)
+        self.ntab = np.asarray(ntab, np.float32)
+        self.vcap, self.quad, self.keep_h = vcap, quad, keep_h
+        self.rain_times = None if rain_times is None else np.asarray(rain_times, np.float64)
+        self.rain_table = None if rain_table is None else np.asarray(rain_table, np.float32)
+        self.rain_lookup = rain_lookup
+        self.dt_max = dt_max
+        if self.rain_table is not None:
+            rmax = float(self.rain_table.max())
+            if rmax > 0.0:
+                lim = (cfl * dx) ** (2.0 / 3.0) / (g * rmax) ** (1.0 / 3.0)
+                self.dt_max = lim if self.dt_max is None else min(self.dt_max, lim)
+        self.max_h = np.zeros(len(self.act), np.float32)
+        self.t = 0.0
+        self.nsteps = 0
+        self._lam = None
+
+    def _lammax(self):
+        q = self.q
+        return float(self.L.gswo_flat_lammax_f32(C.c_int64(len(self.act)), _p(self.act), _p(q[0]), _p(q[1]),
+                                                 _p(q[2]), C.c_float(self.g), C.c_float(self.h_min),
+                                                 C.c_float(self.h_min_cfl), C.c_int(self.linf)))
+
+    def dt_from_lam(self, lam):
+        floor = (self.g * self.h_min) ** 0.5
+        if lam < floor:
+            lam = floor
+        dt = self.cfl * self.dx / (lam + 1e-12)
+        return dt if self.dt_max is None else min(dt, self.dt_max)
+
+    def step(self, dt):
+        rate = None
+        if self.rain_table is not None:
+            it = max(0, min(self.rain_table.shape[0] - 1,
+                            int(np.searchsorted(self.rain_times, self.t, "right") - 1)))
+            rate = np.ascontiguousarray(self.rain_table[it][self.rain_lookup], np.float32)
+        q = self.q
+        qn = [np.empty_like(x) for x in q]
+        inv = C.c_float(np.float32(1.0 / self.dx))
+        lam = self.L.gswo_flat_step_f32(
+            C.c_int64(len(self.act)), _p(self.nbr), _p(self.act), _p(q[0]), _p(q[1]), _p(q[2]), _p(self.b),
+            inv, inv, C.c_float(self.g), C.c_float(self.h_min), C.c_float(self.h_min_cfl), C.c_int(self.linf),
+            C.c_float(np.float32(dt)), _p(rate), _p(self.ncls), _p(self.ntab), C.c_float(self.vcap),
+            C.c_int(int(self.quad)), C.c_int(int(self.keep_h)), _p(qn[0]), _p(qn[1]), _p(qn[2]), _p(self.max_h))
+        self.q = qn
+        self._lam = float(lam)
+        self.t += dt
+        self.nsteps += 1
+
+    def run(self, t_end, max_steps=10 ** 9):
+        steps = 0
+        while self.t < t_end - 1e-9 and steps < max_steps:
+            lam = self._lammax() if self._lam is None else self._lam
+            if not (lam == lam and lam < float("inf")):
+                raise FloatingPointError("non-finite max wave speed")
+            dt = min(self.dt_from_lam(lam), t_end - self.t)
+            self.step(dt)
+            steps += 1
+        return steps

@@ -60,17 +60,14 @@ static inline void SFX(hllc)(R hL, R uNL, R uTL, R sigL, R hR, R uNR, R uTR, R s
     else               { *Fh = FR_h;  *FN = FR_N;  *FT = FR_T; }
 }
 
-/* Residual of one cell (i, j) of a padded row-major field with row pitch P. */
-static void SFX(cell_rhs)(const R* q0, const R* q1, const R* q2, const R* b, int64_t P,
-                          int i, int j, R inv_dx, R inv_dy, R g, R h_min,
-                          R* r0, R* r1, R* r2) {
+/* Residual of one cell from the indices of its 9-point stencil: centre, -i, +i, -2i,
+ * +2i, -j, +j, -2j, +2j (dense: row arithmetic; flat: the neighbour table). */
+static void SFX(cell_rhs_ix)(const R* q0, const R* q1, const R* q2, const R* b,
+                             int64_t idx, int64_t idx_l, int64_t idx_r, int64_t idx_ll, int64_t idx_rr,
+                             int64_t idx_b, int64_t idx_t, int64_t idx_bb, int64_t idx_tt,
+                             R inv_dx, R inv_dy, R g, R h_min, R* r0, R* r1, R* r2) {
     const R dx = (R)1.0 / inv_dx;
     const R dy = (R)1.0 / inv_dy;
-    const int64_t idx = (int64_t)i * P + j;
-    const int64_t idx_l = (int64_t)(i - 1) * P + j, idx_r = (int64_t)(i + 1) * P + j;
-    const int64_t idx_ll = (int64_t)(i - 2) * P + j, idx_rr = (int64_t)(i + 2) * P + j;
-    const int64_t idx_b = (int64_t)i * P + (j - 1), idx_t = (int64_t)i * P + (j + 1);
-    const int64_t idx_bb = (int64_t)i * P + (j - 2), idx_tt = (int64_t)i * P + (j + 2);
     R h_c, u_c, v_c, h_l, u_l, v_l, h_r, u_r, v_r, h_bo, u_bo, v_bo, h_to, u_to, v_to;
 #define PRIMS(II, h, u, v) do { h = q0[II]; { const R _hs = (h > h_min) ? h : h_min; \
         u = (h > h_min) ? q1[II] / _hs : RZ; v = (h > h_min) ? q2[II] / _hs : RZ; } } while (0)
@@ -174,6 +171,16 @@ static void SFX(cell_rhs)(const R* q0, const R* q1, const R* q2, const R* b, int
         rhs_hv += src * inv_dy;
     }
     *r0 = rhs_h; *r1 = rhs_hu; *r2 = rhs_hv;
+}
+
+/* Residual of one cell (i, j) of a padded row-major field with row pitch P. */
+static void SFX(cell_rhs)(const R* q0, const R* q1, const R* q2, const R* b, int64_t P,
+                          int i, int j, R inv_dx, R inv_dy, R g, R h_min,
+                          R* r0, R* r1, R* r2) {
+    SFX(cell_rhs_ix)(q0, q1, q2, b, (int64_t)i * P + j, (int64_t)(i - 1) * P + j, (int64_t)(i + 1) * P + j,
+                     (int64_t)(i - 2) * P + j, (int64_t)(i + 2) * P + j, (int64_t)i * P + (j - 1),
+                     (int64_t)i * P + (j + 1), (int64_t)i * P + (j - 2), (int64_t)i * P + (j + 2),
+                     inv_dx, inv_dy, g, h_min, r0, r1, r2);
 }
 
 /* Wet/dry + friction tail (rhs_cuda.py:1765-1790; friction off: solver.py:2952-2962). */

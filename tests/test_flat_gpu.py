@@ -1,0 +1,109 @@
+"""Compressed (flat) mesh on the GPU: bit-exact against the flat C oracle (which walks
+the reference's int16 neighbour table), and against the dense kernel."""
+import numpy as np
+import pytest
+
+import oracle
+from tests._cases import flowing, same
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _dense(q0, bed, mask, dx=2.0, **cfgkw):
+    from geoswe_b200 import Config, Mesh2D, Solver2D
+    nx, ny = bed.shape
+    kw = dict(bc_x="fall", bc_y="fall")
+    kw.update(cfgkw)
+    s = Solver2D(Mesh2D(nx=nx, ny=ny, dx=dx, dy=dx, ngh=2), Config(**kw), q0, bed)
+    if mask is not None:
+        s.set_inside_mask(mask)
+    return s
+
+
+def _blob_mask(nx, ny, seed=3):
+    from geoswe_b200.synthetic import dilate_cross
+    rng = np.random.default_rng(seed)
+    m = np.zeros((nx, ny), bool)
+    m[rng.integers(4, nx - 4, 12), rng.integers(4, ny - 4, 12)] = True
+    m = dilate_cross(m, 9)
+    m[:3, :] = m[-3:, :] = False
+    m[:, :3] = m[:, -3:] = False
+    return m
+
+
+@pytest.mark.parametrize("bh", [4, 16])
+def test_flat_residual_bitwise_dense_and_oracle(bh):
+    from geoswe_b200.compressed import CompressedSolver
+    q0, bed = flowing(70, 97, seed=12, dtype=np.float32)
+    mask = _blob_mask(70, 97)
+    s = _dense(q0, bed, mask)
+    s.run(t_end=1e9, max_steps=5)                      # a non-trivial fixed state
+    s.apply_bc()
+    r_dense = s.residual().cpu().numpy()
+    cs = CompressedSolver.from_dense(s, brick_h=bh)
+    r_flat = cs.residual().cpu().numpy()
+    act = cs.is_active != 0
+    ij = cs.ij_active
+    for c in range(3):
+        assert same(r_flat[c][act], r_dense[c][ij[act, 0], ij[act, 1]]), c
+    assert np.abs(r_flat[0][act]).max() > 0
+    q = [cs.flat(c).cpu().numpy() for c in range(3)]
+    b = cs._b[cs._slot].cpu().numpy()
+    r_or = oracle.flat_rhs(cs.nbr, cs.is_active, q, b, 2.0, 9.81, 1e-6)
+    assert same(r_flat, r_or)
+
+
+@pytest.mark.parametrize("linf", [False, True])
+def test_flat_run_bitwise_oracle(linf):
+    from geoswe_b200 import RainfallForcing
+    from geoswe_b200.compressed import CompressedSolver
+    from geoswe_b200.synthetic import MANNING_CLASSES, fractal_bed, voronoi_classes
+    nx, ny, dx = 72, 90, 3.0
+    z = fractal_bed(nx, ny, dx, seed=6).astype(np.float32)
+    mask = z < np.percentile(z, 60)
+    mask[:3, :] = mask[-3:, :] = False
+    mask[:, :3] = mask[:, -3:] = False
+    cls = voronoi_classes(nx, ny, n_seeds=16, seed=6)
+    s = _dense(np.zeros((3, nx, ny), np.float32), z, mask, dx=dx, friction="manning")
+    s.set_manning_table(np.pad(cls, 2, mode="edge"), MANNING_CLASSES)
+    cs = CompressedSolver.from_dense(s, cfl_linf=linf)
+    rf = RainfallForcing(time_s=[0.0, 600.0, 1e9], rate_mm_h=[50.0, 20.0, 20.0])
+    cs.set_rain(rf)
+    q = [cs.flat(c).cpu().numpy() for c in range(3)]
+    b = cs._b[cs._slot].cpu().numpy()
+    ncls = cs._ncls[cs._slot].cpu().numpy()
+    o = oracle.OracleFlat(cs.nbr, cs.is_active, q, b, dx, ncls=ncls, ntab=MANNING_CLASSES, linf=linf,
+                          rain_times=rf.time_s, rain_table=(np.asarray(rf.rate_mm_h) / 3.6e6).astype(np.float32)[:, None],
+                          rain_lookup=np.zeros(cs.n_stored, np.int64))
+    n_g = cs.run(t_end=1500.0)
+    n_o = o.run(t_end=1500.0)
+    assert n_g == n_o and n_g > 10
+    assert cs.t == o.t
+    for c in range(3):
+        assert same(cs.flat(c).cpu().numpy(), o.q[c]), c
+
+
+def test_dense_masked_run_equals_flat_run():
+    """With the dense solver's velocity norm (cfl_linf) and a mask away from the edges,
+    the dense run over the whole grid and the compressed run take the same steps and
+    end in the same state on the active cells (the reference's equivalence contract,
+    tests/test_gpu_compressed_equiv.py, bit for bit here)."""
+    from geoswe_b200.compressed import CompressedSolver
+    n = 80
+    i = np.arange(n)[:, None]
+    j = np.arange(n)[None, :]
+    r = np.hypot(i - 40, j - 38)
+    bed = (0.002 * r ** 2).astype(np.float32)           # a bowl
+    h = np.where(r < 10, 1.5, 0.0) + np.maximum(0.8 - bed, 0.0)
+    q0 = np.stack([h, 0 * h, 0 * h]).astype(np.float32)
+    mask = r < 30
+    sd = _dense(q0, bed, mask, dx=1.0, friction="manning", manning_n=0.03)
+    cs = CompressedSolver.from_dense(_dense(q0, bed, mask, dx=1.0, friction="manning", manning_n=0.03),
+                                     cfl_linf=True)
+    nd = sd.run(t_end=40.0)
+    nf = cs.run(t_end=40.0)
+    assert nd == nf
+    hd = sd.depth()
+    hf = cs.depth()
+    assert same(hf[mask], hd[mask])

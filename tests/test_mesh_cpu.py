@@ -1,0 +1,58 @@
+"""Compressed-mesh tables, bit-exact against the reference's CompressedSWE
+(tests/golden/reference_mesh.npz, produced by the reference itself), and the brick
+layout's bookkeeping. Host code only (no GPU)."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from geoswe_b200.compressed import BRICK_PITCH, BRICK_W, build_bricks, build_tables
+from geoswe_b200.synthetic import dilate_cross
+
+M = np.load(Path(__file__).resolve().parent / "golden" / "reference_mesh.npz")
+CASES = sorted({k.split("_")[1] for k in M.files})
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_tables_bit_exact(case):
+    tb = build_tables(M[f"mesh_{case}_inside"], ring=2)
+    assert np.array_equal(tb["ij"], M[f"mesh_{case}_ij"])
+    assert np.array_equal(tb["active_id"], M[f"mesh_{case}_aid"])
+    assert np.array_equal(tb["nbr"], M[f"mesh_{case}_nbr16"])
+    assert tb["nbr"].dtype == np.int16
+    assert np.array_equal(tb["is_active"], M[f"mesh_{case}_active"])
+    assert tb["fully_covered"] == bool(M[f"mesh_{case}_covered"])
+
+
+def test_int16_overflow_refused():
+    inside = np.zeros((6, 33000), np.uint8)
+    inside[2:4, 2:-2] = 1
+    with pytest.raises(ValueError, match="int16"):
+        build_tables(inside, ring=2)
+
+
+def test_dilation_matches_scipy():
+    from scipy.ndimage import binary_dilation
+    rng = np.random.default_rng(3)
+    m = rng.random((57, 43)) < 0.1
+    assert np.array_equal(dilate_cross(m, 2), binary_dilation(m, iterations=2))
+    assert np.array_equal(dilate_cross(m, 8), binary_dilation(m, iterations=8))
+
+
+@pytest.mark.parametrize("bh", [2, 8, 16])
+def test_bricks_cover_stored_cells(bh):
+    inside = M["mesh_blob_inside"]
+    tb = build_tables(inside)
+    stored = tb["active_id"] >= 0
+    bij, bnbr = build_bricks(stored, bh)
+    nb = len(bij)
+    # every stored cell's brick exists, bricks are unique, links are consistent
+    keys = set(map(tuple, bij.tolist()))
+    assert len(keys) == nb
+    for i, j in np.argwhere(stored):
+        assert (i // bh, j // BRICK_W) in keys
+    idx = {tuple(k): n for n, k in enumerate(bij.tolist())}
+    for n, (a, c) in enumerate(bij.tolist()):
+        for d, (da, dc) in enumerate([(-1, 0), (1, 0), (0, -1), (0, 1)]):
+            exp = idx.get((a + da, c + dc), nb)
+            assert bnbr[n, d] == exp
