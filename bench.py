@@ -230,7 +230,77 @@ def run_e2e(args, z, cls, n):
             "what": "Solver2D(host arrays) + run(steps) + depth(); bytes per step = total / steps"}
 
 
-def cpu_baseline(args):
+def build_member(spec, brick_h=16, device="cuda"):
+    """One member of the uneven ensemble as a CompressedSolver (inputs generated on the GPU)."""
+    import torch
+    from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
+    from geoswe_b200.compressed import CompressedSolver
+    from geoswe_b200.synthetic import (MANNING_CLASSES, fractal_bed_device, triangular_hyetograph,
+                                       voronoi_classes_device)
+    nx, ny = spec["nx"], spec["ny"]
+    z = fractal_bed_device(nx, ny, 3.0, seed=spec["seed"], device=device)
+    thr = torch.kthvalue(z.reshape(-1).cpu(), max(1, int(spec["frac"] * nx * ny))).values.item()
+    mask = (z <= thr).cpu().numpy()
+    mask[:3, :] = mask[-3:, :] = False
+    mask[:, :3] = mask[:, -3:] = False
+    cls = voronoi_classes_device(nx, ny, seed=spec["seed"], device=device).cpu().numpy()
+    s = Solver2D(Mesh2D(nx=nx, ny=ny, dx=3.0, dy=3.0, ngh=2), Config(bc_x="fall", bc_y="fall", friction="manning"),
+                 np.zeros((3, nx, ny), np.float32), z.cpu().numpy(), track_max_depth=False)
+    s.set_inside_mask(mask)
+    s.set_manning_table(np.pad(cls, 2, mode="edge"), MANNING_CLASSES * spec["scale"])
+    cs = CompressedSolver.from_dense(s, brick_h=brick_h)
+    del s
+    t, r = triangular_hyetograph(spec["peak"], spec["t_peak"])
+    cs.set_rain(RainfallForcing(time_s=t, rate_mm_h=r))
+    return cs
+
+
+def run_ensemble(args):
+    """Batched ensemble vs looping the plain compressed solver over the same members, for
+    the same simulated window; cell-updates/s = sum over members of active cells x steps."""
+    import torch
+    from geoswe_b200.ensemble import Ensemble
+    from geoswe_b200.synthetic import ensemble_specs
+    torch.cuda.set_device(0)
+    specs = ensemble_specs(n_members=args.members, seed=0)
+    t_end = args.ens_t_end
+    t0 = time.perf_counter()
+    loop_members = [build_member(sp) for sp in specs]
+    build_s = time.perf_counter() - t0
+    # plain solver, one member after another (its own graph-captured device loop)
+    for m in loop_members:                       # warm-up: capture graphs, first steps
+        m.run(t_end=args.warmup * 1e-3 + 1e-3, max_steps=args.warmup)
+    loop_members = [build_member(sp) for sp in specs]
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    steps_loop = [m.run(t_end=t_end) for m in loop_members]
+    e1.record()
+    torch.cuda.synchronize()
+    ms_loop = e0.elapsed_time(e1)
+    work = sum(m.N_active * n for m, n in zip(loop_members, steps_loop))
+    del loop_members
+    torch.cuda.empty_cache()
+    # batched
+    ens = Ensemble([build_member(sp) for sp in specs], warps=args.ens_warps, grid=args.ens_grid)
+    torch.cuda.synchronize()
+    e0.record()
+    steps_ens = ens.run(t_end=t_end, window=args.ens_window)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_ens = e0.elapsed_time(e1)
+    same_steps = steps_ens == steps_loop
+    out = {"metric": METRIC + " [batched ensemble]", "value": work / (ms_ens / 1e3), "unit": UNIT,
+           "n_gpus": 1, "members": len(specs), "cells_total": int(sum(sp["nx"] * sp["ny"] for sp in specs)),
+           "active_total": int(sum(ens.active_cells)), "t_end_s": t_end,
+           "steps_per_member": {"min": int(min(steps_ens)), "max": int(max(steps_ens)),
+                                "sum": int(sum(steps_ens))},
+           "ms_batched": ms_ens, "ms_plain_loop": ms_loop,
+           "plain_loop_value": work / (ms_loop / 1e3), "speedup_vs_plain_loop": ms_loop / ms_ens,
+           "identical_steps_to_plain": bool(same_steps), "gpu_launches": int(ens.kernel_launches),
+           "build_s": build_s, "dtype": "f32", "data": "synthetic"}
+    return out
+
     """The reference's CPU path (its NumPy solver, restated in oracle/numpy_ref.py) on a
     bounded sample of the same workload, on this host's cores."""
     try:
@@ -252,6 +322,12 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--case", default="dense", choices=["dense", "ensemble"])
+    ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--ens-t-end", type=float, default=600.0)
+    ap.add_argument("--ens-window", type=int, default=32)
+    ap.add_argument("--ens-warps", type=int, default=0)
+    ap.add_argument("--ens-grid", type=int, default=0)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -261,6 +337,10 @@ def main():
         from oracle import numpy_ref
         out = numpy_ref.reference_arm(args, METRIC, UNIT)
         print(json.dumps(out), flush=True)
+        return 0
+    if args.case == "ensemble":
+        if rank == 0:
+            print(json.dumps(run_ensemble(args)), flush=True)
         return 0
     if world > 1:
         import torch

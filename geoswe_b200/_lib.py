@@ -87,6 +87,20 @@ class GswFlatArgs(C.Structure):
                 ("quadratic", i32), ("keep_h", i32), ("max_h", vp), ("warps", i32)]
 
 
+class GswMember(C.Structure):
+    _fields_ = [("dt", GswDtParams), ("inv_dx", C.c_float), ("g", C.c_float), ("h_min", C.c_float),
+                ("h_min_cfl", C.c_float), ("vcap", C.c_float), ("linf", i32), ("quadratic", i32),
+                ("keep_h", i32), ("rain_kind", i32), ("reserved0", i32), ("rain", vp), ("n_tab", vp)]
+
+
+class GswEnsembleArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("brick_h", i32), ("n_bricks", i64), ("n_members", i32),
+                ("warps", i32), ("grid", i32), ("reserved0", i32), ("brick_ij", vp), ("brick_nbr", vp),
+                ("brick_member", vp), ("flags", vp), ("n_cls", vp), ("q0", vp), ("q1", vp), ("q2", vp),
+                ("qn0", vp), ("qn1", vp), ("qn2", vp), ("bed", vp), ("max_h", vp), ("members", vp),
+                ("states", vp), ("scratch", vp), ("all_done", vp)]
+
+
 # entry point -> argtypes
 _PROTOS = {
     "gsw_dense_step": [C.POINTER(GswDenseArgs), vp],
@@ -104,6 +118,9 @@ _PROTOS = {
     "gsw_mesh_count": [vp, C.c_int, C.c_int, C.c_int, vp, vp],
     "gsw_mesh_build": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp],
     "gsw_bricks_build": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp],
+    "gsw_ensemble_lammax": [C.POINTER(GswEnsembleArgs), vp],
+    "gsw_ensemble_finalize": [C.POINTER(GswEnsembleArgs), vp],
+    "gsw_ensemble_step": [C.POINTER(GswEnsembleArgs), vp],
 }
 
 

@@ -44,73 +44,9 @@ int sm_count() {
     return cached;
 }
 
-// Commit the previous step (t = t_new, steps += 1).
-__device__ __forceinline__ void commit(GswLoopState* s) {
-    if (s->pending) {
-        s->t = s->t_new;
-        s->steps += 1;
-        s->pending = 0;
-    }
-}
+__global__ void dt_finalize_kernel(GswDtParams p, GswLoopState* s) { dt_finalize_one(p, s, s->lam_bits); }
 
-// One thread. Mirrors, in this order:
-//   Solver2D.run   : while t < t_end - 1e-12 and steps < max_steps        (solver.py:2990)
-//   cfl_dt         : non-finite -> error; lam = max(lam, sqrt(g h_cfl));
-//                    dt = cfl*dmin / (lam + 1e-12)                        (solver.py:2652-2666)
-//   _rain_step_limit: dt = min(dt, (cfl dmin)^(2/3) / (g Rmax)^(1/3))     (solver.py:3005-3027)
-//   dt_max, then the clip onto t_end                                      (solver.py:2992-2995)
-// The flat loop (compressed_solver.py:713-748, 2133-2197) is the same arithmetic with
-// eps_end = 1e-9 and the rain limit folded into dt_max by the caller.
-__global__ void dt_finalize_kernel(GswDtParams p, GswLoopState* s) {
-    commit(s);
-    if (s->done) return;
-    if (!(s->t < p.t_end - p.eps_end) || (p.max_steps > 0 && s->steps >= p.max_steps)) {
-        s->done = 1;
-        return;
-    }
-    const double t = s->t;
-    int idx = 0;
-    if (p.rain_t != nullptr && p.n_rain > 0) {       // bisect_right(time_s, t) - 1, clamped
-        int lo = 0, hi = p.n_rain;
-        while (lo < hi) { const int mid = (lo + hi) >> 1; if (t < p.rain_t[mid]) hi = mid; else lo = mid + 1; }
-        idx = lo - 1;
-        if (idx < 0) idx = 0;
-        if (idx > p.n_rain - 1) idx = p.n_rain - 1;
-    }
-    s->rain_idx = idx;
-    double dt;
-    if (p.mode == 1) {
-        dt = p.fixed_dt;
-        s->lam_used = 0.0;
-    } else {
-        const double lam_in = __longlong_as_double((long long)s->lam_bits);
-        if (!(lam_in <= 1.0e308)) {                   // NaN or Inf: the host raises FloatingPointError
-            s->error = GSW_ERR_NONFINITE;
-            s->done = 1;
-            s->lam_used = lam_in;
-            return;
-        }
-        double lam = lam_in;
-        if (lam < p.lam_floor) lam = p.lam_floor;
-        s->lam_used = lam;
-        dt = __ddiv_rn(p.cfl_dmin, __dadd_rn(lam, 1.0e-12));
-        if (p.rain_lim != nullptr && p.rain_lim[idx] > 0.0 && p.rain_lim[idx] < dt) dt = p.rain_lim[idx];
-        if (p.dt_max > 0.0 && dt > p.dt_max) dt = p.dt_max;
-    }
-    if (p.clip_flat) {
-        const double rem = __dsub_rn(p.t_end, t);
-        if (rem < dt) dt = rem;
-    } else if (__dadd_rn(t, dt) > p.t_end) {
-        dt = __dsub_rn(p.t_end, t);
-    }
-    s->dt = dt;
-    s->dt_f32 = (float)dt;
-    s->t_new = __dadd_rn(t, dt);
-    s->pending = 1;
-    s->lam_bits = 0ull;                               // this step's kernels reduce lambda(next)
-}
-
-__global__ void loop_commit_kernel(GswLoopState* s) { commit(s); }
+__global__ void loop_commit_kernel(GswLoopState* s) { loop_commit(s); }
 
 }  // namespace gsw
 

@@ -107,3 +107,63 @@ def tidal_case(nx, ny, dx=1.0, seed=0, eta0=1.5, noise=0.01, dtype=np.float32):
     eta = eta0 + noise * rng.standard_normal((nx, ny))
     h = np.maximum(eta - z, 0.0)
     return h.astype(dtype), z.astype(dtype)
+
+
+def fractal_bed_device(nx, ny, dx, seed=0, zmax=40.0, slope=0.002, device="cuda"):
+    """fractal_bed with the same seeded noise, transformed on the GPU (float32 result)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    noise = torch.complex(torch.from_numpy(rng.standard_normal((nx, ny))),
+                          torch.from_numpy(rng.standard_normal((nx, ny)))).to(device)
+    kx = torch.fft.fftfreq(nx, device=device, dtype=torch.float64)[:, None]
+    ky = torch.fft.fftfreq(ny, device=device, dtype=torch.float64)[None, :]
+    k = torch.sqrt(kx * kx + ky * ky)
+    amp = torch.where(k > 0, k.clamp_min(1e-300) ** -1.5, torch.zeros_like(k))
+    z = torch.fft.ifft2(noise * amp).real
+    z = (z - z.min()) / (z.max() - z.min()) * zmax
+    x = (torch.arange(nx, device=device, dtype=torch.float64) + 0.5) * dx
+    return (z + slope * x[:, None]).to(torch.float32)
+
+
+def voronoi_classes_device(nx, ny, n_seeds=256, n_classes=4, seed=0, device="cuda"):
+    """voronoi_classes (same seeds and classes), nearest seed found on the GPU."""
+    import torch
+    rng = np.random.default_rng(seed + 7919)
+    pts = torch.from_numpy(rng.random((n_seeds, 2)) * np.array([nx, ny], dtype=np.float64)).to(device)
+    cls_of_seed = torch.from_numpy(rng.integers(n_classes, size=n_seeds).astype(np.uint8)).to(device)
+    out = torch.empty((nx, ny), dtype=torch.uint8, device=device)
+    jj = torch.arange(ny, device=device, dtype=torch.float64) + 0.5
+    rows = max(1, (1 << 22) // max(ny, 1))
+    for i0 in range(0, nx, rows):
+        i1 = min(nx, i0 + rows)
+        ci = (torch.arange(i0, i1, device=device, dtype=torch.float64) + 0.5)[:, None].expand(i1 - i0, ny)
+        cj = jj[None, :].expand(i1 - i0, ny)
+        c = torch.stack([ci.reshape(-1), cj.reshape(-1)], dim=1)
+        d = torch.cdist(c, pts)
+        out[i0:i1] = cls_of_seed[d.argmin(dim=1)].reshape(i1 - i0, ny)
+    return out
+
+
+def triangular_hyetograph(peak_mm_h, t_peak_s, t_end_s=3600.0, every_s=60.0):
+    """Piecewise-constant samples (every `every_s`, value at each interval's midpoint) of a
+    triangle rising from 0 at t=0 to `peak_mm_h` at `t_peak_s` and back to 0 at 2 t_peak."""
+    t = np.arange(0.0, t_end_s + every_s, every_s)
+    mid = t + 0.5 * every_s
+    r = np.where(mid <= t_peak_s, peak_mm_h * mid / t_peak_s,
+                 np.maximum(peak_mm_h * (2.0 * t_peak_s - mid) / t_peak_s, 0.0))
+    return t, r
+
+
+def ensemble_specs(n_members=64, seed=0, side_min=256, side_max=4096):
+    """Member parameters of the uneven-ensemble case: side ~ exp(U(ln 256, ln 4096)) per axis,
+    active fraction ~ U(0.3, 0.9), triangular rain with peak ~ U(20, 120) mm/h at
+    t_p ~ U(0.5, 3) h, Manning scale ~ U(0.7, 1.3)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_members):
+        nx = int(round(np.exp(rng.uniform(np.log(side_min), np.log(side_max)))))
+        ny = int(round(np.exp(rng.uniform(np.log(side_min), np.log(side_max)))))
+        out.append(dict(seed=1000 + k, nx=nx, ny=ny, frac=float(rng.uniform(0.3, 0.9)),
+                        peak=float(rng.uniform(20.0, 120.0)), t_peak=float(rng.uniform(0.5, 3.0)) * 3600.0,
+                        scale=float(rng.uniform(0.7, 1.3))))
+    return out

@@ -291,6 +291,55 @@ GSW_API int gsw_bricks_build(const uint8_t* stored, int nxp, int nyp, int brick_
                              int64_t* n_bricks, int32_t* brick_ij, int32_t* brick_nbr);
 
 /* ------------------------------------------------------------------------- */
+/* Batched ensemble: many compressed meshes advanced by one kernel per step.  */
+/* ------------------------------------------------------------------------- */
+/* Physics and time-step rule of one member. */
+typedef struct GswMember {
+    GswDtParams dt;          /* the member's flat time-step rule (rain limit folded into dt_max) */
+    float    inv_dx, g, h_min, h_min_cfl, vcap;
+    int32_t  linf, quadratic, keep_h;
+    int32_t  rain_kind;      /* GSW_RAIN_NONE or GSW_RAIN_UNIFORM */
+    int32_t  reserved0;
+    const float* rain;       /* uniform rate (m/s) per rain frame */
+    const float* n_tab;      /* the member's Manning class table */
+} GswMember;
+
+typedef struct GswEnsembleArgs {
+    uint32_t abi_version;
+    int32_t  brick_h;
+    int64_t  n_bricks;           /* bricks of all members; brick n_bricks is the zero brick */
+    int32_t  n_members;
+    int32_t  warps;              /* warps per block (0: 4) */
+    int32_t  grid;               /* persistent blocks (0: 2 per SM) */
+    int32_t  reserved0;
+    const int32_t* brick_ij;     /* (n_bricks, 2) */
+    const int32_t* brick_nbr;    /* (n_bricks, 4) global brick ids */
+    const int32_t* brick_member; /* (n_bricks) */
+    const uint8_t* flags;        /* per slot */
+    const uint8_t* n_cls;        /* per slot, or NULL (class 0) */
+    const float* q0; const float* q1; const float* q2;
+    float* qn0; float* qn1; float* qn2;
+    const float* bed;
+    float*   max_h;              /* per slot, or NULL */
+    const GswMember* members;    /* device, n_members */
+    GswLoopState* states;        /* device, n_members */
+    uint32_t* scratch;           /* device, >= 4 words, zero before the first step: block tickets */
+    int32_t* all_done;           /* device int: 1 once every member is done */
+} GswEnsembleArgs;
+
+/* Wave speed of every member's current state into states[m].lam_bits (atomicMax). */
+GSW_API int gsw_ensemble_lammax(const GswEnsembleArgs* a, void* stream);
+/* Each member's dt / rain frame / done from states[m].lam_bits (the flat loop's rule);
+ * sets *all_done. */
+GSW_API int gsw_ensemble_finalize(const GswEnsembleArgs* a, void* stream);
+/* One step of every member that is not done, in one persistent launch: warps take
+ * bricks from the whole ensemble, each with its member's dt, rain and Manning table,
+ * and reduce the member's new wave speed; the last block to finish computes every
+ * member's next dt (no grid barrier). A member's trajectory equals its CompressedSolver
+ * run bit for bit. */
+GSW_API int gsw_ensemble_step(const GswEnsembleArgs* a, void* stream);
+
+/* ------------------------------------------------------------------------- */
 /* Loop control.                                                              */
 /* ------------------------------------------------------------------------- */
 /* Commit the pending t/steps, test the loop condition, and compute this step's dt

@@ -40,7 +40,10 @@ def test_struct_layouts_match_c(tmp_path):
               "GswStageArgs": ["pitch", "bed_is_f32", "time_s", "lam_target", "g", "h_cfl"],
               "GswInflowArgs": ["pitch", "step_off", "nx_n", "t_knots", "state"],
               "GswFlatArgs": ["n_bricks", "flags", "bed", "inv_dx", "h_min_cfl", "linf", "state", "rain",
-                              "ny", "n_tab_len", "vcap", "keep_h", "max_h", "warps"]}
+                              "ny", "n_tab_len", "vcap", "keep_h", "max_h", "warps"],
+              "GswMember": ["dt", "inv_dx", "vcap", "linf", "rain_kind", "rain", "n_tab"],
+              "GswEnsembleArgs": ["n_bricks", "n_members", "grid", "brick_ij", "flags", "q0", "bed",
+                                  "members", "states", "scratch", "all_done"]}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{ROOT}/include/gsw.h"', "int main(){"]
     for s, fs in checks.items():
         lines.append(f'printf("{s} %zu\\n", sizeof({s}));')
