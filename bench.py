@@ -257,39 +257,46 @@ def build_member(spec, brick_h=16, device="cuda"):
 
 def run_ensemble(args):
     """Batched ensemble vs looping the plain compressed solver over the same members, for
-    the same simulated window; cell-updates/s = sum over members of active cells x steps."""
+    the same simulated window; cell-updates/s = sum over members of active cells x steps.
+    Both timed regions include their own CUDA-graph captures."""
     import torch
+    from geoswe_b200 import autotune
     from geoswe_b200.ensemble import Ensemble
     from geoswe_b200.synthetic import ensemble_specs
     torch.cuda.set_device(0)
     specs = ensemble_specs(n_members=args.members, seed=0)
     t_end = args.ens_t_end
+    # warm-up: context, library and capture paths on the smallest member
+    small = min(specs, key=lambda sp: sp["nx"] * sp["ny"])
+    build_member(small).run(t_end=t_end, max_steps=max(args.warmup, 3))
+    Ensemble([build_member(small), build_member(small)]).run(t_end=t_end, max_steps=max(args.warmup, 3), window=8)
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     loop_members = [build_member(sp) for sp in specs]
-    build_s = time.perf_counter() - t0
-    # plain solver, one member after another (its own graph-captured device loop)
-    for m in loop_members:                       # warm-up: capture graphs, first steps
-        m.run(t_end=args.warmup * 1e-3 + 1e-3, max_steps=args.warmup)
-    loop_members = [build_member(sp) for sp in specs]
     torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     steps_loop = [m.run(t_end=t_end) for m in loop_members]
     e1.record()
     torch.cuda.synchronize()
     ms_loop = e0.elapsed_time(e1)
+    loop_launches = int(sum(m.kernel_launches for m in loop_members))
     work = sum(m.N_active * n for m, n in zip(loop_members, steps_loop))
     del loop_members
     torch.cuda.empty_cache()
-    # batched
     ens = Ensemble([build_member(sp) for sp in specs], warps=args.ens_warps, grid=args.ens_grid)
+    tune = None
+    if not args.no_tune and args.ens_warps == 0 and args.ens_grid == 0:
+        best, table = autotune.tune_ensemble(ens, t_end)
+        tune = {"best": best, "table": table}
+    n0 = ens.kernel_launches
     torch.cuda.synchronize()
     e0.record()
     steps_ens = ens.run(t_end=t_end, window=args.ens_window)
     e1.record()
     torch.cuda.synchronize()
     ms_ens = e0.elapsed_time(e1)
-    same_steps = steps_ens == steps_loop
     out = {"metric": METRIC + " [batched ensemble]", "value": work / (ms_ens / 1e3), "unit": UNIT,
            "n_gpus": 1, "members": len(specs), "cells_total": int(sum(sp["nx"] * sp["ny"] for sp in specs)),
            "active_total": int(sum(ens.active_cells)), "t_end_s": t_end,
@@ -297,10 +304,14 @@ def run_ensemble(args):
                                 "sum": int(sum(steps_ens))},
            "ms_batched": ms_ens, "ms_plain_loop": ms_loop,
            "plain_loop_value": work / (ms_loop / 1e3), "speedup_vs_plain_loop": ms_loop / ms_ens,
-           "identical_steps_to_plain": bool(same_steps), "gpu_launches": int(ens.kernel_launches),
+           "identical_steps_to_plain": bool(steps_ens == steps_loop),
+           "gpu_launches": int(ens.kernel_launches - n0), "gpu_launches_plain_loop": loop_launches,
+           "schedule": {"warps": ens.warps or 4, "grid": ens.grid, "brick_h": ens.brick_h}, "autotune": tune,
            "build_s": build_s, "dtype": "f32", "data": "synthetic"}
     return out
 
+
+def cpu_baseline(args):
     """The reference's CPU path (its NumPy solver, restated in oracle/numpy_ref.py) on a
     bounded sample of the same workload, on this host's cores."""
     try:
@@ -324,7 +335,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--case", default="dense", choices=["dense", "ensemble"])
     ap.add_argument("--members", type=int, default=64)
-    ap.add_argument("--ens-t-end", type=float, default=600.0)
+    ap.add_argument("--ens-t-end", type=float, default=3600.0)
     ap.add_argument("--ens-window", type=int, default=32)
     ap.add_argument("--ens-warps", type=int, default=0)
     ap.add_argument("--ens-grid", type=int, default=0)

@@ -118,3 +118,25 @@ def tune_dense(s, reps=8, space=None, store=True, verbose=False):
     if store:
         _store("dense", cells, best)
     return best, table
+
+
+ENSEMBLE_SPACE = dict(warps=(2, 4, 8), blocks_per_sm=(1, 2, 4, 8))
+
+
+def tune_ensemble(ens, t_end, reps=6, space=None, store=True, verbose=False):
+    """Time the ensemble step for every (warps, blocks per SM) of `space` from the
+    ensemble's current state (restored before every launch, so nothing advances); set
+    the winner on `ens` and cache it. Returns (best, table)."""
+    space = space or ENSEMBLE_SPACE
+    sms = torch.cuda.get_device_properties(ens.device).multi_processor_count
+    table = []
+    for w, bps in itertools.product(space["warps"], space["blocks_per_sm"]):
+        ms = ens.time_step(t_end, warps=w, grid=bps * sms, reps=reps)
+        table.append(dict(warps=w, blocks_per_sm=bps, grid=bps * sms, ms=ms))
+        if verbose:
+            print(f"  warps={w} blocks/SM={bps}: {ms:.4f} ms", flush=True)
+    best = min(table, key=lambda e: e["ms"])
+    ens.warps, ens.grid = best["warps"], best["grid"]
+    if store:
+        _store("ensemble", ens.nslots, best)
+    return best, table

@@ -79,7 +79,8 @@ class Ensemble:
         self._states = torch.zeros(M * C.sizeof(L.GswLoopState), dtype=torch.uint8, device=dev)
         self._scratch = torch.zeros(4, dtype=torch.int32, device=dev)
         self._all_done = torch.zeros(1, dtype=torch.int32, device=dev)
-        self._members_dev = None
+        # fixed device buffers: captured graphs hold their addresses across runs
+        self._members_dev = torch.zeros(M * C.sizeof(GswMember), dtype=torch.uint8, device=dev)
         self._parity = np.zeros(M, np.int64)       # buffer of each member's current state
         self.warps, self.grid = int(warps), int(grid)
         self.kernel_launches = 0
@@ -140,8 +141,7 @@ class Ensemble:
             mb.rain_kind = m._rain_kind
             mb.rain = _ptr(m._rain)
             mb.n_tab = _ptr(self._tabs[k])
-        raw = bytes(arr)
-        self._members_dev = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(self.device)
+        self._members_dev.copy_(torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8))
         st = (L.GswLoopState * M)()
         for k, m in enumerate(self.members):
             st[k].t = float(m.t)
@@ -152,10 +152,9 @@ class Ensemble:
         raw = self._states.cpu().numpy().tobytes()
         return (L.GswLoopState * M).from_buffer_copy(raw)
 
-    def run(self, t_end, *, max_steps: int = 10 ** 9, dt_max=None, window: int = 64):
-        """Advance every member to its t_end (scalar or one per member). Returns the list
-        of steps each member took."""
-        Lb = _protos()
+    def _prepare(self, t_end, max_steps, dt_max):
+        """Members' parameters and fresh loop states, every member's state in one buffer,
+        the initial wave speeds reduced and the first dt evaluated. Returns that buffer."""
         M = len(self.members)
         self._build_members(t_end, max_steps, dt_max)
         p0 = int(np.bincount(self._parity, minlength=2).argmax())
@@ -171,6 +170,40 @@ class Ensemble:
         L.call("gsw_ensemble_lammax", C.byref(self._args(self._q[p0], self._q[p0])), s)
         L.call("gsw_ensemble_finalize", C.byref(self._args(self._q[p0], self._q[p0])), s)
         self.kernel_launches += 2
+        return p0
+
+    def time_step(self, t_end, *, warps, grid, reps=6, max_steps: int = 10 ** 9, dt_max=None):
+        """Mean duration (ms) of one ensemble step launch with the given schedule, from the
+        current state; the states are restored before every launch and the members' state
+        is left as it was."""
+        _protos()
+        p0 = self._prepare(t_end, max_steps, dt_max)
+        snap = self._states.clone()
+        saved = (self.warps, self.grid)
+        self.warps, self.grid = int(warps), int(grid)
+        args = self._args(self._q[p0], self._q[1 - p0])
+        self.warps, self.grid = saved
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        total = 0.0
+        for k in range(reps + 1):
+            self._states.copy_(snap)
+            self._scratch.zero_()
+            self._all_done.zero_()
+            e0.record()
+            L.call("gsw_ensemble_step", C.byref(args), _stream())
+            e1.record()
+            torch.cuda.synchronize()
+            if k:
+                total += e0.elapsed_time(e1)
+        self.kernel_launches += reps + 1
+        self._states.copy_(snap)
+        return total / reps
+
+    def run(self, t_end, *, max_steps: int = 10 ** 9, dt_max=None, window: int = 64):
+        """Advance every member to its t_end (scalar or one per member). Returns the list
+        of steps each member took."""
+        _protos()
+        p0 = self._prepare(t_end, max_steps, dt_max)
         K = int(window) + int(window) % 2
 
         def one_window():
@@ -180,7 +213,7 @@ class Ensemble:
                 L.call("gsw_ensemble_step", C.byref(self._args(src, dst)), st)
             return K
 
-        key = (K, p0)
+        key = (K, p0, self.warps, self.grid)
         if key not in self._graph_cache:
             self._graph_cache.clear()
             side = torch.cuda.Stream(device=self.device)

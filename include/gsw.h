@@ -292,6 +292,9 @@ GSW_API int gsw_bricks_build(const uint8_t* stored, int nxp, int nyp, int brick_
 
 /* ------------------------------------------------------------------------- */
 /* Batched ensemble: many compressed meshes advanced by one kernel per step.  */
+/* No counterpart in the reference, which runs scenarios one after another    */
+/* (a Python loop over CompressedSolver.run, geoswe/compressed_solver.py:     */
+/* 3359); each member follows that solver's flat loop exactly.                */
 /* ------------------------------------------------------------------------- */
 /* Physics and time-step rule of one member. */
 typedef struct GswMember {
