@@ -40,7 +40,7 @@ class GswDtParams(C.Structure):
     _fields_ = [("abi_version", u32), ("mode", i32), ("cfl_dmin", f64), ("lam_floor", f64),
                 ("t_end", f64), ("eps_end", f64), ("dt_max", f64), ("fixed_dt", f64),
                 ("max_steps", i64), ("rain_t", vp), ("rain_lim", vp), ("n_rain", i32),
-                ("clip_flat", i32)]
+                ("clip_flat", i32), ("dt_table", vp), ("dt_log", vp)]
 
 
 class GswDenseArgs(C.Structure):
@@ -77,14 +77,19 @@ class GswInflowArgs(C.Structure):
 
 
 class GswFlatArgs(C.Structure):
-    _fields_ = [("abi_version", u32), ("brick_h", i32), ("n_bricks", i64),
+    _fields_ = [("abi_version", u32), ("dtype", i32), ("brick_h", i32), ("warps", i32), ("n_bricks", i64),
                 ("brick_ij", vp), ("brick_nbr", vp), ("flags", vp),
                 ("q0", vp), ("q1", vp), ("q2", vp), ("qn0", vp), ("qn1", vp), ("qn2", vp), ("bed", vp),
-                ("inv_dx", C.c_float), ("inv_dy", C.c_float), ("g", C.c_float), ("h_min", C.c_float),
-                ("h_min_cfl", C.c_float), ("linf", i32), ("state", vp), ("lam_target", vp),
-                ("rain_kind", i32), ("rain", vp), ("ngh", i32), ("nx", i32), ("ny", i32),
-                ("n_cls", vp), ("n_tab", vp), ("n_tab_len", i32), ("vcap", C.c_float),
-                ("quadratic", i32), ("keep_h", i32), ("max_h", vp), ("warps", i32)]
+                ("inv_dx", f64), ("inv_dy", f64), ("g", f64), ("h_min", f64), ("h_min_cfl", f64),
+                ("linf", i32), ("rain_kind", i32), ("state", vp), ("lam_target", vp), ("rain", vp),
+                ("ngh", i32), ("nx", i32), ("ny", i32), ("n_tab_len", i32), ("n_cls", vp), ("n_tab", vp),
+                ("vcap", f64), ("quadratic", i32), ("keep_h", i32), ("max_h", vp)]
+
+
+class GswFlatInflowArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("dtype", i32), ("q0", vp), ("q1", vp), ("q2", vp), ("bed", vp),
+                ("ghost_slot", vp), ("nbr_slot", vp), ("n", i32), ("n_knots", i32), ("nx_n", f64),
+                ("ny_n", f64), ("ds", f64), ("t_knots", vp), ("q_knots", vp), ("state", vp)]
 
 
 class GswMember(C.Structure):
@@ -112,6 +117,7 @@ _PROTOS = {
     "gsw_inflow_apply": [C.POINTER(GswInflowArgs), vp],
     "gsw_dt_finalize": [C.POINTER(GswDtParams), vp, vp],
     "gsw_loop_commit": [vp, vp],
+    "gsw_flat_inflow_apply": [C.POINTER(GswFlatInflowArgs), vp],
     "gsw_flat_step": [C.POINTER(GswFlatArgs), vp],
     "gsw_flat_rhs": [C.POINTER(GswFlatArgs), vp],
     "gsw_flat_lammax": [C.POINTER(GswFlatArgs), vp, vp],

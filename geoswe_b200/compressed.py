@@ -218,6 +218,7 @@ class CompressedSolver:
         self._rain_kind = L.RAIN_NONE
         self._rain_t = None
         self._rain_rmax = 0.0
+        self._inflows = []
         self._graph_cache = {}
         self.t = 0.0
         self.nsteps = 0
@@ -250,6 +251,68 @@ class CompressedSolver:
         self._rain_rmax = float(table.max())
         self._graph_cache.clear()
         return self
+
+    def ghost_boundary_pairs(self):
+        """Ghost (ring) cells that touch the active set, each with its first active
+        neighbour in E, W, N, S order, as canonical flat indices (the pairing
+        ``add_inflow`` takes; compressed_solver.py:468-483)."""
+        nbr = self.nbr.astype(np.int64)
+        act = self.is_active
+        N = act.size
+        k = np.arange(N, dtype=np.int64)
+        best = np.full(N, -1, np.int64)
+        ghost = act == 0
+        for d in range(4):
+            dl = nbr[:, d]
+            cand = k + dl
+            ok = (dl > -32768) & (cand >= 0) & (cand < N)
+            cand = np.where(ok, cand, 0)
+            ok &= (act[cand] != 0) & ghost & (best < 0)
+            best = np.where(ok, cand, best)
+        sel = best >= 0
+        return k[sel], best[sel]
+
+    def add_inflow(self, ghost_idx, nbr_idx, normal, ds, t_series, q_series):
+        """Add one discharge (hydrograph) inlet (compressed_solver.py:3193-3207): ghost and
+        active-neighbour cells as canonical flat indices (from ghost_boundary_pairs), the
+        inward unit normal (axis-aligned), the cell width and the hydrograph Q(t) in m^3/s."""
+        g = np.asarray(ghost_idx, np.int64).reshape(-1)
+        a = np.asarray(nbr_idx, np.int64).reshape(-1)
+        if g.size != a.size:
+            raise ValueError("add_inflow: ghost_idx and nbr_idx must have the same length")
+        nx_n, ny_n = (float(normal[0]), float(normal[1]))
+        if sorted((abs(nx_n), abs(ny_n))) != [0.0, 1.0]:
+            raise ValueError(f"add_inflow: the inward normal must be axis-aligned, got {normal}")
+        t = np.asarray(t_series, np.float64).reshape(-1)
+        qs = np.asarray(q_series, np.float64).reshape(-1)
+        if t.size != qs.size or t.size < 1:
+            raise ValueError("add_inflow: t_series and q_series must be non-empty and of equal length")
+        if g.size:
+            act = self.is_active
+            if (g < 0).any() or (g >= act.size).any() or (a < 0).any() or (a >= act.size).any():
+                raise ValueError("add_inflow: index out of range of the stored cells")
+            if act[g].any() or not act[a].all():
+                raise ValueError("add_inflow: ghost_idx must be ring cells and nbr_idx active cells")
+        dev = self.device
+        slot = self._slot
+        self._inflows.append(dict(
+            ghost=slot[torch.from_numpy(g).to(dev)].to(torch.int64).contiguous(),
+            nbr=slot[torch.from_numpy(a).to(dev)].to(torch.int64).contiguous(),
+            n=int(g.size), nx=nx_n, ny=ny_n, ds=float(ds),
+            t=torch.from_numpy(t.copy()).to(dev), q=torch.from_numpy(qs.copy()).to(dev)))
+        self._graph_cache.clear()
+        return self
+
+    def _inflow_args(self, f, q):
+        a = L.GswFlatInflowArgs()
+        a.abi_version = L.ABI_VERSION
+        a.dtype = L.F32
+        a.q0, a.q1, a.q2, a.bed = _ptr(q[0]), _ptr(q[1]), _ptr(q[2]), _ptr(self._b)
+        a.ghost_slot, a.nbr_slot, a.n = _ptr(f["ghost"]), _ptr(f["nbr"]), f["n"]
+        a.nx_n, a.ny_n, a.ds = f["nx"], f["ny"], f["ds"]
+        a.t_knots, a.q_knots, a.n_knots = _ptr(f["t"]), _ptr(f["q"]), int(f["t"].numel())
+        a.state = _ptr(self._state)
+        return a
 
     # ---------------------------------------------------------------- views
     def _canonical(self):
@@ -305,6 +368,7 @@ class CompressedSolver:
     def _args(self, src, dst, step=True):
         a = GswFlatArgs()
         a.abi_version = L.ABI_VERSION
+        a.dtype = L.F32
         a.brick_h, a.n_bricks = self.brick_h, self.n_bricks
         a.brick_ij, a.brick_nbr, a.flags = _ptr(self._bij), _ptr(self._bnbr), _ptr(self._flags)
         a.q0, a.q1, a.q2 = _ptr(src[0]), _ptr(src[1]), _ptr(src[2])
@@ -400,10 +464,12 @@ class CompressedSolver:
             for k in range(K):
                 L.call("gsw_dt_finalize", C.byref(p), _ptr(self._state), s)
                 src, dst = self._q[(start + k) % 2], self._q[(start + k + 1) % 2]
+                for f in self._inflows:             # inlet ghosts at t_n, before the step
+                    L.call("gsw_flat_inflow_apply", C.byref(self._inflow_args(f, src)), s)
                 L.call("gsw_flat_step", C.byref(self._args(src, dst)), s)
-            return 2 * K
+            return (2 + len(self._inflows)) * K
 
-        key = (K, start, float(t_end), p.dt_max, int(max_steps), self._rain_kind)
+        key = (K, start, float(t_end), p.dt_max, int(max_steps), self._rain_kind, len(self._inflows))
         if key not in self._graph_cache:
             self._graph_cache.clear()
             side = torch.cuda.Stream(device=self.device)

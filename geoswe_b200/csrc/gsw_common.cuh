@@ -59,6 +59,7 @@ __device__ __forceinline__ void loop_commit(GswLoopState* s) {
 //   dt_max, then the clip onto t_end                                      (solver.py:2992-2995)
 // The flat loop (compressed_solver.py:713-748, 2133-2197) is the same arithmetic with
 // eps_end = 1e-9, the rain limit folded into dt_max and dt = min(dt, t_end - t).
+// Mode 2 replays a recorded dt schedule (the adjoint's frozen forward); dt_log records one.
 __device__ __forceinline__ void dt_finalize_one(const GswDtParams& p, GswLoopState* s,
                                                 unsigned long long lam_bits) {
     loop_commit(s);
@@ -81,6 +82,15 @@ __device__ __forceinline__ void dt_finalize_one(const GswDtParams& p, GswLoopSta
     if (p.mode == 1) {
         dt = p.fixed_dt;
         s->lam_used = 0.0;
+    } else if (p.mode == 2) {                         // a recorded schedule, replayed as is
+        dt = p.dt_table[s->steps];
+        s->lam_used = 0.0;
+        s->dt = dt;
+        s->dt_f32 = (float)dt;
+        s->t_new = __dadd_rn(t, dt);
+        s->pending = 1;
+        s->lam_bits = 0ull;
+        return;
     } else {
         const double lam_in = __longlong_as_double((long long)lam_bits);
         if (!(lam_in <= 1.0e308)) {                   // NaN or Inf: the host raises FloatingPointError
@@ -107,6 +117,7 @@ __device__ __forceinline__ void dt_finalize_one(const GswDtParams& p, GswLoopSta
     s->t_new = __dadd_rn(t, dt);
     s->pending = 1;
     s->lam_bits = 0ull;                               // this step's kernels reduce lambda(next)
+    if (p.dt_log != nullptr) p.dt_log[s->steps] = dt;
 }
 
 }  // namespace gsw

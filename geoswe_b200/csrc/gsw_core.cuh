@@ -302,5 +302,17 @@ __device__ __forceinline__ unsigned long long lam_flat_bits(float h, float hu, f
     const float l = speed + c;
     return (unsigned long long)__double_as_longlong((double)l);
 }
+// The same rule in double (the flat tier is fp32 in the reference; fp64 runs exist for
+// the adjoint's finite-difference and autograd checks).
+__device__ __forceinline__ unsigned long long lam_flat_bits(double h, double hu, double hv, double g,
+                                                            double h_min, double h_min_cfl, bool linf) {
+    if (h != h) return 0x7ff8000000000000ull;
+    if (h < h_min) return 0ull;
+    const double hs = h > h_min_cfl ? h : h_min_cfl;
+    const double u = hu / hs, v = hv / hs;
+    const double c = sqrt(g * (h > 0.0 ? h : 0.0));
+    const double speed = linf ? fmax(fabs(u), fabs(v)) : sqrt(u * u + v * v);
+    return (unsigned long long)__double_as_longlong(speed + c);
+}
 
 }  // namespace gsw

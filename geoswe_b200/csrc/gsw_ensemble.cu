@@ -12,8 +12,8 @@
 
 namespace gsw {
 
-__device__ __forceinline__ FlatPhys member_phys(const GswMember& mb) {
-    FlatPhys ph;
+__device__ __forceinline__ FlatPhys<float> member_phys(const GswMember& mb) {
+    FlatPhys<float> ph;
     ph.inv_dx = mb.inv_dx; ph.inv_dy = mb.inv_dx;
     ph.half_dx = 0.5f * (1.0f / mb.inv_dx); ph.half_dy = ph.half_dx;
     ph.g = mb.g; ph.h_min = mb.h_min; ph.h_min_cfl = mb.h_min_cfl; ph.vcap = mb.vcap;
@@ -23,7 +23,7 @@ __device__ __forceinline__ FlatPhys member_phys(const GswMember& mb) {
     return ph;
 }
 
-__global__ void __launch_bounds__(256) ensemble_step_kernel(GswEnsembleArgs a, FlatMesh m) {
+__global__ void __launch_bounds__(256) ensemble_step_kernel(GswEnsembleArgs a, FlatMesh<float> m) {
     if (*a.all_done) return;
     const int lane = threadIdx.x;
     const int W = blockDim.y;
@@ -32,10 +32,10 @@ __global__ void __launch_bounds__(256) ensemble_step_kernel(GswEnsembleArgs a, F
         const GswLoopState* st = a.states + mi;
         if (st->done) continue;                                   // warp-uniform
         const GswMember& mb = a.members[mi];
-        const FlatPhys ph = member_phys(mb);
+        const FlatPhys<float> ph = member_phys(mb);
         const float dt = st->dt_f32;
         const float rate = (mb.rain_kind == GSW_RAIN_UNIFORM) ? mb.rain[st->rain_idx] : 0.0f;
-        unsigned long long lam = flat_brick<true>(m, ph, b, dt, rate, nullptr);
+        unsigned long long lam = flat_brick<float, true>(m, ph, b, dt, rate, nullptr);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const unsigned long long w = __shfl_xor_sync(0xffffffffu, lam, o);
@@ -141,7 +141,7 @@ extern "C" int gsw_ensemble_step(const GswEnsembleArgs* a, void* stream) {
     const int W = a->warps > 0 ? a->warps : 4;
     if (W < 1 || W > 8) return set_error(GSW_ERR_INVALID, "ensemble: warps must be in [1, 8]");
     const int grid = a->grid > 0 ? a->grid : 2 * sm_count();
-    FlatMesh m;
+    FlatMesh<float> m;
     m.q0 = a->q0; m.q1 = a->q1; m.q2 = a->q2;
     m.o0 = a->qn0; m.o1 = a->qn1; m.o2 = a->qn2;
     m.b = a->bed; m.flags = a->flags; m.ncls = a->n_cls; m.max_h = a->max_h;

@@ -127,6 +127,73 @@ __global__ void inflow_kernel(GswInflowArgs a) {
     }
 }
 
+// Flat-tier inlet (compressed_solver.py:2144-2167, dry seed :1559-1594). One block per
+// inlet; thread 0 evaluates Q, the depth sum and the dry seed, all threads write ghosts.
+template <typename T>
+__global__ void flat_inflow_kernel(GswFlatInflowArgs a) {
+    if (a.state->done) return;
+    T* q0 = (T*)a.q0; T* q1 = (T*)a.q1; T* q2 = (T*)a.q2;
+    const T* bed = (const T*)a.bed;
+    __shared__ double s_Q, s_sum, s_zmin, s_add, s_nlow;
+    __shared__ T s_seed;
+    __shared__ int s_wet, s_flat;
+    if (threadIdx.x == 0) {
+        s_Q = np_interp(a.state->t, a.t_knots, a.q_knots, a.n_knots);
+        const T sum = pairwise_sum<T>(q0, a.nbr_slot, 0, a.n);
+        s_sum = (double)sum;
+        s_wet = s_sum > 0.0;
+        if (!s_wet) {
+            T zmin = bed[a.nbr_slot[0]], zmax = zmin;
+            for (int k = 1; k < a.n; ++k) {
+                const T z = bed[a.nbr_slot[k]];
+                zmin = z < zmin ? z : zmin;
+                zmax = z > zmax ? z : zmax;
+            }
+            const double zlo = (double)zmin, zhi = (double)zmax;
+            const T seed = (T)__dadd_rn(zlo, __dmul_rn(0.10, __dsub_rn(zhi, zlo)));
+            int nlow = 0;
+            T hmax = (T)0;
+            for (int k = 0; k < a.n; ++k) {
+                const T z = bed[a.nbr_slot[k]];
+                nlow += (z <= zmin);
+                T hf = seed - z;
+                hf = hf > (T)0 ? hf : (T)0;
+                hmax = (k == 0 || hf > hmax) ? hf : hmax;
+            }
+            s_seed = seed;
+            s_zmin = zlo;
+            s_nlow = nlow > 0 ? (double)nlow : 1.0;
+            s_flat = !((double)hmax > 0.0);
+            s_add = 0.0;
+            if (s_flat) {
+                const double qc = __ddiv_rn(fabs(s_Q), __dmul_rn(s_nlow, a.ds));
+                s_add = pow(__ddiv_rn(__dmul_rn(qc, qc), 9.80665), 1.0 / 3.0);
+            }
+        }
+    }
+    __syncthreads();
+    const T qds = (T)__ddiv_rn(s_Q, a.ds);
+    for (int k = threadIdx.x; k < a.n; k += blockDim.x) {
+        const int64_t src = a.nbr_slot[k];
+        T hf, w;
+        if (s_wet) {
+            hf = q0[src];
+            w = hf / (T)s_sum;
+        } else {
+            const T z = bed[src];
+            hf = s_seed - z;
+            hf = hf > (T)0 ? hf : (T)0;
+            if (s_flat) hf = hf + (T)s_add;
+            w = ((double)z <= s_zmin) ? (T)__ddiv_rn(1.0, s_nlow) : (T)0;
+        }
+        const T qn = qds * w;
+        const int64_t go = a.ghost_slot[k];
+        q0[go] = hf;
+        q1[go] = qn * (T)a.nx_n;
+        q2[go] = qn * (T)a.ny_n;
+    }
+}
+
 }  // namespace gsw
 
 using namespace gsw;
@@ -142,4 +209,17 @@ extern "C" int gsw_inflow_apply(const GswInflowArgs* a, void* stream) {
     else if (a->dtype == GSW_F64) inflow_kernel<double><<<1, 256, 0, s>>>(*a);
     else return set_error(GSW_ERR_INVALID, "inflow: bad dtype");
     return check_launch("inflow");
+}
+
+extern "C" int gsw_flat_inflow_apply(const GswFlatInflowArgs* a, void* stream) {
+    GSW_CHECK_ABI(a);
+    if (a->n <= 0) return GSW_OK;
+    if (!a->ghost_slot || !a->nbr_slot || !a->q0 || !a->q1 || !a->q2 || !a->bed || !a->t_knots ||
+        !a->q_knots || a->n_knots < 1 || !a->state || !(a->ds > 0.0))
+        return set_error(GSW_ERR_INVALID, "flat inflow: null pointer, empty hydrograph or ds <= 0");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (a->dtype == GSW_F32) flat_inflow_kernel<float><<<1, 256, 0, s>>>(*a);
+    else if (a->dtype == GSW_F64) flat_inflow_kernel<double><<<1, 256, 0, s>>>(*a);
+    else return set_error(GSW_ERR_INVALID, "flat inflow: bad dtype");
+    return check_launch("flat_inflow");
 }

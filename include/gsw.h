@@ -111,7 +111,7 @@ typedef struct GswLoopState {
  * The loop stops (done = 1) when !(t < t_end - eps_end) or steps >= max_steps. */
 typedef struct GswDtParams {
     uint32_t abi_version;
-    int32_t  mode;        /* 0: CFL rule above; 1: fixed dt (fixed_dt) */
+    int32_t  mode;        /* 0: CFL rule above; 1: fixed dt (fixed_dt); 2: dt_table[steps] */
     double   cfl_dmin;    /* cfl * min(dx, dy), computed by the caller in fp64 */
     double   lam_floor;   /* sqrt(g * h_floor), computed by the caller */
     double   t_end;
@@ -123,6 +123,8 @@ typedef struct GswDtParams {
     const double* rain_lim; /* device, per-frame rain step limit (<= 0: none) or NULL */
     int32_t  n_rain;
     int32_t  clip_flat;     /* 0: dense clip (t + dt > t_end -> t_end - t); 1: flat dt = min(dt, t_end - t) */
+    const double* dt_table; /* mode 2: dt = dt_table[steps] (a recorded schedule, replayed exactly) */
+    double*  dt_log;        /* non-NULL: dt_log[steps] = the dt this step takes */
 } GswDtParams;
 
 /* ------------------------------------------------------------------------- */
@@ -246,28 +248,55 @@ GSW_API int gsw_inflow_apply(const GswInflowArgs* a, void* stream);
 
 typedef struct GswFlatArgs {
     uint32_t abi_version;
+    int32_t  dtype;            /* GSW_F32 or GSW_F64: q*, qn*, bed, rain, n_tab and max_h */
     int32_t  brick_h;          /* rows per brick (>= 2) */
+    int32_t  warps;            /* warps per block (0: 4) */
     int64_t  n_bricks;         /* brick n_bricks is the all-zero brick (a missing neighbour) */
     const int32_t* brick_ij;   /* (n_bricks, 2) brick row, brick column */
     const int32_t* brick_nbr;  /* (n_bricks, 4) up, down, left, right */
     const uint8_t* flags;      /* per slot: GSW_SLOT_STORED | GSW_SLOT_ACTIVE */
-    const float* q0; const float* q1; const float* q2;   /* state in, slot-indexed */
-    float* qn0; float* qn1; float* qn2;                  /* state out (step) / residual (rhs) */
-    const float* bed;
-    float    inv_dx, inv_dy, g, h_min, h_min_cfl;
+    const void* q0; const void* q1; const void* q2;   /* state in, slot-indexed */
+    void* qn0; void* qn1; void* qn2;                  /* state out (step) / residual (rhs) */
+    const void* bed;
+    double   inv_dx, inv_dy, g, h_min, h_min_cfl;     /* rounded to dtype by the kernels */
     int32_t  linf;             /* 1: CFL norm max(|u|,|v|); 0: sqrt(u^2+v^2) */
     /* step only */
+    int32_t  rain_kind;        /* GSW_RAIN_NONE / UNIFORM / GRIDDED */
     const GswLoopState* state;
     uint64_t* lam_target;
-    int32_t  rain_kind;        /* GSW_RAIN_NONE / UNIFORM / GRIDDED */
-    const float* rain;         /* uniform: rates[n_frames]; gridded: frames[n_frames][nx][ny] */
+    const void* rain;          /* uniform: rates[n_frames]; gridded: frames[n_frames][nx][ny] */
     int32_t  ngh, nx, ny;      /* dense padding and interior extents (gridded rain index) */
-    const uint8_t* n_cls; const float* n_tab; int32_t n_tab_len;
-    float    vcap;
+    int32_t  n_tab_len;
+    const uint8_t* n_cls; const void* n_tab;
+    double   vcap;
     int32_t  quadratic, keep_h;
-    float*   max_h;            /* slot-indexed, or NULL */
-    int32_t  warps;
+    void*    max_h;            /* slot-indexed, or NULL */
 } GswFlatArgs;
+
+/* Discharge inlet of the compressed mesh: one ghost (ring) slot per inlet cell, next to
+ * its active neighbour. Per step, at state->t: Q = np.interp(t, t_knots, q_knots);
+ * wet inlet (sum of the neighbours' depths > 0): ghost h = neighbour h, unit discharge
+ * (float)(Q/ds) * h/sum; dry inlet: depth seeded from the bed relief of the neighbours
+ * (10 %), plus the critical depth where that relief is flat, flow in the lowest cells.
+ * Ghost hu, hv = unit discharge * inward normal. Replaces the flat loop's inlet block
+ * and its dry seed (geoswe/compressed_solver.py:2144-2167, 1559-1594). The depth sum
+ * is taken in NumPy's pairwise order (bitwise with a NumPy sum; the reference's CuPy
+ * reduction may order a multi-cell sum differently, so results can differ there in
+ * the last bit of the weights). */
+typedef struct GswFlatInflowArgs {
+    uint32_t abi_version;
+    int32_t  dtype;               /* GSW_F32 or GSW_F64 */
+    void* q0; void* q1; void* q2; /* brick storage, written at the ghost slots */
+    const void* bed;
+    const int64_t* ghost_slot;    /* n ghost slots */
+    const int64_t* nbr_slot;      /* n active neighbour slots */
+    int32_t  n;
+    int32_t  n_knots;
+    double   nx_n, ny_n, ds;      /* inward unit normal (axis-aligned) and cell width */
+    const double* t_knots; const double* q_knots;
+    const GswLoopState* state;    /* Q is taken at state->t; nothing is written when done */
+} GswFlatInflowArgs;
+GSW_API int gsw_flat_inflow_apply(const GswFlatInflowArgs* a, void* stream);
 
 /* Fused step on the compressed mesh: active cells get the SRM-HLLC residual, rain,
  * Euler, wet/dry and Manning (table); stored ring cells are carried unchanged.

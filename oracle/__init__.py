@@ -363,6 +363,43 @@ class OracleFlat:
         self.t = 0.0
         self.nsteps = 0
         self._lam = None
+        self.inflows = []
+
+    def add_inflow(self, ghost_idx, nbr_idx, normal, ds, t_series, q_series):
+        """A discharge inlet with the reference's dry seed (compressed_solver.py:1559-1594)."""
+        a = np.asarray(nbr_idx, np.int64)
+        zb = self.b[a]
+        zmin, zmax = float(zb.min()), float(zb.max())
+        h_dry = np.maximum(np.float32(zmin + 0.10 * (zmax - zmin)) - zb, np.float32(0.0))
+        low = zb <= np.float32(zmin)
+        nlow = float(low.sum()) or 1.0
+        self.inflows.append(dict(g=np.asarray(ghost_idx, np.int64), a=a, nx=float(normal[0]),
+                                 ny=float(normal[1]), ds=float(ds), t=np.asarray(t_series, np.float64),
+                                 q=np.asarray(q_series, np.float64), h_dry=h_dry.astype(np.float32),
+                                 nlow=nlow, flat=bool(float(h_dry.max()) <= 0.0),
+                                 w_dry=np.where(low, np.float32(1.0 / nlow), np.float32(0.0))))
+        return self
+
+    def _apply_inflows(self):
+        """The flat loop's inlet block (compressed_solver.py:2144-2167), NumPy sums."""
+        q0, q1, q2 = self.q
+        for f in self.inflows:
+            Q = float(np.interp(self.t, f["t"], f["q"]))
+            h_a = q0[f["a"]]
+            ssum = float(h_a.sum())
+            if ssum > 0.0:
+                w = h_a / np.float32(ssum)
+                h_face = h_a
+            else:
+                h_face = f["h_dry"]
+                if f["flat"]:
+                    qc = abs(Q) / (f["nlow"] * f["ds"])
+                    h_face = h_face + np.float32((qc * qc / 9.80665) ** (1.0 / 3.0))
+                w = f["w_dry"]
+            qn = (np.float32(Q / f["ds"]) * w).astype(np.float32)
+            q0[f["g"]] = np.asarray(h_face, np.float32)
+            q1[f["g"]] = (qn * np.float32(f["nx"])).astype(np.float32)
+            q2[f["g"]] = (qn * np.float32(f["ny"])).astype(np.float32)
 
     def _lammax(self):
         q = self.q
@@ -403,6 +440,7 @@ class OracleFlat:
             if not (lam == lam and lam < float("inf")):
                 raise FloatingPointError("non-finite max wave speed")
             dt = min(self.dt_from_lam(lam), t_end - self.t)
+            self._apply_inflows()
             self.step(dt)
             steps += 1
         return steps

@@ -107,3 +107,46 @@ def test_dense_masked_run_equals_flat_run():
     hd = sd.depth()
     hf = cs.depth()
     assert same(hf[mask], hd[mask])
+
+
+def _inlet_pairs(cs, n_cells):
+    """The first `n_cells` ghost/active pairs whose active neighbour lies at +i (inward
+    normal (1, 0)), in canonical order."""
+    g, a = cs.ghost_boundary_pairs()
+    ij = cs.ij_active
+    d = ij[a] - ij[g]
+    sel = np.nonzero((d[:, 0] == 1) & (d[:, 1] == 0))[0][:n_cells]
+    return g[sel], a[sel]
+
+
+@pytest.mark.parametrize("n_cells", [1, 5])
+def test_flat_inflow_run_bitwise_oracle(n_cells):
+    """A discharge inlet on the compressed mesh (dry start: relief seed and critical
+    depth, then the depth-weighted split) against the oracle's restatement of the flat
+    loop's inlet block."""
+    from geoswe_b200.compressed import CompressedSolver
+    from geoswe_b200.synthetic import fractal_bed
+    nx, ny, dx = 64, 70, 3.0
+    z = fractal_bed(nx, ny, dx, seed=9).astype(np.float32)
+    mask = z < np.percentile(z, 70)
+    mask[:3, :] = mask[-3:, :] = False
+    mask[:, :3] = mask[:, -3:] = False
+    s = _dense(np.zeros((3, nx, ny), np.float32), z, mask, dx=dx, friction="manning", manning_n=0.035)
+    cs = CompressedSolver.from_dense(s)
+    g, a = _inlet_pairs(cs, n_cells)
+    assert g.size == n_cells
+    t_k = [0.0, 300.0, 900.0, 1800.0]
+    q_k = [0.0, 12.0, 20.0, 4.0]
+    cs.add_inflow(g, a, (1.0, 0.0), dx, t_k, q_k)
+    q = [cs.flat(c).cpu().numpy() for c in range(3)]
+    b = cs._b[cs._slot].cpu().numpy()
+    o = oracle.OracleFlat(cs.nbr, cs.is_active, q, b, dx, ntab=[np.float32(0.035)])
+    o.add_inflow(g, a, (1.0, 0.0), dx, t_k, q_k)
+    n_g = cs.run(t_end=700.0)
+    n_o = o.run(t_end=700.0)
+    assert n_g == n_o and n_g > 20
+    assert cs.t == o.t
+    h = cs.flat(0).cpu().numpy()
+    assert h[cs.is_active != 0].sum() > 0          # water entered
+    for c in range(3):
+        assert same(cs.flat(c).cpu().numpy(), o.q[c]), c
