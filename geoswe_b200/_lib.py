@@ -127,6 +127,7 @@ _PROTOS = {
     "gsw_ensemble_lammax": [C.POINTER(GswEnsembleArgs), vp],
     "gsw_ensemble_finalize": [C.POINTER(GswEnsembleArgs), vp],
     "gsw_ensemble_step": [C.POINTER(GswEnsembleArgs), vp],
+    "gsw_ensemble_step_static": [C.POINTER(GswEnsembleArgs), vp],
 }
 
 

@@ -9,6 +9,7 @@
 // their own CFL dt with no grid-wide barrier and no host round trip; a member that
 // reaches its end time drops out while the others continue.
 #include "gsw_flat_brick.cuh"
+#include <mutex>
 
 namespace gsw {
 
@@ -148,4 +149,44 @@ extern "C" int gsw_ensemble_step(const GswEnsembleArgs* a, void* stream) {
     m.bij = a->brick_ij; m.bnbr = a->brick_nbr; m.nb = a->n_bricks; m.bh = a->brick_h;
     ensemble_step_kernel<<<grid, dim3(32, W), 0, (cudaStream_t)stream>>>(*a, m);
     return check_launch("ensemble_step");
+}
+
+// ---------------------------------------------------------------------------
+// gsw_ensemble_step_static: the same launch with the ticket counter in library memory.
+static __device__ __align__(256) unsigned int g_ens_static_scratch[GSW_ENS_STATIC_SCRATCH_WORDS];
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+unsigned int* g_static_ptr[kMaxDevices] = {};
+}  // namespace
+
+extern "C" int gsw_ensemble_step_static(const GswEnsembleArgs* a, void* stream) {
+    GSW_CHECK_ABI(a);
+    if (GSW_ENS_SCRATCH_WORDS > GSW_ENS_STATIC_SCRATCH_WORDS)
+        return set_error(GSW_ERR_RANGE, "ensemble step (static scratch): needs %d words, the static array "
+                         "holds %d", GSW_ENS_SCRATCH_WORDS, GSW_ENS_STATIC_SCRATCH_WORDS);
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return set_error(GSW_ERR_CUDA, "ensemble step (static scratch): no device");
+    if (dev < 0 || dev >= kMaxDevices)
+        return set_error(GSW_ERR_RANGE, "ensemble step (static scratch): device %d >= %d", dev, kMaxDevices);
+    unsigned int* ptr = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        if (g_static_ptr[dev] == nullptr) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_ens_static_scratch);
+            if (e != cudaSuccess || p == nullptr)
+                return set_error(GSW_ERR_CUDA, "ensemble step (static scratch): cudaGetSymbolAddress: %s",
+                                 cudaGetErrorString(e));
+            e = cudaMemsetAsync(p, 0, sizeof(g_ens_static_scratch), (cudaStream_t)stream);
+            if (e != cudaSuccess)
+                return set_error(GSW_ERR_CUDA, "ensemble step (static scratch): clearing the ticket: %s",
+                                 cudaGetErrorString(e));
+            g_static_ptr[dev] = (unsigned int*)p;
+        }
+        ptr = g_static_ptr[dev];
+    }
+    GswEnsembleArgs b = *a;
+    b.scratch = ptr;
+    return gsw_ensemble_step(&b, stream);
 }

@@ -371,6 +371,21 @@ GSW_API int gsw_ensemble_finalize(const GswEnsembleArgs* a, void* stream);
  * run bit for bit. */
 GSW_API int gsw_ensemble_step(const GswEnsembleArgs* a, void* stream);
 
+/* gsw_ensemble_step without caller scratch. No counterpart in the reference (its
+ * scenarios run one after another, with no device scratch).
+ * The step's scratch is its block ticket counter: GSW_ENS_SCRATCH_WORDS uint32 words,
+ * zero before a launch and left at zero by it. This entry point keeps those words in a
+ * static, 256-byte aligned device array of the library (GSW_ENS_STATIC_SCRATCH_WORDS
+ * words per device) and ignores a->scratch; a requirement above that size is refused
+ * with GSW_ERR_RANGE. It allocates nothing: on the first call on a device it looks the
+ * array up (cudaGetSymbolAddress) and zeroes it on `stream`, so make that first call
+ * outside any stream capture. The array is shared by all callers on a device: calls
+ * whose launches overlap in time (other streams, other threads) race on the ticket
+ * counter and must be serialised by the caller. */
+#define GSW_ENS_SCRATCH_WORDS        1
+#define GSW_ENS_STATIC_SCRATCH_WORDS 64
+GSW_API int gsw_ensemble_step_static(const GswEnsembleArgs* a, void* stream);
+
 /* ------------------------------------------------------------------------- */
 /* Loop control.                                                              */
 /* ------------------------------------------------------------------------- */
