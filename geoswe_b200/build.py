@@ -58,8 +58,8 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> Path:
         obj = build_dir / (src.stem + ".o")
         cmd = [nvcc, *ARCH, *NVCC_FLAGS, *extra, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
         if src.suffix == ".cpp":
-            cmd = [nvcc, "-x", "c++", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
-                   "-fvisibility=hidden", *extra, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc, "-x", "c++", "-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+                   "-Xcompiler", "-fvisibility=hidden", *extra, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -111,11 +111,13 @@ def test_dense_masked_run_equals_flat_run():
 
 def _inlet_pairs(cs, n_cells):
     """The first `n_cells` ghost/active pairs whose active neighbour lies at +i (inward
-    normal (1, 0)), in canonical order."""
+    normal (1, 0)) and whose ghost bed is not below the neighbour's (an inlet the water
+    can leave), in canonical order."""
     g, a = cs.ghost_boundary_pairs()
     ij = cs.ij_active
+    b = cs._b[cs._slot].cpu().numpy()
     d = ij[a] - ij[g]
-    sel = np.nonzero((d[:, 0] == 1) & (d[:, 1] == 0))[0][:n_cells]
+    sel = np.nonzero((d[:, 0] == 1) & (d[:, 1] == 0) & (b[g] >= b[a]))[0][:n_cells]
     return g[sel], a[sel]
 
 
