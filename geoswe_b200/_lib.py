@@ -92,6 +92,18 @@ class GswFlatInflowArgs(C.Structure):
                 ("ny_n", f64), ("ds", f64), ("t_knots", vp), ("q_knots", vp), ("state", vp)]
 
 
+class GswFlatAdjArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("reserved0", i32), ("f", GswFlatArgs),
+                ("lam_in0", vp), ("lam_in1", vp), ("lam_in2", vp), ("lam_out0", vp), ("lam_out1", vp),
+                ("lam_out2", vp), ("rbar0", vp), ("rbar1", vp), ("rbar2", vp), ("n_bar", vp), ("rate_bar", vp)]
+
+
+class GswGaugeArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("dtype", i32), ("q0", vp), ("slots", vp), ("n", i32), ("offset", i32),
+                ("first", i64), ("count", i64), ("series", vp), ("target", vp), ("weight", f64), ("lam0", vp),
+                ("state", vp)]
+
+
 class GswMember(C.Structure):
     _fields_ = [("dt", GswDtParams), ("inv_dx", C.c_float), ("g", C.c_float), ("h_min", C.c_float),
                 ("h_min_cfl", C.c_float), ("vcap", C.c_float), ("linf", i32), ("quadratic", i32),
@@ -118,6 +130,10 @@ _PROTOS = {
     "gsw_dt_finalize": [C.POINTER(GswDtParams), vp, vp],
     "gsw_loop_commit": [vp, vp],
     "gsw_flat_inflow_apply": [C.POINTER(GswFlatInflowArgs), vp],
+    "gsw_adj_flat_step": [C.POINTER(GswFlatAdjArgs), vp],
+    "gsw_adj_flat_inflow": [C.POINTER(GswFlatInflowArgs), vp, vp, vp, vp, vp],
+    "gsw_gauge_record": [C.POINTER(GswGaugeArgs), vp],
+    "gsw_gauge_adjoint": [C.POINTER(GswGaugeArgs), vp],
     "gsw_flat_step": [C.POINTER(GswFlatArgs), vp],
     "gsw_flat_rhs": [C.POINTER(GswFlatArgs), vp],
     "gsw_flat_lammax": [C.POINTER(GswFlatArgs), vp, vp],

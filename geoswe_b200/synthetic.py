@@ -167,3 +167,49 @@ def ensemble_specs(n_members=64, seed=0, side_min=256, side_max=4096):
                         peak=float(rng.uniform(20.0, 120.0)), t_peak=float(rng.uniform(0.5, 3.0)) * 3600.0,
                         scale=float(rng.uniform(0.7, 1.3))))
     return out
+
+
+def calibration_case(n=2048, *, seed=0, dx=3.0, frac=0.7, pond=0.3, n_gauges=32, n_knots=16,
+                     peak_q=20.0, t_peak=900.0, t_knots_end=3600.0, rain_mm_h=40.0, brick_h=16,
+                     device="cuda"):
+    """The Manning / rain / inflow calibration case on the compressed mesh: an n x n
+    fractal bed (as rain_on_terrain), 4 Voronoi Manning classes, active set z < the
+    `frac` quantile (three border rows/columns left out), a pond filling the lowest
+    `pond` fraction of the bed to a flat surface at rest, uniform rain of `rain_mm_h`
+    times the rain scale, and one point inlet (a single ghost/active pair on the mask
+    edge whose ghost bed is not below its neighbour) with an `n_knots` hydrograph
+    rising linearly to `peak_q` m^3/s at `t_peak` and falling back to 0 at 2 t_peak.
+    Gauges: `n_gauges` seeded active cells among the lower half of the active bed.
+    Returns a dict of the CompressedSolver and the pieces FlatAdjoint takes."""
+    from . import Config, Mesh2D, Solver2D
+    from .adjoint import Inlet
+    from .compressed import CompressedSolver
+    z = fractal_bed(n, n, dx, seed=seed).astype(np.float32)
+    cls = voronoi_classes_fast(n, n, seed=seed) if n * n > (1 << 20) else voronoi_classes(n, n, seed=seed)
+    mask = z < np.quantile(z, frac)
+    mask[:3, :] = mask[-3:, :] = False
+    mask[:, :3] = mask[:, -3:] = False
+    eta0 = np.float32(np.quantile(z, pond))
+    h0 = np.where(mask, np.maximum(eta0 - z, 0.0), 0.0).astype(np.float32)
+    q0 = np.stack([h0, np.zeros_like(h0), np.zeros_like(h0)])
+    s = Solver2D(Mesh2D(nx=n, ny=n, dx=dx, dy=dx, ngh=2), Config(bc_x="fall", bc_y="fall", friction="manning"),
+                 q0, z, device=device, track_max_depth=False)
+    s.set_inside_mask(mask)
+    s.set_manning_table(np.pad(cls, 2, mode="edge"), MANNING_CLASSES)
+    cs = CompressedSolver.from_dense(s, brick_h=brick_h)
+    del s
+    rng = np.random.default_rng(seed + 101)
+    g, a = cs.ghost_boundary_pairs()
+    ij = cs.ij_active
+    b = cs._b[cs._slot].cpu().numpy()
+    ok = np.nonzero(b[g] >= b[a])[0]
+    k = int(ok[rng.integers(ok.size)])
+    d = ij[a[k]] - ij[g[k]]
+    inlet_t = np.linspace(0.0, t_knots_end, n_knots)
+    inlet_q = np.maximum(0.0, peak_q * (1.0 - np.abs(inlet_t - t_peak) / t_peak))
+    inlet = Inlet(ghost=g[k:k + 1], nbr=a[k:k + 1], normal=(float(d[0]), float(d[1])), ds=dx, t_knots=inlet_t)
+    act = np.nonzero(cs.is_active != 0)[0]
+    low = act[b[act] <= np.quantile(b[act], 0.5)]
+    gauges = np.sort(rng.choice(low, size=min(n_gauges, low.size), replace=False))
+    return dict(cs=cs, gauges=gauges, inlet=inlet, knots=inlet_q, rain_times=np.array([0.0]),
+                rain_base=np.array([rain_mm_h / 3.6e6]), n_tab=MANNING_CLASSES.copy())

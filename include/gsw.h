@@ -320,6 +320,50 @@ GSW_API int gsw_bricks_build(const uint8_t* stored, int nxp, int nyp, int brick_
                              int64_t* n_bricks, int32_t* brick_ij, int32_t* brick_nbr);
 
 /* ------------------------------------------------------------------------- */
+/* Adjoint of the compressed-mesh step. No counterpart in the reference, which */
+/* has no derivatives; it reverses gsw_flat_step (+ gsw_flat_inflow_apply)     */
+/* for calibration of Manning's n, the rain scale and inlet hydrographs.       */
+/* ------------------------------------------------------------------------- */
+typedef struct GswFlatAdjArgs {
+    uint32_t abi_version;
+    int32_t  reserved0;
+    GswFlatArgs f;     /* the step being reversed: q* = the state it read (inlet ghosts written),
+                          state = its dt, rain frame and step index (steps); qn*, max_h unused */
+    const void* lam_in0; const void* lam_in1; const void* lam_in2;   /* adjoint of the new state */
+    void* lam_out0; void* lam_out1; void* lam_out2;                   /* adjoint of the old state (written) */
+    void* rbar0; void* rbar1; void* rbar2;   /* scratch of the residual adjoints, slot-indexed; must be
+                                                zero on every slot that is not stored (and the zero brick) */
+    double*  n_bar;    /* += dL/dn per Manning class (f.n_tab_len <= 256) */
+    double*  rate_bar; /* uniform rain: rate_bar[state->steps] += dL/d(rate of this step), or NULL */
+} GswFlatAdjArgs;
+/* lam_out = (d step / d q)^T lam_in with dt, the rain frame and every branch of the
+ * forward step held fixed; n_bar and rate_bar accumulate. Two launches. */
+GSW_API int gsw_adj_flat_step(const GswFlatAdjArgs* a, void* stream);
+/* Reverse of gsw_flat_inflow_apply for the same state and time: the ghost slots'
+ * adjoint (lam*) moves to the inlet's active cells and to q_bar[state->steps]
+ * (dL/dQ of this step); the ghost slots' adjoint is then zeroed. */
+GSW_API int gsw_adj_flat_inflow(const GswFlatInflowArgs* a, void* lam0, void* lam1, void* lam2,
+                                double* q_bar, void* stream);
+
+/* Gauge series: depth at n slots, recorded per step, and the adjoint of a squared misfit. */
+typedef struct GswGaugeArgs {
+    uint32_t abi_version;
+    int32_t  dtype;
+    const void* q0;          /* depth, slot-indexed */
+    const int64_t* slots;
+    int32_t  n;
+    int32_t  offset;         /* row = state->steps + offset - first (state NULL: steps = 0) */
+    int64_t  first, count;   /* rows [0, count) are kept */
+    double*  series;         /* record: (count, n) */
+    const double* target;    /* adjoint: (count, n) */
+    double   weight;         /* adjoint: lam0[slot] += weight * 2 * (depth - target) */
+    void*    lam0;
+    const GswLoopState* state;
+} GswGaugeArgs;
+GSW_API int gsw_gauge_record(const GswGaugeArgs* a, void* stream);
+GSW_API int gsw_gauge_adjoint(const GswGaugeArgs* a, void* stream);
+
+/* ------------------------------------------------------------------------- */
 /* Batched ensemble: many compressed meshes advanced by one kernel per step.  */
 /* No counterpart in the reference, which runs scenarios one after another    */
 /* (a Python loop over CompressedSolver.run, geoswe/compressed_solver.py:     */
