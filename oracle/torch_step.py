@@ -197,7 +197,7 @@ def inflow(q, b, ghost, nbr, normal, ds, t, t_knots, knots):
     Q = interp_row(t, t_knots) @ knots
     h_a = q[0, nbr]
     ssum = h_a.sum()
-    if float(ssum) > 0.0:
+    if float(ssum.detach()) > 0.0:
         w = h_a / ssum
         h_face = h_a
     else:
@@ -208,7 +208,9 @@ def inflow(q, b, ghost, nbr, normal, ds, t, t_knots, knots):
         nlow = float(low.sum()) or 1.0
         if float(h_face.max()) <= 0.0:
             qc = Q.abs() / (nlow * ds)
-            h_face = h_face + (qc * qc / 9.80665) ** (1.0 / 3.0)
+            pos = qc > 0
+            qs = _w(pos, qc, torch.ones_like(qc))
+            h_face = h_face + _w(pos, (qs * qs / 9.80665) ** (1.0 / 3.0), torch.zeros_like(qc))
         w = _w(low, torch.full_like(zb, 1.0 / nlow), torch.zeros_like(zb))
     qn = (Q / ds) * w
     out = q.clone()
