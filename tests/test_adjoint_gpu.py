@@ -18,6 +18,7 @@ def _problem(n, N, window, n_gauges, seed=3, snapshots=6):
     from geoswe_b200.synthetic import calibration_case
     case = calibration_case(n, seed=seed, n_gauges=n_gauges, t_peak=4.0, t_knots_end=16.0, rain_mm_h=80.0)
     cs = case["cs"]
+    case["gauges"] = np.union1d(case["gauges"], case["inlet"].nbr)   # a gauge the inlet reaches
     prob = FlatAdjoint(cs, gauges=case["gauges"], n_steps=N, window=window, snapshots=snapshots,
                        dtype="float64", rain_times=case["rain_times"], rain_base=case["rain_base"],
                        inlet=case["inlet"])
@@ -52,7 +53,7 @@ def _torch_grads(case, prob, target, wrt_state=False):
                                    rain_base=prob.rain_base, gauges=case["gauges"], window=prob.K,
                                    target=target, inlet=inlet)
     loss.backward()
-    return float(loss), ntab.grad.numpy(), float(s.grad), knots.grad.numpy(), (q0.grad if wrt_state else None)
+    return float(loss.detach()), ntab.grad.numpy(), float(s.grad), knots.grad.numpy(), (q0.grad if wrt_state else None)
 
 
 def _rel(a, b):
@@ -126,4 +127,5 @@ def test_rollout_gradients_autograd_and_finite_differences():
             checked += 1
         else:
             assert abs(g_adj) <= 1e-5 * scale, (name, j, g_adj, g_fd)
-    assert checked >= 6
+    print(f"\nfinite-difference checks: {checked} of {len(fd)} parameters (others below 1e-6 of the largest)")
+    assert checked >= 8
