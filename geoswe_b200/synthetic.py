@@ -171,14 +171,15 @@ def ensemble_specs(n_members=64, seed=0, side_min=256, side_max=4096):
 
 def calibration_case(n=2048, *, seed=0, dx=3.0, frac=0.7, pond=0.3, n_gauges=32, n_knots=16,
                      peak_q=20.0, t_peak=900.0, t_knots_end=3600.0, rain_mm_h=40.0, brick_h=16,
-                     device="cuda"):
+                     base_q=0.0, device="cuda"):
     """The Manning / rain / inflow calibration case on the compressed mesh: an n x n
     fractal bed (as rain_on_terrain), 4 Voronoi Manning classes, active set z < the
     `frac` quantile (three border rows/columns left out), a pond filling the lowest
     `pond` fraction of the bed to a flat surface at rest, uniform rain of `rain_mm_h`
     times the rain scale, and one point inlet (a single ghost/active pair on the mask
     edge whose ghost bed is not below its neighbour) with an `n_knots` hydrograph
-    rising linearly to `peak_q` m^3/s at `t_peak` and falling back to 0 at 2 t_peak.
+    rising linearly to `peak_q` m^3/s at `t_peak` and falling back to 0 at 2 t_peak,
+    never below `base_q`.
     Gauges: `n_gauges` seeded active cells among the lower half of the active bed.
     Returns a dict of the CompressedSolver and the pieces FlatAdjoint takes."""
     from . import Config, Mesh2D, Solver2D
@@ -206,7 +207,7 @@ def calibration_case(n=2048, *, seed=0, dx=3.0, frac=0.7, pond=0.3, n_gauges=32,
     k = int(ok[rng.integers(ok.size)])
     d = ij[a[k]] - ij[g[k]]
     inlet_t = np.linspace(0.0, t_knots_end, n_knots)
-    inlet_q = np.maximum(0.0, peak_q * (1.0 - np.abs(inlet_t - t_peak) / t_peak))
+    inlet_q = np.maximum(base_q, peak_q * (1.0 - np.abs(inlet_t - t_peak) / t_peak))
     inlet = Inlet(ghost=g[k:k + 1], nbr=a[k:k + 1], normal=(float(d[0]), float(d[1])), ds=dx, t_knots=inlet_t)
     act = np.nonzero(cs.is_active != 0)[0]
     low = act[b[act] <= np.quantile(b[act], 0.5)]

@@ -3,7 +3,9 @@ torch.autograd through the plain-PyTorch restatement of the same step
 (oracle/torch_step.py) and against central finite differences of the GPU forward with
 the recorded dt schedule replayed (dt frozen, as the adjoint holds it). The loss is a
 squared gauge misfit against a run with perturbed parameters (Manning n x 1.2, rain
-x 0.9); parameters: the 4 class n values, the rain scale, the inlet's hydrograph knots."""
+x 0.9); parameters: the 4 class n values, the rain scale, the inlet's hydrograph knots.
+The hydrograph keeps a base flow: at Q = 0 a dry inlet's critical depth, |Q|^(2/3), has
+a cusp where no derivative exists (the adjoint and autograd both take 0 there)."""
 import numpy as np
 import pytest
 
@@ -16,7 +18,8 @@ from oracle import torch_step  # noqa: E402
 def _problem(n, N, window, n_gauges, seed=3, snapshots=6):
     from geoswe_b200.adjoint import FlatAdjoint
     from geoswe_b200.synthetic import calibration_case
-    case = calibration_case(n, seed=seed, n_gauges=n_gauges, t_peak=4.0, t_knots_end=16.0, rain_mm_h=80.0)
+    case = calibration_case(n, seed=seed, n_gauges=n_gauges, t_peak=4.0, t_knots_end=16.0, rain_mm_h=80.0,
+                           base_q=1.0)
     cs = case["cs"]
     case["gauges"] = np.union1d(case["gauges"], case["inlet"].nbr)   # a gauge the inlet reaches
     prob = FlatAdjoint(cs, gauges=case["gauges"], n_steps=N, window=window, snapshots=snapshots,
