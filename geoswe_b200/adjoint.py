@@ -392,8 +392,10 @@ class FlatAdjoint:
         return float((d * d).sum())
 
     # ----------------------------------------------------------------- reverse
-    def gradients(self, target):
-        """Reverse sweep after forward(): (dL/dn_tab (C,), dL/drain_scale, dL/dknots or None)."""
+    def gradients(self, target, *, timing=False):
+        """Reverse sweep after forward(): (dL/dn_tab (C,), dL/drain_scale, dL/dknots or None).
+        With `timing`, CUDA events bracket every reverse step and every recomputation;
+        their totals (ms) land in self.timing."""
         if not (self._schedule and self._ready):
             raise RuntimeError("gradients() needs a forward() pass that kept its snapshots")
         dev = self.dev
@@ -427,20 +429,39 @@ class FlatAdjoint:
         def free(n):
             self._snaps.pop(n, None)
 
+        ev_rev, ev_adv = [], []
+
+        def events():
+            e = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            e[0].record()
+            return e
+
         def advance(n0, n1):
+            e = events() if timing else None
             self._set_state_n(n0)
             for _ in range(n0, n1):
                 self._one_step(work[self._cur], work[1 - self._cur], p2, False)
                 self._cur = 1 - self._cur
+            if timing:
+                e[1].record()
+                ev_adv.append(e)
 
         def reverse(n):
+            e = events() if timing else None
             self._reverse_step(n, work[self._cur], p2)
+            if timing:
+                e[1].record()
+                ev_rev.append(e)
 
         tv = Treeverse(self.N, self.S, store, restore, advance, free, reverse, stored=self._snaps.keys())
         tv.run()
         self.recompute_steps = tv.forward_steps
         self.max_snapshots = tv.max_live
         torch.cuda.current_stream().synchronize()
+        if timing:
+            self.timing = dict(reverse_ms=sum(a.elapsed_time(b) for a, b in ev_rev), reverse_steps=len(ev_rev),
+                               recompute_ms=sum(a.elapsed_time(b) for a, b in ev_adv),
+                               recompute_steps=tv.forward_steps)
         self._ready = False                      # snapshots used up, final state overwritten
         g_n = self.n_bar.clone()
         idx = np.clip(np.searchsorted(self.rain_t, self._t_tab[: self.N], "right") - 1, 0, len(self.rain_t) - 1)
