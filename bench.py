@@ -321,15 +321,28 @@ def run_adjoint(args):
     import torch
     from geoswe_b200.adjoint import FlatAdjoint
     from geoswe_b200.synthetic import calibration_case
+    from geoswe_b200.adjoint import Inlet
     torch.cuda.set_device(0)
     t0 = time.perf_counter()
-    case = calibration_case(args.adj_n, seed=0)
+    case = calibration_case(args.adj_n, seed=0, base_q=0.5, inlet_gauges=4)
     build_s = time.perf_counter() - t0
     cs = case["cs"]
-    prob = FlatAdjoint(cs, gauges=case["gauges"], n_steps=args.adj_steps, window=args.adj_window,
-                       snapshots=args.adj_snapshots, dtype="float32", rain_times=case["rain_times"],
-                       rain_base=case["rain_base"], inlet=case["inlet"])
-    n0, k0 = case["n_tab"], case["knots"]
+
+    def problem(inlet):
+        return FlatAdjoint(cs, gauges=case["gauges"], n_steps=args.adj_steps, window=args.adj_window,
+                           snapshots=args.adj_snapshots, dtype="float32", rain_times=case["rain_times"],
+                           rain_base=case["rain_base"], inlet=inlet)
+
+    # the hydrograph's 16 knots span the simulated time of the N steps (probe run first)
+    prob = problem(case["inlet"])
+    prob.set_params(case["n_tab"], 1.0, case["knots"])
+    prob.forward(snapshots=False)
+    t_sim = prob.t_end
+    inl = case["inlet"]
+    kt = np.linspace(0.0, t_sim, len(inl.t_knots))
+    k0 = np.maximum(0.5, 20.0 * (1.0 - np.abs(kt - t_sim / 3.0) / (t_sim / 3.0)))
+    prob = problem(Inlet(ghost=inl.ghost, nbr=inl.nbr, normal=inl.normal, ds=inl.ds, t_knots=kt))
+    n0 = case["n_tab"]
     prob.set_params(n0 * 1.2, 0.9, k0)
     target = prob.forward(snapshots=False).cpu().numpy()
     prob.set_params(n0, 1.0, k0)
@@ -370,7 +383,8 @@ def run_adjoint(args):
             "total_gradient_cost_in_forward_passes": (rec_ms + grad_ms) / fwd_ms,
             "max_live_snapshots": prob.max_snapshots, "gpu_launches_sweep": int(prob.kernel_launches - l0),
             "loss": loss, "grad_n": [float(x) for x in gn.cpu()], "grad_rain_scale": gs,
-            "grad_knots": [float(x) for x in gk], "simulated_s": prob.t_end, "build_s": build_s}
+            "grad_knots": [float(x) for x in gk], "knot_times_s": [float(x) for x in kt],
+            "knot_values": [float(x) for x in k0], "simulated_s": prob.t_end, "build_s": build_s}
 
 
 def cpu_baseline(args):

@@ -171,7 +171,7 @@ def ensemble_specs(n_members=64, seed=0, side_min=256, side_max=4096):
 
 def calibration_case(n=2048, *, seed=0, dx=3.0, frac=0.7, pond=0.3, n_gauges=32, n_knots=16,
                      peak_q=20.0, t_peak=900.0, t_knots_end=3600.0, rain_mm_h=40.0, brick_h=16,
-                     base_q=0.0, device="cuda"):
+                     base_q=0.0, inlet_gauges=0, device="cuda"):
     """The Manning / rain / inflow calibration case on the compressed mesh: an n x n
     fractal bed (as rain_on_terrain), 4 Voronoi Manning classes, active set z < the
     `frac` quantile (three border rows/columns left out), a pond filling the lowest
@@ -180,7 +180,8 @@ def calibration_case(n=2048, *, seed=0, dx=3.0, frac=0.7, pond=0.3, n_gauges=32,
     edge whose ghost bed is not below its neighbour) with an `n_knots` hydrograph
     rising linearly to `peak_q` m^3/s at `t_peak` and falling back to 0 at 2 t_peak,
     never below `base_q`.
-    Gauges: `n_gauges` seeded active cells among the lower half of the active bed.
+    Gauges: `n_gauges` seeded active cells, `inlet_gauges` of them the active cells
+    nearest the inlet and the rest among the lower half of the active bed.
     Returns a dict of the CompressedSolver and the pieces FlatAdjoint takes."""
     from . import Config, Mesh2D, Solver2D
     from .adjoint import Inlet
@@ -210,7 +211,12 @@ def calibration_case(n=2048, *, seed=0, dx=3.0, frac=0.7, pond=0.3, n_gauges=32,
     inlet_q = np.maximum(base_q, peak_q * (1.0 - np.abs(inlet_t - t_peak) / t_peak))
     inlet = Inlet(ghost=g[k:k + 1], nbr=a[k:k + 1], normal=(float(d[0]), float(d[1])), ds=dx, t_knots=inlet_t)
     act = np.nonzero(cs.is_active != 0)[0]
-    low = act[b[act] <= np.quantile(b[act], 0.5)]
-    gauges = np.sort(rng.choice(low, size=min(n_gauges, low.size), replace=False))
+    near = np.empty(0, np.int64)
+    if inlet_gauges > 0:
+        dist = np.abs(ij[act] - ij[a[k]]).max(axis=1)
+        near = act[np.argsort(dist, kind="stable")[:inlet_gauges]]
+    low = np.setdiff1d(act[b[act] <= np.quantile(b[act], 0.5)], near)
+    rest = rng.choice(low, size=min(max(n_gauges - near.size, 0), low.size), replace=False)
+    gauges = np.sort(np.concatenate([near, rest]))
     return dict(cs=cs, gauges=gauges, inlet=inlet, knots=inlet_q, rain_times=np.array([0.0]),
                 rain_base=np.array([rain_mm_h / 3.6e6]), n_tab=MANNING_CLASSES.copy())
