@@ -387,6 +387,84 @@ def run_adjoint(args):
             "knot_values": [float(x) for x in k0], "simulated_s": prob.t_end, "build_s": build_s}
 
 
+def run_tidal(args):
+    """Everywhere-wet throughput on the compressed mesh: 32000 x 20000 = 640 M cells, all
+    active, dx = 1 m, bed 0.5 sin(2 pi x / 2000) cos(2 pi y / 1500) m, free surface 1.5 m
+    plus 1 cm seeded noise, zero velocity, n = 0.03, tidal stage 1.5 + 0.3 sin(2 pi t /
+    44712 s) on the x- ghost ring (one gauge, weight 1), CFL 0.5, fp32, `steps` timed
+    steps. The roofline basis is 38 B per active cell (the reference's table format:
+    state, bed, class, int16 neighbours, flag); the brick layout's own DRAM traffic is
+    measured with ncu on a smaller all-wet case."""
+    import torch
+    import warnings
+    from geoswe_b200 import Config, Mesh2D, Solver2D, autotune
+    from geoswe_b200.compressed import CompressedSolver
+    torch.cuda.set_device(0)
+    nx, ny, dx = args.tidal_nx, args.tidal_ny, 1.0
+    t0 = time.perf_counter()
+    dev = torch.device("cuda")
+    x = (torch.arange(nx, device=dev, dtype=torch.float64) + 0.5) * dx
+    y = (torch.arange(ny, device=dev, dtype=torch.float64) + 0.5) * dx
+    z = (0.5 * torch.sin(2 * np.pi * x / 2000.0)[:, None] * torch.cos(2 * np.pi * y / 1500.0)[None, :]).float()
+    gen = torch.Generator(device=dev).manual_seed(0)
+    eta = 1.5 + 0.01 * torch.randn((nx, ny), generator=gen, device=dev, dtype=torch.float32)
+    h = torch.clamp(eta - z, min=0.0)
+    del eta
+    q0 = np.zeros((3, nx, ny), np.float32)
+    q0[0] = h.cpu().numpy()
+    zh = z.cpu().numpy()
+    del h, z, x, y
+    torch.cuda.empty_cache()
+    cfg = Config(bc_x="wall", bc_y="wall", friction="manning", manning_n=0.03, cfl=0.5)
+    s = Solver2D(Mesh2D(nx=nx, ny=ny, dx=dx, dy=dx, ngh=2), cfg, q0, zh, track_max_depth=False)
+    del q0, zh
+    s.apply_bc()
+    ngh = s.mesh.ngh
+    ri = np.repeat(np.arange(ngh), s.nyp)
+    rj = np.tile(np.arange(s.nyp), ngh)
+    rbed = s._b[:ngh, : s.nyp].reshape(-1).cpu().numpy().astype(np.float32)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        cs = CompressedSolver.from_dense(s, track_max_depth=False)
+    del s
+    torch.cuda.empty_cache()
+    t_c = np.arange(0.0, 3600.0 + 60.0, 60.0)
+    stage = (1.5 + 0.3 * np.sin(2 * np.pi * t_c / 44712.0)).astype(np.float32)[None, :]
+    cs.set_ring(dict(i=ri, j=rj, bed=rbed, wg=np.ones((ri.size, 1), np.float32), NG=1, n=int(ri.size),
+                     t_common=t_c, stage_all=stage))
+    build_s = time.perf_counter() - t0
+    cs.run(t_end=1e12, max_steps=args.warmup)
+    torch.cuda.synchronize()
+    clk = Clocks(0)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = cs.kernel_launches
+    e0.record()
+    steps = cs.run(t_end=1e12, max_steps=args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    launches = cs.kernel_launches - l0
+    kern_ms = autotune.time_flat_step(cs, reps=args.kernel_reps)
+    cells = int(cs.N_active)
+    peak, peak_kind = _peaks()
+    achieved = 38.0 * cells / (kern_ms / 1e3) / 1e9
+    stored_bytes = 29.0 * cs.nslots                      # q in + bed + flag + q out per slot
+    return {"metric": METRIC + " [compressed, everywhere wet]", "value": cells * steps / (ms / 1e3), "unit": UNIT,
+            "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"tidal everywhere-wet compressed {nx}x{ny}, dx=1 m, sinusoidal bed, "
+                                   f"n=0.03, tidal stage on the x- ring, CFL 0.5, fp32",
+                       "active_cells": cells, "stored_slots": int(cs.nslots), "bricks": int(cs.n_bricks),
+                       "l2": "inputs larger than L2 (no flush)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "flat_march_kernel<float,1>",
+                         "kernel_ms": kern_ms, "bytes_per_cell": 38, "peak_source": peak_kind,
+                         "brick_bytes_GBs": stored_bytes / (kern_ms / 1e3) / 1e9},
+            "gpu_launches": int(launches), "clocks": clocks, "build_s": build_s, "simulated_s": cs.t}
+
+
 def cpu_baseline(args):
     """The reference's CPU path (its NumPy solver, restated in oracle/numpy_ref.py) on a
     bounded sample of the same workload, on this host's cores."""
@@ -409,7 +487,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
-    ap.add_argument("--case", default="dense", choices=["dense", "ensemble", "adjoint"])
+    ap.add_argument("--case", default="dense", choices=["dense", "ensemble", "adjoint", "tidal"])
+    ap.add_argument("--tidal-nx", type=int, default=32000)
+    ap.add_argument("--tidal-ny", type=int, default=20000)
     ap.add_argument("--adj-n", type=int, default=2048)
     ap.add_argument("--adj-steps", type=int, default=3000)
     ap.add_argument("--adj-window", type=int, default=1000)
@@ -429,9 +509,9 @@ def main():
         out = numpy_ref.reference_arm(args, METRIC, UNIT)
         print(json.dumps(out), flush=True)
         return 0
-    if args.case in ("ensemble", "adjoint"):
+    if args.case in ("ensemble", "adjoint", "tidal"):
         if rank == 0:
-            out = run_ensemble(args) if args.case == "ensemble" else run_adjoint(args)
+            out = {"ensemble": run_ensemble, "adjoint": run_adjoint, "tidal": run_tidal}[args.case](args)
             print(json.dumps(out), flush=True)
         return 0
     if world > 1:

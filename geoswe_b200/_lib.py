@@ -104,6 +104,12 @@ class GswGaugeArgs(C.Structure):
                 ("state", vp)]
 
 
+class GswFlatRingArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("dtype", i32), ("q0", vp), ("q1", vp), ("q2", vp), ("slots", vp),
+                ("bed", vp), ("wg", vp), ("n", i32), ("NG", i32), ("t_common", vp), ("n_t", i32),
+                ("reserved0", i32), ("stage_all", vp), ("state", vp)]
+
+
 class GswMember(C.Structure):
     _fields_ = [("dt", GswDtParams), ("inv_dx", C.c_float), ("g", C.c_float), ("h_min", C.c_float),
                 ("h_min_cfl", C.c_float), ("vcap", C.c_float), ("linf", i32), ("quadratic", i32),
@@ -130,6 +136,7 @@ _PROTOS = {
     "gsw_dt_finalize": [C.POINTER(GswDtParams), vp, vp],
     "gsw_loop_commit": [vp, vp],
     "gsw_flat_inflow_apply": [C.POINTER(GswFlatInflowArgs), vp],
+    "gsw_flat_ring_stage": [C.POINTER(GswFlatRingArgs), vp],
     "gsw_adj_flat_step": [C.POINTER(GswFlatAdjArgs), vp],
     "gsw_adj_flat_inflow": [C.POINTER(GswFlatInflowArgs), vp, vp, vp, vp, vp],
     "gsw_gauge_record": [C.POINTER(GswGaugeArgs), vp],

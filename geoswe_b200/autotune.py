@@ -140,3 +140,36 @@ def tune_ensemble(ens, t_end, reps=6, space=None, store=True, verbose=False):
     if store:
         _store("ensemble", ens.nslots, best)
     return best, table
+
+
+def time_flat_step(cs, reps=10, dt=None, warps=0):
+    """Mean duration (ms) of one fused flat-step launch of compressed solver `cs` on
+    scratch copies of its state (the solver is not advanced)."""
+    from .solver import _ptr, _stream
+    if dt is None:
+        dt = getattr(cs, "last_dt", None) or 0.01
+    st = L.GswLoopState()
+    st.t = cs.t
+    st.dt = float(dt)
+    st.dt_f32 = float(np.float32(dt))
+    state = torch.zeros(128, dtype=torch.uint8, device=cs.device)
+    state.copy_(torch.frombuffer(bytearray(bytes(st) + bytes(128 - C.sizeof(st))), dtype=torch.uint8))
+    src = [x.clone() for x in cs._q[cs._cur]]
+    dst = [torch.empty_like(x) for x in src]
+    args = []
+    for k in (0, 1):
+        a = cs._args(src if k == 0 else dst, dst if k == 0 else src)
+        a.state = _ptr(state)
+        a.lam_target = C.c_void_p(state.data_ptr() + L.GswLoopState.lam_bits.offset)
+        a.warps = int(warps)
+        args.append(a)
+    for k in range(2):
+        L.call("gsw_flat_step", C.byref(args[k % 2]), _stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(reps):
+        L.call("gsw_flat_step", C.byref(args[k % 2]), _stream())
+    e1.record()
+    torch.cuda.synchronize()
+    del src, dst
+    return e0.elapsed_time(e1) / reps

@@ -88,6 +88,7 @@ class CompressedSolver:
 
     @classmethod
     def from_dense(cls, s: Solver2D, *, cfl_linf: bool = False, dt_max=None, brick_h: Optional[int] = None,
+                   track_max_depth: bool = True,
                    h_min: Optional[float] = None, cfl: Optional[float] = None, g: Optional[float] = None,
                    say=None):
         """Pack the dense solver ``s`` (its inside mask, state, bed, Manning) into the
@@ -211,7 +212,7 @@ class CompressedSolver:
             n = float(np.float32(cfg.manning_n)) if cfg.friction is not None else 0.0
             self._ncls = None
             self._ntab = torch.tensor([n], dtype=torch.float32, device=dev)
-        self._max_h = torch.zeros(self.nslots, dtype=torch.float32, device=dev)
+        self._max_h = torch.zeros(self.nslots, dtype=torch.float32, device=dev) if track_max_depth else None
         self._state = torch.zeros(128, dtype=torch.uint8, device=dev)
         self._state_host = torch.zeros(128, dtype=torch.uint8).pin_memory()
         self._rain = None
@@ -219,6 +220,7 @@ class CompressedSolver:
         self._rain_t = None
         self._rain_rmax = 0.0
         self._inflows = []
+        self._ring = None
         self._graph_cache = {}
         self.t = 0.0
         self.nsteps = 0
@@ -302,6 +304,53 @@ class CompressedSolver:
             t=torch.from_numpy(t.copy()).to(dev), q=torch.from_numpy(qs.copy()).to(dev)))
         self._graph_cache.clear()
         return self
+
+    def set_ring(self, ring):
+        """Stage on ghost-ring cells (the reference's set_ring dict, compressed_solver.py:
+        3146, 3264-3268, applied as ring_bc_flat after every step): keys i, j (padded
+        indices of the ring cells), bed (their bed, float32), wg ((n, NG) gauge weights),
+        NG, n, t_common (T times, s), stage_all ((NG, T) stages, m). None removes it."""
+        if ring is None or int(ring.get("n", 0)) == 0:
+            self._ring = None
+            self._graph_cache.clear()
+            return self
+        n, NG = int(ring["n"]), int(ring["NG"])
+        i = np.asarray(ring["i"], np.int64).reshape(-1)
+        j = np.asarray(ring["j"], np.int64).reshape(-1)
+        if i.size != n or j.size != n:
+            raise ValueError("set_ring: i and j must hold n indices")
+        t_c = np.asarray(ring["t_common"], np.float64).reshape(-1)
+        st = np.asarray(ring["stage_all"], np.float32).reshape(NG, -1)
+        if t_c.size < 2 or st.shape[1] != t_c.size:
+            raise ValueError("set_ring: stage_all must be (NG, T) with T = len(t_common) >= 2")
+        wg = np.asarray(ring["wg"], np.float32).reshape(n, NG)
+        if (i < 0).any() or (i >= self.nxp).any() or (j < 0).any() or (j >= self.nyp).any():
+            raise ValueError("set_ring: ring index outside the padded grid")
+        dev = self.device
+        lin = torch.from_numpy(i * self.nyp + j).to(dev)
+        slot_of_cell = torch.full((self.nxp * self.nyp,), -1, dtype=torch.int64, device=dev)
+        slot_of_cell[self._lin_of_slot.to(torch.int64)] = self._slot_cells.to(torch.int64)
+        slots = slot_of_cell[lin].contiguous()
+        del slot_of_cell
+        self._ring = dict(slots=slots, n=n, NG=NG,
+                          bed=torch.from_numpy(np.asarray(ring["bed"], np.float32).reshape(-1).copy()).to(dev),
+                          wg=torch.from_numpy(wg.copy()).to(dev),
+                          t=torch.from_numpy(t_c.copy()).to(dev),
+                          stage=torch.from_numpy(np.ascontiguousarray(st)).to(dev))
+        self._graph_cache.clear()
+        return self
+
+    def _ring_args(self, q):
+        r = self._ring
+        a = L.GswFlatRingArgs()
+        a.abi_version = L.ABI_VERSION
+        a.dtype = L.F32
+        a.q0, a.q1, a.q2 = _ptr(q[0]), _ptr(q[1]), _ptr(q[2])
+        a.slots, a.bed, a.wg = _ptr(r["slots"]), _ptr(r["bed"]), _ptr(r["wg"])
+        a.n, a.NG = r["n"], r["NG"]
+        a.t_common, a.n_t, a.stage_all = _ptr(r["t"]), int(r["t"].numel()), _ptr(r["stage"])
+        a.state = _ptr(self._state)
+        return a
 
     def _inflow_args(self, f, q):
         a = L.GswFlatInflowArgs()
@@ -467,9 +516,12 @@ class CompressedSolver:
                 for f in self._inflows:             # inlet ghosts at t_n, before the step
                     L.call("gsw_flat_inflow_apply", C.byref(self._inflow_args(f, src)), s)
                 L.call("gsw_flat_step", C.byref(self._args(src, dst)), s)
-            return (2 + len(self._inflows)) * K
+                if self._ring is not None:          # ring stage at t_n, after the step
+                    L.call("gsw_flat_ring_stage", C.byref(self._ring_args(dst)), s)
+            return (2 + len(self._inflows) + (self._ring is not None)) * K
 
-        key = (K, start, float(t_end), p.dt_max, int(max_steps), self._rain_kind, len(self._inflows))
+        key = (K, start, float(t_end), p.dt_max, int(max_steps), self._rain_kind, len(self._inflows),
+               self._ring is not None)
         if key not in self._graph_cache:
             self._graph_cache.clear()
             side = torch.cuda.Stream(device=self.device)

@@ -149,6 +149,40 @@ __global__ void flat_inflow_kernel(GswFlatInflowArgs a) {
     }
 }
 
+// Ring stage of the compressed mesh (ring_bc_flat, compressed_solver.py:287-307, with
+// the on-device stage interpolation of :2338-2350). One thread per ring cell.
+template <typename T>
+__global__ void flat_ring_kernel(GswFlatRingArgs a) {
+    if (a.state->done) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n) return;
+    const double t = a.state->t;
+    int lo = 0, hi = a.n_t;                          // searchsorted(t_common, t, side="left")
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (a.t_common[mid] < t) lo = mid + 1; else hi = mid; }
+    int ti = lo - 1;
+    if (ti > a.n_t - 2) ti = a.n_t - 2;
+    if (ti < 0) ti = 0;
+    double wt = __ddiv_rn(__dsub_rn(t, a.t_common[ti]),
+                          __dadd_rn(__dsub_rn(a.t_common[ti + 1], a.t_common[ti]), 1.0e-12));
+    wt = wt < 1.0 ? wt : 1.0;
+    wt = wt > 0.0 ? wt : 0.0;
+    const T w0 = (T)__dsub_rn(1.0, wt), w1 = (T)wt;
+    const T* st = (const T*)a.stage_all;
+    const T* w = (const T*)a.wg + (int64_t)k * a.NG;
+    T eta = (T)0;
+    for (int g = 0; g < a.NG; ++g) {
+        T s = st[(int64_t)g * a.n_t + ti] * w0;
+        s = s + st[(int64_t)g * a.n_t + ti + 1] * w1;
+        eta = eta + w[g] * s;
+    }
+    const int64_t idx = a.slots[k];
+    if (idx < 0) return;
+    const T h = eta - ((const T*)a.bed)[k];
+    ((T*)a.q0)[idx] = h > (T)0 ? h : (T)0;
+    ((T*)a.q1)[idx] = (T)0;
+    ((T*)a.q2)[idx] = (T)0;
+}
+
 }  // namespace gsw
 
 using namespace gsw;
@@ -177,4 +211,18 @@ extern "C" int gsw_flat_inflow_apply(const GswFlatInflowArgs* a, void* stream) {
     else if (a->dtype == GSW_F64) flat_inflow_kernel<double><<<1, 256, 0, s>>>(*a);
     else return set_error(GSW_ERR_INVALID, "flat inflow: bad dtype");
     return check_launch("flat_inflow");
+}
+
+extern "C" int gsw_flat_ring_stage(const GswFlatRingArgs* a, void* stream) {
+    GSW_CHECK_ABI(a);
+    if (a->n <= 0) return GSW_OK;
+    if (!a->q0 || !a->q1 || !a->q2 || !a->slots || !a->bed || !a->wg || !a->t_common || !a->stage_all ||
+        !a->state || a->NG < 1 || a->n_t < 2)
+        return set_error(GSW_ERR_INVALID, "ring stage: null pointer, NG < 1 or fewer than 2 stage times");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int grid = (a->n + 255) / 256;
+    if (a->dtype == GSW_F32) flat_ring_kernel<float><<<grid, 256, 0, s>>>(*a);
+    else if (a->dtype == GSW_F64) flat_ring_kernel<double><<<grid, 256, 0, s>>>(*a);
+    else return set_error(GSW_ERR_INVALID, "ring stage: bad dtype");
+    return check_launch("flat_ring");
 }

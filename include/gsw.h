@@ -298,6 +298,30 @@ typedef struct GswFlatInflowArgs {
 } GswFlatInflowArgs;
 GSW_API int gsw_flat_inflow_apply(const GswFlatInflowArgs* a, void* stream);
 
+/* Stage on ghost-ring cells of the compressed mesh, applied after the step at the
+ * step's start time state->t: per gauge g the stage is interpolated in the (NG, n_t)
+ * table at ti = clamp(searchsorted_left(t_common, t) - 1, 0, n_t - 2) with weight
+ * wt = clamp((t - t_common[ti]) / (t_common[ti+1] - t_common[ti] + 1e-12), 0, 1) as
+ * stage[g][ti]*(1-wt) + stage[g][ti+1]*wt in the array type; per ring cell k,
+ * eta = sum_g wg[k][g] * stage_g, h = max(0, eta - bed[k]), hu = hv = 0. Replaces
+ * ring_bc_flat and its on-device interpolation (geoswe/compressed_solver.py:287-307,
+ * 1622-1634, 2338-2350). Nothing is written when state->done. */
+typedef struct GswFlatRingArgs {
+    uint32_t abi_version;
+    int32_t  dtype;              /* GSW_F32 or GSW_F64 */
+    void* q0; void* q1; void* q2;/* brick storage */
+    const int64_t* slots;        /* n ring slots (-1: not stored, skipped) */
+    const void* bed;             /* n ring-cell beds */
+    const void* wg;              /* (n, NG) gauge weights */
+    int32_t  n, NG;
+    const double* t_common;      /* n_t >= 2 increasing times */
+    int32_t  n_t;
+    int32_t  reserved0;
+    const void* stage_all;       /* (NG, n_t) gauge stages (m) */
+    const GswLoopState* state;
+} GswFlatRingArgs;
+GSW_API int gsw_flat_ring_stage(const GswFlatRingArgs* a, void* stream);
+
 /* Fused step on the compressed mesh: active cells get the SRM-HLLC residual, rain,
  * Euler, wet/dry and Manning (table); stored ring cells are carried unchanged.
  * Replaces the flat fused step + CFL launch (geoswe/compressed_rhs.py:673-865, 990-1118;

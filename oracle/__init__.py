@@ -380,6 +380,33 @@ class OracleFlat:
                                  w_dry=np.where(low, np.float32(1.0 / nlow), np.float32(0.0))))
         return self
 
+    def set_ring(self, ids, bed, wg, t_common, stage_all):
+        """Ring stage on canonical ids (-1: skipped), as ring_bc_flat with the on-device
+        interpolation (compressed_solver.py:287-307, 2338-2350)."""
+        self.ring = dict(ids=np.asarray(ids, np.int64), bed=np.asarray(bed, np.float32),
+                         wg=np.asarray(wg, np.float32).reshape(len(ids), -1),
+                         t=np.asarray(t_common, np.float64), st=np.asarray(stage_all, np.float32))
+        return self
+
+    def _apply_ring(self):
+        r = getattr(self, "ring", None)
+        if r is None:
+            return
+        tc, st = r["t"], r["st"]
+        ti = max(0, min(len(tc) - 2, int(np.searchsorted(tc, self.t) - 1)))
+        wt = float((self.t - tc[ti]) / (tc[ti + 1] - tc[ti] + 1e-12))
+        wt = min(1.0, max(0.0, wt))
+        stage = (st[:, ti] * np.float32(1.0 - wt)).astype(np.float32)
+        stage = (stage + st[:, ti + 1] * np.float32(wt)).astype(np.float32)
+        eta = np.zeros(len(r["ids"]), np.float32)
+        for g in range(stage.size):
+            eta = (eta + r["wg"][:, g] * stage[g]).astype(np.float32)
+        ok = r["ids"] >= 0
+        idx = r["ids"][ok]
+        self.q[0][idx] = np.maximum(np.float32(0.0), (eta - r["bed"])[ok]).astype(np.float32)
+        self.q[1][idx] = np.float32(0.0)
+        self.q[2][idx] = np.float32(0.0)
+
     def _apply_inflows(self):
         """The flat loop's inlet block (compressed_solver.py:2144-2167), NumPy sums."""
         q0, q1, q2 = self.q
@@ -430,6 +457,7 @@ class OracleFlat:
             C.c_int(int(self.quad)), C.c_int(int(self.keep_h)), _p(qn[0]), _p(qn[1]), _p(qn[2]), _p(self.max_h))
         self.q = qn
         self._lam = float(lam)
+        self._apply_ring()                      # at the step's start time, after the step
         self.t += dt
         self.nsteps += 1
 

@@ -152,3 +152,37 @@ def test_flat_inflow_run_bitwise_oracle(n_cells):
     assert h[cs.is_active != 0].sum() > 0          # water entered
     for c in range(3):
         assert same(cs.flat(c).cpu().numpy(), o.q[c]), c
+
+
+def test_flat_ring_stage_tidal_bitwise_oracle():
+    """Everywhere-wet sinusoidal bed with a tidal stage on the x- ghost ring (one gauge,
+    weight 1): the compressed run against the oracle's restatement of ring_bc_flat."""
+    import warnings
+    from geoswe_b200.compressed import CompressedSolver
+    from geoswe_b200.synthetic import tidal_case
+    nx, ny, dx = 60, 70, 25.0
+    h, z = tidal_case(nx, ny, dx=dx, seed=4)
+    q0 = np.stack([h, np.zeros_like(h), np.zeros_like(h)]).astype(np.float32)
+    s = _dense(q0, z, None, dx=dx, bc_x="wall", bc_y="wall", friction="manning", manning_n=0.03)
+    s.apply_bc()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        cs = CompressedSolver.from_dense(s, track_max_depth=False)
+    ij = cs.ij_active
+    ids = np.nonzero(ij[:, 0] < 2)[0]
+    b = cs._b[cs._slot].cpu().numpy()
+    t_c = np.arange(0.0, 4000.0, 300.0)
+    stage = (1.5 + 0.3 * np.sin(2 * np.pi * t_c / 2400.0)).astype(np.float32)[None, :]
+    ring = dict(i=ij[ids, 0], j=ij[ids, 1], bed=b[ids], wg=np.ones((ids.size, 1), np.float32), NG=1,
+                n=int(ids.size), t_common=t_c, stage_all=stage)
+    cs.set_ring(ring)
+    q = [cs.flat(c).cpu().numpy() for c in range(3)]
+    o = oracle.OracleFlat(cs.nbr, cs.is_active, q, b, dx, ntab=[np.float32(0.03)])
+    o.set_ring(ids, b[ids], ring["wg"], t_c, stage)
+    n_g = cs.run(t_end=900.0)
+    n_o = o.run(t_end=900.0)
+    assert n_g == n_o and n_g > 20
+    assert cs.t == o.t
+    for c in range(3):
+        assert same(cs.flat(c).cpu().numpy(), o.q[c]), c
+    assert abs(float(cs.flat(1).cpu().numpy()[cs.is_active != 0].max())) > 0   # the tide drives a flow
