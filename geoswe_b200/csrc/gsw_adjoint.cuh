@@ -35,12 +35,12 @@ __device__ __forceinline__ void hllc_bwd(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
                                          T& hL_b, T& uNL_b, T& uTL_b, T& hR_b, T& uNR_b, T& uTR_b) {
     const T z = Real<T>::zero();
     const T half = (T)0.5, quarter = (T)0.25, two = (T)2.0;
-    const T aL = gsqrt(g * (hL > z ? hL : z));
-    const T aR = gsqrt(g * (hR > z ? hR : z));
+    const T aL = sqrt_z(g * (hL > z ? hL : z));
+    const T aR = sqrt_z(g * (hR > z ? hR : z));
     const T u_st = half * (uNL + uNR) + aL - aR;
     const T h_rt = half * (aL + aR) + quarter * (uNL - uNR);
     const T h_st = (h_rt > z) ? (h_rt * h_rt) / g : z;
-    const T a_st = gsqrt(g * (h_st > z ? h_st : z));
+    const T a_st = sqrt_z(g * (h_st > z ? h_st : z));
     const T A1 = uNL - aL, A2 = u_st - a_st;
     const T B1 = uNR + aR, B2 = u_st + a_st;
     const bool dryL = (hL <= h_min);
@@ -52,7 +52,7 @@ __device__ __forceinline__ void hllc_bwd(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
     const T denom = hR * dR - hL * dL;
     const bool big = gabs(denom) > (T)1.0e-14;
     T SM;
-    if (big) SM = (SL * hR * dR - SR * hL * dL) / denom;
+    if (big) SM = div_z(SL * hR * dR - SR * hL * dL, denom);
     else     SM = half * (uNL + uNR);
     const bool left = SM >= z;
 
@@ -233,8 +233,8 @@ __device__ __forceinline__ void wetdry_friction_bwd(T h1, T hu1, T hv1, T n, T d
     }
     const bool pass = h1 > h_min;
     const T hs = pass ? h1 : h_min;
-    const T u = hu1 / hs, v = hv1 / hs;
-    const T modU = gsqrt(u * u + v * v);
+    const T u = div_z(hu1, hs), v = div_z(hv1, hs);
+    const T modU = sqrt_z(u * u + v * v);
     const T h43 = pow_m43(hs);
     T ne = n, K = z, ncri = z;
     bool capped = false;

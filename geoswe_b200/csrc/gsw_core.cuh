@@ -32,6 +32,24 @@ __device__ __forceinline__ double gsqrt(double a) { return sqrt(a); }
 __device__ __forceinline__ float  gabs(float a)   { return fabsf(a); }
 __device__ __forceinline__ double gabs(double a)  { return fabs(a); }
 
+// Exact-zero operands take the IEEE square root's and division's out-of-range path,
+// which is a subroutine call; dry faces (sqrt(g * 0)) and fluid at rest (0 / h) hit it
+// on most cells. These forms keep every result bit for bit and keep the call off the
+// zero case: sqrt(+-0) = +-0, and 0 / b = 0 * b (the same signed zero) for b finite
+// and non-zero. Any other operand goes through the IEEE operation itself.
+template <typename T>
+__device__ __forceinline__ T sqrt_z(T x) {
+    const bool zr = (x == (T)0);
+    const T r = gsqrt(zr ? (T)1 : x);
+    return zr ? x : r;
+}
+template <typename T>
+__device__ __forceinline__ T div_z(T a, T b) {
+    const bool zr = (a == (T)0) && (b != (T)0) && (gabs(b) < (T)INFINITY);
+    const T q = (zr ? (T)1 : a) / b;
+    return zr ? a * b : q;
+}
+
 // Primitive state of one cell (PRIMS macro, rhs_cuda.py:931-938) plus what the
 // faces need: free surface and the central bed gradients.
 template <typename T>
@@ -45,8 +63,8 @@ struct Cell {
 template <typename T>
 __device__ __forceinline__ void make_prims(Cell<T>& c, T h_min) {
     const T hs = (c.h > h_min) ? c.h : h_min;
-    c.u = (c.h > h_min) ? c.hu / hs : Real<T>::zero();
-    c.v = (c.h > h_min) ? c.hv / hs : Real<T>::zero();
+    c.u = (c.h > h_min) ? div_z(c.hu, hs) : Real<T>::zero();
+    c.v = (c.h > h_min) ? div_z(c.hv, hs) : Real<T>::zero();
     c.eta = c.h + c.b;
 }
 
@@ -100,12 +118,12 @@ __device__ __forceinline__ void hllc(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
                                      T g, T h_min, T& Fh, T& FN, T& FT) {
     const T z = Real<T>::zero();
     const T half = (T)0.5, quarter = (T)0.25, two = (T)2.0;
-    const T aL = gsqrt(g * (hL > z ? hL : z));
-    const T aR = gsqrt(g * (hR > z ? hR : z));
+    const T aL = sqrt_z(g * (hL > z ? hL : z));
+    const T aR = sqrt_z(g * (hR > z ? hR : z));
     const T u_st = half * (uNL + uNR) + aL - aR;
     const T h_rt = half * (aL + aR) + quarter * (uNL - uNR);
     const T h_st = (h_rt > z) ? (h_rt * h_rt) / g : z;
-    const T a_st = gsqrt(g * (h_st > z ? h_st : z));
+    const T a_st = sqrt_z(g * (h_st > z ? h_st : z));
     const T SL_w = gmin(uNL - aL, u_st - a_st);
     const T SR_w = gmax(uNR + aR, u_st + a_st);
     const bool dryL = (hL <= h_min);
@@ -116,7 +134,7 @@ __device__ __forceinline__ void hllc(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
     const T denom = hR * (uNR - SR) - hL * (uNL - SL);
     T SM;
     if (gabs(denom) > (T)1.0e-14) {
-        SM = (SL * hR * (uNR - SR) - SR * hL * (uNL - SL)) / denom;
+        SM = div_z(SL * hR * (uNR - SR) - SR * hL * (uNL - SL), denom);
     } else {
         SM = half * (uNL + uNR);
     }
@@ -234,9 +252,9 @@ __device__ __forceinline__ void wetdry_friction(T& h, T& hu, T& hv, bool frictio
     }
     if (!friction) return;
     const T hs = (h > h_min) ? h : h_min;
-    const T u = hu / hs;
-    const T v = hv / hs;
-    const T modU = gsqrt(u * u + v * v);
+    const T u = div_z(hu, hs);
+    const T v = div_z(hv, hs);
+    const T modU = sqrt_z(u * u + v * v);
     const T h43 = pow_m43(hs);
     if (modU > vcap) {
         const T n_cri = gsqrt((T)1.0 / (((T)1.0e-10 + dt) * g * h43 * (modU + (T)1.0e-30)));
@@ -263,8 +281,8 @@ __device__ __forceinline__ void wetdry_friction(T& h, T& hu, T& hv, bool frictio
 __device__ __forceinline__ unsigned long long lam_dense_bits(float h, float hu, float hv,
                                                              float g, float h_cfl) {
     if (h < h_cfl) return 0ull;
-    const float u = hu / h;
-    const float v = hv / h;
+    const float u = div_z(hu, h);
+    const float v = div_z(hv, h);
     const float au = fabsf(u), av = fabsf(v);
     const float lam = ((au > av) ? au : av) + sqrtf(g * h);
     const bool fin = (lam <= 3.0e38f) && (au <= 3.0e38f) && (av <= 3.0e38f);
@@ -278,8 +296,8 @@ __device__ __forceinline__ unsigned long long lam_dense_bits(double h, double hu
                                                              double g, double h_cfl) {
     const bool dry = h <= h_cfl;
     const double hs = h > h_cfl ? h : h_cfl;
-    const double u = dry ? 0.0 : hu / hs;
-    const double v = dry ? 0.0 : hv / hs;
+    const double u = dry ? 0.0 : div_z(hu, hs);
+    const double v = dry ? 0.0 : div_z(hv, hs);
     const double c = sqrt(g * (h > 0.0 ? h : 0.0));
     const double au = fabs(u), av = fabs(v);
     const double lam = ((au > av) ? au : av) + c;
@@ -296,9 +314,9 @@ __device__ __forceinline__ unsigned long long lam_flat_bits(float h, float hu, f
     if (h != h) return 0x7ff8000000000000ull;
     if (h < h_min) return 0ull;
     const float hs = h > h_min_cfl ? h : h_min_cfl;
-    const float u = hu / hs, v = hv / hs;
+    const float u = div_z(hu, hs), v = div_z(hv, hs);
     const float c = sqrtf(g * (h > 0.0f ? h : 0.0f));
-    const float speed = linf ? fmaxf(fabsf(u), fabsf(v)) : sqrtf(u * u + v * v);
+    const float speed = linf ? fmaxf(fabsf(u), fabsf(v)) : sqrt_z(u * u + v * v);
     const float l = speed + c;
     return (unsigned long long)__double_as_longlong((double)l);
 }
@@ -309,9 +327,9 @@ __device__ __forceinline__ unsigned long long lam_flat_bits(double h, double hu,
     if (h != h) return 0x7ff8000000000000ull;
     if (h < h_min) return 0ull;
     const double hs = h > h_min_cfl ? h : h_min_cfl;
-    const double u = hu / hs, v = hv / hs;
+    const double u = div_z(hu, hs), v = div_z(hv, hs);
     const double c = sqrt(g * (h > 0.0 ? h : 0.0));
-    const double speed = linf ? fmax(fabs(u), fabs(v)) : sqrt(u * u + v * v);
+    const double speed = linf ? fmax(fabs(u), fabs(v)) : sqrt_z(u * u + v * v);
     return (unsigned long long)__double_as_longlong(speed + c);
 }
 
