@@ -275,6 +275,13 @@ def run_ensemble(args):
     loop_members = [build_member(sp) for sp in specs]
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
+    loop_shape = None
+    if not args.no_tune:                     # the plain solver gets its own tuned launch shape
+        big = max(loop_members, key=lambda m: m.nslots)
+        best, _ = autotune.tune_flat(big, store=False)
+        for m in loop_members:
+            m.warps, m.min_blocks = best["warps"], best["min_blocks"]
+        loop_shape = best
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     steps_loop = [m.run(t_end=t_end) for m in loop_members]
@@ -306,7 +313,8 @@ def run_ensemble(args):
            "plain_loop_value": work / (ms_loop / 1e3), "speedup_vs_plain_loop": ms_loop / ms_ens,
            "identical_steps_to_plain": bool(steps_ens == steps_loop),
            "gpu_launches": int(ens.kernel_launches - n0), "gpu_launches_plain_loop": loop_launches,
-           "schedule": {"warps": ens.warps or 4, "grid": ens.grid, "brick_h": ens.brick_h}, "autotune": tune,
+           "schedule": {"warps": ens.warps or 4, "grid": ens.grid, "min_blocks": ens.min_blocks,
+                        "brick_h": ens.brick_h}, "autotune": tune, "plain_loop_shape": loop_shape,
            "build_s": build_s, "dtype": "f32", "data": "synthetic"}
     return out
 
@@ -434,6 +442,10 @@ def run_tidal(args):
                      t_common=t_c, stage_all=stage))
     build_s = time.perf_counter() - t0
     cs.run(t_end=1e12, max_steps=args.warmup)
+    tune = None
+    if not args.no_tune:
+        best, table = autotune.tune_flat(cs, reps=4)
+        tune = {"best": best, "table": table}
     torch.cuda.synchronize()
     clk = Clocks(0)
     clk.start()
@@ -462,7 +474,8 @@ def run_tidal(args):
                          "frac": achieved / peak, "traffic": None, "kernel": "flat_march_kernel<float,1>",
                          "kernel_ms": kern_ms, "bytes_per_cell": 38, "peak_source": peak_kind,
                          "brick_bytes_GBs": stored_bytes / (kern_ms / 1e3) / 1e9},
-            "gpu_launches": int(launches), "clocks": clocks, "build_s": build_s, "simulated_s": cs.t}
+            "gpu_launches": int(launches), "clocks": clocks, "build_s": build_s, "simulated_s": cs.t,
+            "launch_shape": {"warps": cs.warps or 4, "min_blocks": cs.min_blocks}, "autotune": tune}
 
 
 def cpu_baseline(args):

@@ -77,7 +77,8 @@ class GswInflowArgs(C.Structure):
 
 
 class GswFlatArgs(C.Structure):
-    _fields_ = [("abi_version", u32), ("dtype", i32), ("brick_h", i32), ("warps", i32), ("n_bricks", i64),
+    _fields_ = [("abi_version", u32), ("dtype", i32), ("brick_h", i32), ("warps", i32), ("min_blocks", i32),
+                ("reserved1", i32), ("n_bricks", i64),
                 ("brick_ij", vp), ("brick_nbr", vp), ("flags", vp),
                 ("q0", vp), ("q1", vp), ("q2", vp), ("qn0", vp), ("qn1", vp), ("qn2", vp), ("bed", vp),
                 ("inv_dx", f64), ("inv_dy", f64), ("g", f64), ("h_min", f64), ("h_min_cfl", f64),
@@ -118,7 +119,7 @@ class GswMember(C.Structure):
 
 class GswEnsembleArgs(C.Structure):
     _fields_ = [("abi_version", u32), ("brick_h", i32), ("n_bricks", i64), ("n_members", i32),
-                ("warps", i32), ("grid", i32), ("reserved0", i32), ("brick_ij", vp), ("brick_nbr", vp),
+                ("warps", i32), ("grid", i32), ("min_blocks", i32), ("brick_ij", vp), ("brick_nbr", vp),
                 ("brick_member", vp), ("flags", vp), ("n_cls", vp), ("q0", vp), ("q1", vp), ("q2", vp),
                 ("qn0", vp), ("qn1", vp), ("qn2", vp), ("bed", vp), ("max_h", vp), ("members", vp),
                 ("states", vp), ("scratch", vp), ("all_done", vp)]

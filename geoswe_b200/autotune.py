@@ -120,29 +120,30 @@ def tune_dense(s, reps=8, space=None, store=True, verbose=False):
     return best, table
 
 
-ENSEMBLE_SPACE = dict(warps=(2, 4, 8), blocks_per_sm=(1, 2, 4, 8))
+ENSEMBLE_SPACE = dict(warps=(4, 8), blocks_per_sm=(1, 2, 4, 8), min_blocks=(0, 4, 5))
+FLAT_SPACE = dict(warps=(2, 4, 8), min_blocks=(0, 4, 5))
 
 
 def tune_ensemble(ens, t_end, reps=6, space=None, store=True, verbose=False):
-    """Time the ensemble step for every (warps, blocks per SM) of `space` from the
+    """Time the ensemble step for every (warps, blocks per SM, register cap) of `space` from the
     ensemble's current state (restored before every launch, so nothing advances); set
     the winner on `ens` and cache it. Returns (best, table)."""
     space = space or ENSEMBLE_SPACE
     sms = torch.cuda.get_device_properties(ens.device).multi_processor_count
     table = []
-    for w, bps in itertools.product(space["warps"], space["blocks_per_sm"]):
-        ms = ens.time_step(t_end, warps=w, grid=bps * sms, reps=reps)
-        table.append(dict(warps=w, blocks_per_sm=bps, grid=bps * sms, ms=ms))
+    for w, bps, mb in itertools.product(space["warps"], space["blocks_per_sm"], space.get("min_blocks", (0,))):
+        ms = ens.time_step(t_end, warps=w, grid=bps * sms, min_blocks=mb, reps=reps)
+        table.append(dict(warps=w, blocks_per_sm=bps, grid=bps * sms, min_blocks=mb, ms=ms))
         if verbose:
-            print(f"  warps={w} blocks/SM={bps}: {ms:.4f} ms", flush=True)
+            print(f"  warps={w} blocks/SM={bps} min_blocks={mb}: {ms:.4f} ms", flush=True)
     best = min(table, key=lambda e: e["ms"])
-    ens.warps, ens.grid = best["warps"], best["grid"]
+    ens.warps, ens.grid, ens.min_blocks = best["warps"], best["grid"], best["min_blocks"]
     if store:
         _store("ensemble", ens.nslots, best)
     return best, table
 
 
-def time_flat_step(cs, reps=10, dt=None, warps=0):
+def time_flat_step(cs, reps=10, dt=None, warps=0, min_blocks=0):
     """Mean duration (ms) of one fused flat-step launch of compressed solver `cs` on
     scratch copies of its state (the solver is not advanced)."""
     from .solver import _ptr, _stream
@@ -161,7 +162,7 @@ def time_flat_step(cs, reps=10, dt=None, warps=0):
         a = cs._args(src if k == 0 else dst, dst if k == 0 else src)
         a.state = _ptr(state)
         a.lam_target = C.c_void_p(state.data_ptr() + L.GswLoopState.lam_bits.offset)
-        a.warps = int(warps)
+        a.warps, a.min_blocks = int(warps), int(min_blocks)
         args.append(a)
     for k in range(2):
         L.call("gsw_flat_step", C.byref(args[k % 2]), _stream())
@@ -173,3 +174,21 @@ def time_flat_step(cs, reps=10, dt=None, warps=0):
     torch.cuda.synchronize()
     del src, dst
     return e0.elapsed_time(e1) / reps
+
+
+def tune_flat(cs, reps=6, space=None, store=True, verbose=False):
+    """Time the fused flat step for every (warps, register cap) of `space` on scratch
+    copies of `cs`'s state; set the winner on `cs` and cache it. Returns (best, table)."""
+    space = space or FLAT_SPACE
+    table = []
+    for w, mb in itertools.product(space["warps"], space["min_blocks"]):
+        ms = time_flat_step(cs, reps=reps, warps=w, min_blocks=mb)
+        table.append(dict(warps=w, min_blocks=mb, ms=ms))
+        if verbose:
+            print(f"  warps={w} min_blocks={mb}: {ms:.4f} ms", flush=True)
+    best = min(table, key=lambda e: e["ms"])
+    cs.warps, cs.min_blocks = best["warps"], best["min_blocks"]
+    cs._graph_cache.clear()
+    if store:
+        _store("flat", cs.nslots, best)
+    return best, table

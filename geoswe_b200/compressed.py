@@ -221,6 +221,11 @@ class CompressedSolver:
         self._rain_rmax = 0.0
         self._inflows = []
         self._ring = None
+        self.warps, self.min_blocks = 0, 0
+        from . import autotune
+        best = autotune.load("flat", self.nslots)
+        if best:
+            self.warps, self.min_blocks = int(best["warps"]), int(best["min_blocks"])
         self._graph_cache = {}
         self.t = 0.0
         self.nsteps = 0
@@ -428,6 +433,7 @@ class CompressedSolver:
         a.g, a.h_min, a.h_min_cfl = self.g, self.h_min, self.h_min_cfl
         a.linf = int(self.cfl_linf)
         a.ngh, a.nx, a.ny = self.ngh, self.nx, self.ny
+        a.warps, a.min_blocks = self.warps, self.min_blocks
         if step:
             a.state = _ptr(self._state)
             a.lam_target = C.c_void_p(self._state.data_ptr() + L.GswLoopState.lam_bits.offset)
@@ -521,7 +527,7 @@ class CompressedSolver:
             return (2 + len(self._inflows) + (self._ring is not None)) * K
 
         key = (K, start, float(t_end), p.dt_max, int(max_steps), self._rain_kind, len(self._inflows),
-               self._ring is not None)
+               self._ring is not None, self.warps, self.min_blocks)
         if key not in self._graph_cache:
             self._graph_cache.clear()
             side = torch.cuda.Stream(device=self.device)

@@ -24,7 +24,8 @@ __device__ __forceinline__ FlatPhys<float> member_phys(const GswMember& mb) {
     return ph;
 }
 
-__global__ void __launch_bounds__(256) ensemble_step_kernel(GswEnsembleArgs a, FlatMesh<float> m) {
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArgs a, FlatMesh<float> m) {
     if (*a.all_done) return;
     const int lane = threadIdx.x;
     const int W = blockDim.y;
@@ -147,7 +148,11 @@ extern "C" int gsw_ensemble_step(const GswEnsembleArgs* a, void* stream) {
     m.o0 = a->qn0; m.o1 = a->qn1; m.o2 = a->qn2;
     m.b = a->bed; m.flags = a->flags; m.ncls = a->n_cls; m.max_h = a->max_h;
     m.bij = a->brick_ij; m.bnbr = a->brick_nbr; m.nb = a->n_bricks; m.bh = a->brick_h;
-    ensemble_step_kernel<<<grid, dim3(32, W), 0, (cudaStream_t)stream>>>(*a, m);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (a->min_blocks == 4) ensemble_step_kernel<4><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else if (a->min_blocks == 5) ensemble_step_kernel<5><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else if (a->min_blocks == 0) ensemble_step_kernel<1><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else return set_error(GSW_ERR_INVALID, "ensemble: min_blocks must be 0, 4 or 5");
     return check_launch("ensemble_step");
 }
 

@@ -15,8 +15,8 @@
 
 namespace gsw {
 
-template <typename T, bool STEP>
-__global__ void __launch_bounds__(256) flat_march_kernel(FlatK<T> p) {
+template <typename T, bool STEP, int MINB>
+__global__ void __launch_bounds__(256, MINB) flat_march_kernel(FlatK<T> p) {
     if (STEP && p.st->done) return;
     const int64_t bidx = (int64_t)blockIdx.x * blockDim.y + threadIdx.y;
     unsigned long long lam_local = 0ull;
@@ -92,7 +92,11 @@ static int launch_flat(const GswFlatArgs* a, cudaStream_t s) {
     if (W < 1 || W > 8) return set_error(GSW_ERR_INVALID, "flat: warps must be in [1, 8]");
     const int64_t blocks = (k.m.nb + W - 1) / W;
     if (blocks > 0x7fffffffLL) return set_error(GSW_ERR_INVALID, "flat: too many bricks");
-    flat_march_kernel<T, STEP><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
+    const int mb = a->min_blocks;
+    if (mb != 0 && mb != 4 && mb != 5) return set_error(GSW_ERR_INVALID, "flat: min_blocks must be 0, 4 or 5");
+    if (STEP && sizeof(T) == 4 && mb == 4) flat_march_kernel<T, STEP, 4><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
+    else if (STEP && sizeof(T) == 4 && mb == 5) flat_march_kernel<T, STEP, 5><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
+    else flat_march_kernel<T, STEP, 1><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
     return check_launch("flat_march");
 }
 

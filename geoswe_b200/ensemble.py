@@ -82,7 +82,7 @@ class Ensemble:
         # fixed device buffers: captured graphs hold their addresses across runs
         self._members_dev = torch.zeros(M * C.sizeof(GswMember), dtype=torch.uint8, device=dev)
         self._parity = np.zeros(M, np.int64)       # buffer of each member's current state
-        self.warps, self.grid = int(warps), int(grid)
+        self.warps, self.grid, self.min_blocks = int(warps), int(grid), 0
         self.kernel_launches = 0
         self._graph_cache = {}
 
@@ -116,7 +116,7 @@ class Ensemble:
         a = GswEnsembleArgs()
         a.abi_version = L.ABI_VERSION
         a.brick_h, a.n_bricks, a.n_members = self.brick_h, self.n_bricks, len(self.members)
-        a.warps, a.grid = self.warps, self.grid
+        a.warps, a.grid, a.min_blocks = self.warps, self.grid, self.min_blocks
         a.brick_ij, a.brick_nbr, a.brick_member = _ptr(self._bij), _ptr(self._bnbr), _ptr(self._bmem)
         a.flags, a.n_cls = _ptr(self._flags), _ptr(self._ncls)
         a.q0, a.q1, a.q2 = _ptr(src[0]), _ptr(src[1]), _ptr(src[2])
@@ -172,17 +172,17 @@ class Ensemble:
         self.kernel_launches += 2
         return p0
 
-    def time_step(self, t_end, *, warps, grid, reps=6, max_steps: int = 10 ** 9, dt_max=None):
+    def time_step(self, t_end, *, warps, grid, min_blocks=0, reps=6, max_steps: int = 10 ** 9, dt_max=None):
         """Mean duration (ms) of one ensemble step launch with the given schedule, from the
         current state; the states are restored before every launch and the members' state
         is left as it was."""
         _protos()
         p0 = self._prepare(t_end, max_steps, dt_max)
         snap = self._states.clone()
-        saved = (self.warps, self.grid)
-        self.warps, self.grid = int(warps), int(grid)
+        saved = (self.warps, self.grid, self.min_blocks)
+        self.warps, self.grid, self.min_blocks = int(warps), int(grid), int(min_blocks)
         args = self._args(self._q[p0], self._q[1 - p0])
-        self.warps, self.grid = saved
+        self.warps, self.grid, self.min_blocks = saved
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         total = 0.0
         for k in range(reps + 1):
@@ -213,7 +213,7 @@ class Ensemble:
                 L.call("gsw_ensemble_step", C.byref(self._args(src, dst)), st)
             return K
 
-        key = (K, p0, self.warps, self.grid)
+        key = (K, p0, self.warps, self.grid, self.min_blocks)
         if key not in self._graph_cache:
             self._graph_cache.clear()
             side = torch.cuda.Stream(device=self.device)

@@ -251,6 +251,8 @@ typedef struct GswFlatArgs {
     int32_t  dtype;            /* GSW_F32 or GSW_F64: q*, qn*, bed, rain, n_tab and max_h */
     int32_t  brick_h;          /* rows per brick (>= 2) */
     int32_t  warps;            /* warps per block (0: 4) */
+    int32_t  min_blocks;       /* fp32 step register cap: 0 (compiler's choice), 4 (64 regs) or 5 (48 regs) */
+    int32_t  reserved1;
     int64_t  n_bricks;         /* brick n_bricks is the all-zero brick (a missing neighbour) */
     const int32_t* brick_ij;   /* (n_bricks, 2) brick row, brick column */
     const int32_t* brick_nbr;  /* (n_bricks, 4) up, down, left, right */
@@ -411,7 +413,7 @@ typedef struct GswEnsembleArgs {
     int32_t  n_members;
     int32_t  warps;              /* warps per block (0: 4) */
     int32_t  grid;               /* persistent blocks (0: 2 per SM) */
-    int32_t  reserved0;
+    int32_t  min_blocks;         /* register cap: 0 (compiler's choice), 4 (64 regs) or 5 (48 regs) */
     const int32_t* brick_ij;     /* (n_bricks, 2) */
     const int32_t* brick_nbr;    /* (n_bricks, 4) global brick ids */
     const int32_t* brick_member; /* (n_bricks) */
