@@ -123,6 +123,13 @@ def make_solver(z, cls, n, dtype="float32"):
     return s
 
 
+# DRAM bytes per cell and launch of the step kernels, measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on the 4096 x 4096 case of
+# the same workload and scaled to a launch here by the cells it processes (the traffic
+# is proportional to the cells: no re-reads beyond the bricks' halo rows).
+DRAM_BYTES_PER_CELL = {"dense": 39.04, "flat": 32.24}
+
+
 def bytes_per_cell(track_max=True):
     # read h, hu, hv, z (16 B) + class id (1 B); write h, hu, hv (12 B); running max 8 B
     return 16 + 1 + 12 + (8 if track_max else 0)
@@ -187,7 +194,8 @@ def run_gsw(args, rank, world):
         "e2e": e2e,
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": DRAM_BYTES_PER_CELL["dense"] * cells / 1e9,
+                     "traffic_unit": "GB per launch (ncu, 4096x4096 capture scaled by cells)",
                      "kernel": "dense_march_kernel<float,true>", "kernel_ms": kern_ms,
                      "bytes_per_cell": bpc, "peak_source": peak_kind},
         "clocks": clocks,
@@ -471,7 +479,9 @@ def run_tidal(args):
                        "active_cells": cells, "stored_slots": int(cs.nslots), "bricks": int(cs.n_bricks),
                        "l2": "inputs larger than L2 (no flush)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": "flat_march_kernel<float,1>",
+                         "frac": achieved / peak, "traffic": DRAM_BYTES_PER_CELL["flat"] * cells / 1e9,
+                         "traffic_unit": "GB per launch (ncu, 4096x4096 capture scaled by cells)",
+                         "kernel": "flat_march_kernel<float,1>",
                          "kernel_ms": kern_ms, "bytes_per_cell": 38, "peak_source": peak_kind,
                          "brick_bytes_GBs": stored_bytes / (kern_ms / 1e3) / 1e9},
             "gpu_launches": int(launches), "clocks": clocks, "build_s": build_s, "simulated_s": cs.t,

@@ -143,9 +143,10 @@ def tune_ensemble(ens, t_end, reps=6, space=None, store=True, verbose=False):
     return best, table
 
 
-def time_flat_step(cs, reps=10, dt=None, warps=0, min_blocks=0):
+def time_flat_step(cs, reps=10, dt=None, warps=None, min_blocks=None):
     """Mean duration (ms) of one fused flat-step launch of compressed solver `cs` on
-    scratch copies of its state (the solver is not advanced)."""
+    scratch copies of its state (the solver is not advanced), with the solver's own
+    launch shape unless `warps` / `min_blocks` are given."""
     from .solver import _ptr, _stream
     if dt is None:
         dt = getattr(cs, "last_dt", None) or 0.01
@@ -162,7 +163,10 @@ def time_flat_step(cs, reps=10, dt=None, warps=0, min_blocks=0):
         a = cs._args(src if k == 0 else dst, dst if k == 0 else src)
         a.state = _ptr(state)
         a.lam_target = C.c_void_p(state.data_ptr() + L.GswLoopState.lam_bits.offset)
-        a.warps, a.min_blocks = int(warps), int(min_blocks)
+        if warps is not None:
+            a.warps = int(warps)
+        if min_blocks is not None:
+            a.min_blocks = int(min_blocks)
         args.append(a)
     for k in range(2):
         L.call("gsw_flat_step", C.byref(args[k % 2]), _stream())
