@@ -130,6 +130,13 @@ def make_solver(z, cls, n, dtype="float32"):
 DRAM_BYTES_PER_CELL = {"dense": 39.04, "flat": 32.24}
 
 
+def dense_config(n, world):
+    """The `config` of the default line (both arms)."""
+    return {"workload": f"rain-on-terrain dense {n}x{n}, dx=3 m, fractal bed, 4-class Voronoi Manning, dry "
+                        f"start, 50 mm/h uniform rain, x+ open, walls elsewhere, CFL 0.5, fp32",
+            "cells": n * n, "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"}
+
+
 def bytes_per_cell(track_max=True):
     # read h, hu, hv, z (16 B) + class id (1 B); write h, hu, hv (12 B); running max 8 B
     return 16 + 1 + 12 + (8 if track_max else 0)
@@ -187,10 +194,7 @@ def run_gsw(args, rank, world):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"rain-on-terrain dense {n}x{n}, dx=3 m, fractal bed, 4-class Voronoi "
-                               f"Manning, dry start, 50 mm/h uniform rain, x+ open, walls elsewhere, "
-                               f"CFL 0.5, fp32", "cells": cells, "l2": "inputs larger than L2 (no flush)",
-                   "parallelism": f"replicas x{world}"},
+        "config": dense_config(n, world),
         "e2e": e2e,
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -529,7 +533,7 @@ def main():
         if rank != 0:
             return 0
         from oracle import numpy_ref
-        out = numpy_ref.reference_arm(args, METRIC, UNIT)
+        out = numpy_ref.reference_arm(args, METRIC, UNIT, config=dense_config(args.n, world))
         print(json.dumps(out), flush=True)
         return 0
     if args.case in ("ensemble", "adjoint", "tidal"):
