@@ -130,6 +130,14 @@ def make_solver(z, cls, n, dtype="float32"):
 DRAM_BYTES_PER_CELL = {"dense": 39.04, "flat": 32.24}
 
 
+def max_over_ranks(x, device):
+    """The maximum of a per-rank time over the process group (every rank gets it)."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dense_config(n, world):
     """The `config` of the default line (both arms)."""
     return {"workload": f"rain-on-terrain dense {n}x{n}, dx=3 m, fractal bed, 4-class Voronoi Manning, dry "
@@ -183,9 +191,7 @@ def run_gsw(args, rank, world):
     del s
     torch.cuda.empty_cache()
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, "cuda")
     value = cells * args.steps * world / (ms / 1e3)
     peak, peak_kind = _peaks()
     bpc = bytes_per_cell(True)
@@ -499,7 +505,38 @@ def cpu_baseline(args):
         from oracle import numpy_ref
     except Exception as e:                      # pragma: no cover
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "port", "sample": f"unavailable: {e}"}
-    return numpy_ref.time_rain_on_terrain(n=args.cpu_n, steps=args.cpu_steps)
+    out = numpy_ref.time_rain_on_terrain(n=args.cpu_n, steps=args.cpu_steps)
+    if args.err_n > 0:
+        out["depth_error_vs_fp64"] = fp64_depth_error(args.err_n, args.err_t_end)
+    return out
+
+
+def fp64_depth_error(n, t_end):
+    """Depth error of the product (fp32, GPU) against an fp64 run of the same scheme on
+    the CPU (the reference's NumPy path, restated in the oracle), on an n x n sample of
+    the rain-on-terrain case run to the same simulated time."""
+    import torch
+    from oracle import numpy_ref
+    from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
+    from geoswe_b200.synthetic import MANNING_CLASSES, fractal_bed, voronoi_classes
+    t0 = time.perf_counter()
+    ref = numpy_ref._rain_on_terrain_solver(n, dtype=np.float64)
+    steps64 = ref.run(t_end=t_end)
+    z = fractal_bed(n, n, 3.0, seed=0).astype(np.float32)
+    cls = voronoi_classes(n, n, seed=0)
+    cfg = Config(bc_x="wall", bc_y="wall", bc={"x+": "fall"}, friction="manning",
+                 rainfall_forcing=RainfallForcing(time_s=[0.0, 1e9], rate_mm_h=[50.0, 50.0]))
+    s = Solver2D(Mesh2D(nx=n, ny=n, dx=3.0, dy=3.0, ngh=2), cfg, np.zeros((3, n, n), np.float32), z)
+    s.set_manning_table(np.pad(cls, 2, mode="edge"), MANNING_CLASSES)
+    steps32 = s.run(t_end=t_end)
+    torch.cuda.synchronize()
+    h32 = s.depth().astype(np.float64)
+    h64 = ref.q[0][2:-2, 2:-2]
+    d = h32 - h64
+    return {"case": f"rain-on-terrain {n}x{n}, t = {t_end:g} s", "max_m": float(np.abs(d).max()),
+            "rmse_m": float(np.sqrt(np.mean(d * d))), "mean_depth_m": float(h64.mean()),
+            "steps_fp32_gpu": int(steps32), "steps_fp64_cpu": int(steps64),
+            "seconds": time.perf_counter() - t0}
 
 
 def main():
@@ -513,6 +550,8 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=512)
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--err-n", type=int, default=96, help="fp64 depth-error sample size (0: skip)")
+    ap.add_argument("--err-t-end", type=float, default=600.0)
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--case", default="dense", choices=["dense", "ensemble", "adjoint", "tidal"])
     ap.add_argument("--tidal-nx", type=int, default=32000)

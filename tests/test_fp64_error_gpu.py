@@ -1,0 +1,40 @@
+"""Depth error of the product (fp32 on the GPU) against an fp64 run of the same scheme
+(the reference's NumPy path, restated in oracle/numpy_ref.py) on the CPU, run to the
+same simulated time: the circular dam break (walls, no friction) and rain on fractal
+terrain with Manning classes and an open edge. The figures are printed; the bounds are
+stated in each test."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _stats(h32, h64):
+    d = np.asarray(h32, np.float64) - np.asarray(h64, np.float64)
+    return float(np.abs(d).max()), float(np.sqrt(np.mean(d * d)))
+
+
+def test_dam_break_fp32_gpu_vs_fp64():
+    from geoswe_b200 import Config, Mesh2D, Solver2D
+    from geoswe_b200.synthetic import dam_break
+    from oracle import numpy_ref
+    n, t_end = 256, 20.0
+    q0, bed = dam_break(n, radius=32.0)
+    s = Solver2D(Mesh2D(nx=n, ny=n, dx=1.0, dy=1.0, ngh=2), Config(bc_x="wall", bc_y="wall"), q0, bed)
+    n32 = s.run(t_end=t_end)
+    qp = np.zeros((3, n + 4, n + 4))
+    qp[:, 2:-2, 2:-2] = q0
+    ref = numpy_ref.NumpySolver2D(qp, np.zeros((n + 4, n + 4)), 2, 1.0, 1.0, kinds=("wall",) * 4)
+    n64 = ref.run(t_end=t_end)
+    mx, rmse = _stats(s.depth(), ref.q[0][2:-2, 2:-2])
+    print(f"\ndam break {n}x{n}, t={t_end}s: steps fp32={n32} fp64={n64}; depth max {mx:.3g} m, RMSE {rmse:.3g} m")
+    assert abs(n32 - n64) <= 1
+    assert rmse < 1e-4 and mx < 5e-3
+
+
+def test_rain_on_terrain_fp32_gpu_vs_fp64():
+    import bench
+    r = bench.fp64_depth_error(96, 600.0)
+    print(f"\n{r}")
+    assert r["rmse_m"] < 5e-4 and r["max_m"] < 5e-2

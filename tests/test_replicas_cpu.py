@@ -1,0 +1,34 @@
+"""bench.py under torchrun runs one independent replica per rank (the step does not
+shard); the only collective is the max over ranks of the timed region. Two gloo ranks
+on the CPU check that reduction and that every rank sees the same value."""
+import os
+import socket
+
+import pytest
+
+torch = pytest.importorskip("torch")
+import torch.distributed as dist  # noqa: E402
+import torch.multiprocessing as mp  # noqa: E402
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+    out[rank] = bench.max_over_ranks(10.0 + 5.0 * rank, "cpu")
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_max_over_ranks_gloo_world_2():
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_rank, args=(2, _free_port(), out), nprocs=2, start_method="spawn", join=True)
+        assert dict(out) == {0: 15.0, 1: 15.0}
