@@ -34,11 +34,37 @@ def test_dam_break_fp32_gpu_vs_fp64():
 
 
 def test_rain_on_terrain_fp32_gpu_vs_fp64():
+    """Thin films on steep terrain amplify fp32 rounding of the bed source (small
+    differences of large bed values), so the bar is the reference's own fp32 CUDA kernel
+    (its kernel text compiled in oracle/_ref, strict and as NVRTC builds it) measured
+    against the same fp64 run: the product's error is within 1.5x of the larger of the
+    two. The reference's NumPy fp32 path, which accumulates the bed source in float64,
+    is reported beside them."""
     import bench
-    r = bench.fp64_depth_error(96, 600.0)
-    print(f"\n{r}")
-    # thin films on steep terrain amplify fp32 rounding; the bar is the reference's own
-    # fp32 path measured against the same fp64 run (within 3x of its error)
-    ref = r["reference_fp32_cpu_vs_fp64"]
+    from oracle import ref_runner
+    from tests._cases import pad_state
+    from geoswe_b200.synthetic import MANNING_CLASSES, fractal_bed, voronoi_classes
+    n, t_end = 96, 600.0
+    r = bench.fp64_depth_error(n, t_end)
+    from oracle import numpy_ref
+    ref64 = numpy_ref._rain_on_terrain_solver(n, dtype=np.float64)
+    ref64.run(t_end=t_end)
+    h64 = ref64.q[0][2:-2, 2:-2]
+    out = {}
+    if ref_runner.available("fma"):
+        z = fractal_bed(n, n, 3.0, seed=0).astype(np.float32)
+        clsp = np.pad(voronoi_classes(n, n, seed=0), 2, mode="edge")
+        qp, bp = pad_state(np.zeros((3, n, n), np.float32), z, 2, np.float32)
+        for variant in ("strict", "fma"):
+            k = ref_runner.RefDenseGPU(qp, bp, 2, 3.0, 3.0, kinds=["wall", "fall", "wall", "wall"], ncls=clsp,
+                                       ntab=MANNING_CLASSES, friction=True, rain_rate=50.0 / 3.6e6,
+                                       variant=variant)
+            steps = k.run(t_end=t_end)
+            out[variant] = (steps, _stats(k.q[0].cpu().numpy()[2:-2, 2:-2], h64))
+    print(f"\n{r}\nreference CUDA fp32 vs fp64 (steps, (max, rmse)): {out}")
     assert abs(r["steps_fp32_gpu"] - r["steps_fp64_cpu"]) <= max(5, r["steps_fp64_cpu"] // 200)
-    assert r["rmse_m"] <= max(3.0 * ref["rmse_m"], 1e-4)
+    if out:
+        worst = max(v[1][1] for v in out.values())
+        assert r["rmse_m"] <= 1.5 * worst
+    else:
+        assert r["rmse_m"] < 5e-3
