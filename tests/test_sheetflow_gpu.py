@@ -1,0 +1,51 @@
+"""Known answer: steady sheet flow on a rained plane (the reference's verification case
+of its paper's Sect. 5.5). Rain on a 300 m plane of slope 0.015, Manning n = 0.12,
+walled laterally, draining into a toe pit; the run goes to steady state and the mean
+cross-slope depth over x = 30..294 m is scored against the exact steady profile
+(oracle/sheetflow.py). The production configuration (SRM-HLLC, Euler, quadratic
+point-implicit Manning, keep-h wet/dry, fp32) must land on the reference's own
+published mean error within 0.25 percentage points, and the run must be steady."""
+import numpy as np
+import pytest
+
+from oracle import sheetflow
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _plane(rate_mm_h, dx, t_end, ny=16, n_pit=10, S=0.015, n_man=0.12):
+    from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
+    n_plane = int(round(300.0 / dx))
+    nx = n_plane + n_pit
+    bed = np.zeros((nx, ny), np.float32)
+    for i in range(n_plane):
+        bed[i, :] = S * dx * (n_plane - i - 0.5)
+    bed[n_plane:, :] = -5.0
+    rain = np.zeros((1, nx, ny))
+    rain[0, :n_plane, :] = rate_mm_h
+    cfg = Config(bc_x="wall", bc_y="wall", cfl=0.5, friction="manning", friction_quadratic_alpha=True,
+                 h_min=1e-6, h_min_cfl=1e-3, rainfall_forcing=RainfallForcing(time_s=[0.0], rate_mm_h=rain))
+    s = Solver2D(Mesh2D(nx=nx, ny=ny, dx=dx, dy=dx, ngh=2), cfg, np.zeros((3, nx, ny), np.float32), bed)
+    s.set_manning_table(np.zeros((nx + 4, ny + 4), np.uint8), np.array([n_man], np.float32))
+    s.run(t_end=t_end * 2.0 / 3.0)
+    mid = s.depth().mean(axis=1)[:n_plane].astype(np.float64)
+    steps = s.run(t_end=t_end)
+    prof = s.depth().mean(axis=1)[:n_plane].astype(np.float64)
+    return prof, mid, n_plane
+
+
+@pytest.mark.parametrize("rate,dx,t_end", [(22.04, 3.0, 21600.0), (348.0, 3.0, 3600.0), (22.04, 1.0, 21600.0)])
+def test_sheetflow_matches_exact_profile(rate, dx, t_end):
+    prof, mid, n_plane = _plane(rate, dx, t_end)
+    x = sheetflow.plane_x(dx, n_plane)
+    h_ex = sheetflow.exact_profile(x, rate / 3.6e6)
+    b = sheetflow.band(dx)
+    err = (prof[b] - h_ex[b]) / h_ex[b]
+    drift = float(np.abs(prof - mid)[b].max())
+    pub = sheetflow.PUBLISHED_MEAN_ERROR[(rate, dx)]
+    print(f"\nrate {rate} mm/h dx {dx} m: film {prof[b].min()*1e3:.1f}-{prof[b].max()*1e3:.1f} mm, "
+          f"mean error {err.mean()*100:+.3f} % (reference published {pub*100:+.2f} %), "
+          f"range {err.min()*100:+.2f}..{err.max()*100:+.2f} %, drift {drift*1e3:.4f} mm")
+    assert drift < 1e-4
+    assert abs(err.mean() - pub) < 0.0025
