@@ -84,7 +84,8 @@ class GswFlatArgs(C.Structure):
                 ("inv_dx", f64), ("inv_dy", f64), ("g", f64), ("h_min", f64), ("h_min_cfl", f64),
                 ("linf", i32), ("rain_kind", i32), ("state", vp), ("lam_target", vp), ("rain", vp),
                 ("ngh", i32), ("nx", i32), ("ny", i32), ("n_tab_len", i32), ("n_cls", vp), ("n_tab", vp),
-                ("vcap", f64), ("quadratic", i32), ("keep_h", i32), ("max_h", vp)]
+                ("vcap", f64), ("quadratic", i32), ("keep_h", i32), ("max_h", vp), ("rain_lookup", vp),
+                ("rain_ncol", i32), ("reserved2", i32)]
 
 
 class GswFlatInflowArgs(C.Structure):

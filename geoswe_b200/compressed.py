@@ -119,20 +119,13 @@ class CompressedSolver:
                           f"carried over. The compressed mesh closes its edge with the state stored in its "
                           f"ghost halo, which acts like the 'fall' boundary.", stacklevel=2)
         self = cls()
-        self.brick_h = int(brick_h or cls.brick_h)
-        self.device = s.device
-        self.nxp, self.nyp, self.ngh = s.nxp, s.nyp, s.mesh.ngh
-        self.nx, self.ny = s.mesh.nx, s.mesh.ny
-        self.dx = float(s.mesh.dx)
-        self.g = float(cfg.g if g is None else g)
-        self.cfl = float(cfg.cfl if cfl is None else cfl)
-        self.h_min = max(float(cfg.h_min), 1.0e-6) if h_min is None else float(h_min)
-        self.h_min_cfl = max(self.h_min, 1.0e-6)
-        self.cfl_linf = bool(cfl_linf)
-        self.vcap = float(cfg.friction_velocity_cap_ms)
-        self.quad = bool(cfg.friction_quadratic_alpha)
-        self.keep_h = bool(cfg.wetdry_keep_h)
-        self.dt_max_user = dt_max
+        self._init_physics(device=s.device, nxp=s.nxp, nyp=s.nyp, ngh=s.mesh.ngh, nx=s.mesh.nx, ny=s.mesh.ny,
+                           dx=float(s.mesh.dx), g=float(cfg.g if g is None else g),
+                           cfl=float(cfg.cfl if cfl is None else cfl),
+                           h_min=max(float(cfg.h_min), 1.0e-6) if h_min is None else float(h_min),
+                           cfl_linf=cfl_linf, vcap=float(cfg.friction_velocity_cap_ms),
+                           quad=bool(cfg.friction_quadratic_alpha), keep_h=bool(cfg.wetdry_keep_h),
+                           dt_max=dt_max, brick_h=brick_h)
         self._dense_had_rain = cfg.rainfall_forcing is not None or cfg.rainfall > 0.0
         t0 = time.perf_counter()
         dev = self.device
@@ -142,8 +135,153 @@ class CompressedSolver:
             inside[g_:-g_, g_:-g_] = 1
         else:
             inside = s._mask[:, :s.nyp].contiguous()
+        sl, lin, ii, jj = self._build_layout(inside)
+        pidx_of_slot = ii * s.pitch + jj
+
+        def pack_dense(field2d_pitched, dtype=torch.float32):
+            out = torch.zeros(self.nslots, dtype=dtype, device=dev)
+            out[sl] = field2d_pitched.reshape(-1)[pidx_of_slot].to(dtype)
+            return out
+
+        q = s._buf[s._cur]
+        self._q = [[pack_dense(q[c]) for c in range(3)], [torch.zeros(self.nslots, device=dev) for _ in range(3)]]
+        self._cur = 0
+        self._b = pack_dense(s._b)
+        T = s._tables()
+        if T.fkind == L.FRICTION_TABLE and T.ncls is not None:
+            self._ncls = pack_dense(T.ncls, torch.uint8)
+            self._ntab = T.ntab.to(torch.float32).clone()
+        elif T.fkind == L.FRICTION_FIELD:
+            nf = T.nfield[:, :s.nyp].cpu().numpy()
+            vals, inv = np.unique(nf, return_inverse=True)
+            if vals.size > 256:
+                raise ValueError("the compressed mesh stores Manning's n as a table of at most 256 classes")
+            clsp = np.zeros((s.nxp, s.pitch), np.uint8)
+            clsp[:, :s.nyp] = inv.reshape(nf.shape)
+            self._ncls = pack_dense(torch.from_numpy(clsp).to(dev), torch.uint8)
+            self._ntab = torch.from_numpy(vals.astype(np.float32)).to(dev)
+        else:
+            n = float(np.float32(cfg.manning_n)) if cfg.friction is not None else 0.0
+            self._ncls = None
+            self._ntab = torch.tensor([n], dtype=torch.float32, device=dev)
+        self._init_runtime(track_max_depth)
+        self.build_seconds = time.perf_counter() - t0
+        if say:
+            say(f"[compressed] N_active={self.N_active} N_stored={self.N_stored} bricks={self.n_bricks} "
+                f"built in {self.build_seconds:.2f}s")
+        return self
+
+    @classmethod
+    def from_cache(cls, cache_dir, *, cfl: float = 0.5, h_min: float = 1e-6, g: float = 9.81, dt_max=None,
+                   cfl_linf: bool = False, brick_h: Optional[int] = None, track_max_depth: bool = True,
+                   device=None, say=None):
+        """Load a flat-mesh cache in the reference's format (save_cache /
+        run_cached, compressed_solver.py:2504-2560, 2616-2780): meta.json plus .npy files
+        (nbr int16 deltas, is_active, ij_active, q0..q2, bed_f, mcls_f, m_tab, and the
+        ring and rain bundles), straight to the GPU without a dense domain. Physics
+        scalars are the cached loop's (CFL, h_min, g as given; quadratic Manning, keep-h,
+        15 m/s velocity cap). Multi-rank caches, porosity (Sigma), sponge and drain bundles
+        are refused with an error."""
+        import json
+        import os
+        t0 = time.perf_counter()
+        path = lambda n: os.path.join(cache_dir, n)
+        meta = json.load(open(path("meta.json")))
+        if meta.get("mpi") or int(meta.get("nranks", 1)) != 1:
+            raise NotImplementedError("from_cache: multi-rank caches are not supported (one GPU per solver)")
+        for key, what in (("has_sponge", "sponge"), ("has_drain", "drain")):
+            if meta.get(key):
+                raise NotImplementedError(f"from_cache: the cache holds a {what} bundle, which this solver "
+                                          f"does not apply")
+        ld = lambda n: np.load(path(n + ".npy"))
+        nbr = ld("nbr")
+        is_active = ld("is_active").astype(np.uint8)
+        ij = ld("ij_active").astype(np.int64)
+        N = int(is_active.shape[0])
+        if int(meta.get("N", N)) != N or nbr.shape[0] != N or ij.shape[0] != N:
+            raise RuntimeError(f"cache {cache_dir}: inconsistent row counts (torn or mixed-vintage cache)")
+        if not bool(meta.get("no_sigma", True)) and os.path.exists(path("sig_f.npy")) and ld("sig_f").any():
+            raise NotImplementedError("from_cache: porosity (Sigma) caches are not supported")
+        nxp, nyp, ngh = int(meta["nxp"]), int(meta["nyp"]), int(meta["ngh"])
+        self = cls()
+        dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self._init_physics(device=dev, nxp=nxp, nyp=nyp, ngh=ngh, nx=nxp - 2 * ngh, ny=nyp - 2 * ngh,
+                           dx=float(meta["dx"]), g=g, cfl=cfl, h_min=max(float(h_min), 1.0e-6),
+                           cfl_linf=cfl_linf, vcap=15.0, quad=True, keep_h=True, dt_max=dt_max, brick_h=brick_h)
+        self.cache_meta = meta
+        inside = np.zeros((nxp, nyp), np.uint8)
+        act = is_active != 0
+        inside[ij[act, 0], ij[act, 1]] = 1
+        self._build_layout(torch.from_numpy(inside).to(dev))
+        stored = self._stored.cpu().numpy()
+        canon_ij = np.argwhere(stored)
+        if self.N_stored != N or not np.array_equal(canon_ij, ij):
+            raise ValueError(f"cache {cache_dir}: its stored cells are not the two-cell ring of its active set "
+                             f"in row-major order")
+        slot = self._slot
+
+        def pack(flat, dtype):
+            out = torch.zeros(self.nslots, dtype=dtype, device=dev)
+            out[slot] = torch.from_numpy(np.ascontiguousarray(flat)).to(dev).to(dtype)
+            return out
+
+        self._q = [[pack(ld(f"q{c}").astype(np.float32), torch.float32) for c in range(3)],
+                   [torch.zeros(self.nslots, device=dev) for _ in range(3)]]
+        self._cur = 0
+        self._b = pack(ld("bed_f").astype(np.float32), torch.float32)
+        self._ncls = pack(ld("mcls_f").astype(np.uint8), torch.uint8)
+        self._ntab = torch.from_numpy(ld("m_tab").astype(np.float32).reshape(-1)).to(dev)
+        self._init_runtime(track_max_depth)
+        if meta.get("has_rain"):
+            if os.path.exists(path("rain_lookup_flat.npz")):
+                lookup = np.load(path("rain_lookup_flat.npz"))["lookup_flat"]
+            else:
+                lookup = ld("rain_lookup_flat")
+            table = ld("rain_native_rate_dev").astype(np.float32)
+            table = table.reshape(table.shape[0], -1)
+            self._set_rain_table(np.asarray(ld("rain_t_s"), np.float64), table, pack(lookup.astype(np.int32),
+                                                                                     torch.int32))
+        if meta.get("has_ring"):
+            rflat = ld("ring_rflat").astype(np.int64).reshape(-1)
+            n, NG = int(meta["ring_n"]), int(meta["ring_NG"])
+            if rflat.size and int(rflat.max()) >= N:
+                raise RuntimeError(f"cache {cache_dir}: ring_rflat max >= N={N} (torn cache)")
+            rf = torch.from_numpy(rflat).to(dev)
+            slots = torch.where(rf >= 0, slot[rf.clamp_min(0)], torch.full_like(rf, -1))
+            self._ring = dict(slots=slots.contiguous(), n=n, NG=NG,
+                              bed=torch.from_numpy(ld("ring_rbed").astype(np.float32).reshape(-1)).to(dev),
+                              wg=torch.from_numpy(ld("ring_rwg").astype(np.float32).reshape(n, NG)).to(dev),
+                              t=torch.from_numpy(ld("ring_t_common").astype(np.float64).reshape(-1)).to(dev),
+                              stage=torch.from_numpy(np.ascontiguousarray(
+                                  ld("ring_stage_all").astype(np.float32).reshape(NG, -1))).to(dev))
+        self.build_seconds = time.perf_counter() - t0
+        if say:
+            say(f"[compressed] loaded {cache_dir}: N_active={self.N_active} N_stored={self.N_stored} "
+                f"bricks={self.n_bricks} in {self.build_seconds:.2f}s")
+        return self
+
+    # ------------------------------------------------------------- construction
+    def _init_physics(self, *, device, nxp, nyp, ngh, nx, ny, dx, g, cfl, h_min, cfl_linf, vcap, quad, keep_h,
+                      dt_max, brick_h):
+        self.brick_h = int(brick_h or type(self).brick_h)
+        self.device = torch.device(device)
+        self.nxp, self.nyp, self.ngh = int(nxp), int(nyp), int(ngh)
+        self.nx, self.ny = int(nx), int(ny)
+        self.dx = float(dx)
+        self.g, self.cfl, self.h_min = float(g), float(cfl), float(h_min)
+        self.h_min_cfl = max(self.h_min, 1.0e-6)
+        self.cfl_linf = bool(cfl_linf)
+        self.vcap, self.quad, self.keep_h = float(vcap), bool(quad), bool(keep_h)
+        self.dt_max_user = dt_max
+        self._dense_had_rain = False
+
+    def _build_layout(self, inside):
+        """Stored set (the inside mask dilated twice with the 4-neighbour cross,
+        compressed_rhs.py:256), Hilbert bricks, the canonical id -> slot map and the slot
+        flags. `inside` is a device uint8 (nxp, nyp) mask. Returns (slots, padded linear
+        index, i, j) of every stored cell."""
+        dev = self.device
         self._inside = inside
-        # stored = inside dilated twice with the 4-neighbour cross (compressed_rhs.py:256)
         st = inside.bool()
         for _ in range(2):
             d = st.clone()
@@ -168,9 +306,9 @@ class CompressedSolver:
         r_, c_ = rem // BRICK_PITCH, rem % BRICK_PITCH
         ii = self._bij[b_, 0].to(torch.int64) * self.brick_h + r_
         jj = self._bij[b_, 1].to(torch.int64) * BRICK_W + c_
-        ok = (c_ < BRICK_W) & (ii < s.nxp) & (jj < s.nyp)
+        ok = (c_ < BRICK_W) & (ii < self.nxp) & (jj < self.nyp)
         ii, jj, sl = ii[ok], jj[ok], sl[ok]
-        lin = ii * s.nyp + jj
+        lin = ii * self.nyp + jj
         keep = st.reshape(-1)[lin]
         ii, jj, sl, lin = ii[keep], jj[keep], sl[keep], lin[keep]
         canon = torch.cumsum(st.reshape(-1).to(torch.int64), 0) - 1
@@ -181,37 +319,13 @@ class CompressedSolver:
         flags = torch.zeros(self.nslots, dtype=torch.uint8, device=dev)
         flags[sl] = (1 + 2 * inside.reshape(-1)[lin].to(torch.uint8))
         self._flags = flags
-        pidx_of_slot = ii * s.pitch + jj
-
-        def pack_dense(field2d_pitched, dtype=torch.float32):
-            out = torch.zeros(self.nslots, dtype=dtype, device=dev)
-            out[sl] = field2d_pitched.reshape(-1)[pidx_of_slot].to(dtype)
-            return out
-
         self._tables_cache = None
         self._slot_cells = sl
         self._lin_of_slot = lin
-        q = s._buf[s._cur]
-        self._q = [[pack_dense(q[c]) for c in range(3)], [torch.zeros(self.nslots, device=dev) for _ in range(3)]]
-        self._cur = 0
-        self._b = pack_dense(s._b)
-        T = s._tables()
-        if T.fkind == L.FRICTION_TABLE and T.ncls is not None:
-            self._ncls = pack_dense(T.ncls, torch.uint8)
-            self._ntab = T.ntab.to(torch.float32).clone()
-        elif T.fkind == L.FRICTION_FIELD:
-            nf = T.nfield[:, :s.nyp].cpu().numpy()
-            vals, inv = np.unique(nf, return_inverse=True)
-            if vals.size > 256:
-                raise ValueError("the compressed mesh stores Manning's n as a table of at most 256 classes")
-            clsp = np.zeros((s.nxp, s.pitch), np.uint8)
-            clsp[:, :s.nyp] = inv.reshape(nf.shape)
-            self._ncls = pack_dense(torch.from_numpy(clsp).to(dev), torch.uint8)
-            self._ntab = torch.from_numpy(vals.astype(np.float32)).to(dev)
-        else:
-            n = float(np.float32(cfg.manning_n)) if cfg.friction is not None else 0.0
-            self._ncls = None
-            self._ntab = torch.tensor([n], dtype=torch.float32, device=dev)
+        return sl, lin, ii, jj
+
+    def _init_runtime(self, track_max_depth):
+        dev = self.device
         self._max_h = torch.zeros(self.nslots, dtype=torch.float32, device=dev) if track_max_depth else None
         self._state = torch.zeros(128, dtype=torch.uint8, device=dev)
         self._state_host = torch.zeros(128, dtype=torch.uint8).pin_memory()
@@ -219,6 +333,8 @@ class CompressedSolver:
         self._rain_kind = L.RAIN_NONE
         self._rain_t = None
         self._rain_rmax = 0.0
+        self._rain_lookup = None
+        self._rain_ncol = 0
         self._inflows = []
         self._ring = None
         self.warps, self.min_blocks = 0, 0
@@ -230,17 +346,14 @@ class CompressedSolver:
         self.t = 0.0
         self.nsteps = 0
         self.kernel_launches = 0
-        self.build_seconds = time.perf_counter() - t0
-        if say:
-            say(f"[compressed] N_active={self.N_active} N_stored={self.N_stored} bricks={self.n_bricks} "
-                f"built in {self.build_seconds:.2f}s")
-        return self
 
     # ------------------------------------------------------------- forcings
     def set_rain(self, rain):
         """Attach a RainfallForcing (uniform or (nt, nx, ny) gridded)."""
         if rain is None:
             self._rain, self._rain_kind, self._rain_t = None, L.RAIN_NONE, None
+            self._rain_lookup, self._rain_ncol = None, 0
+            self._graph_cache.clear()
             return self
         rate = np.asarray(rain.rate_mm_h)
         t_s = np.asarray(rain.time_s, np.float64)
@@ -258,6 +371,17 @@ class CompressedSolver:
         self._rain_rmax = float(table.max())
         self._graph_cache.clear()
         return self
+
+    def _set_rain_table(self, t_s, table, lookup_slots):
+        """Rain as the reference's flat bundle: a (nt, ncol) table of rates (m/s), the
+        frame times, and per slot the column it reads (compressed_solver.py:3273-3282)."""
+        self._rain = torch.from_numpy(np.ascontiguousarray(table, np.float32)).to(self.device)
+        self._rain_t = torch.from_numpy(np.asarray(t_s, np.float64).copy()).to(self.device)
+        self._rain_kind = L.RAIN_LOOKUP
+        self._rain_lookup = lookup_slots.to(torch.int32).contiguous()
+        self._rain_ncol = int(table.shape[1])
+        self._rain_rmax = float(np.max(table)) if table.size else 0.0
+        self._graph_cache.clear()
 
     def ghost_boundary_pairs(self):
         """Ghost (ring) cells that touch the active set, each with its first active
@@ -439,6 +563,7 @@ class CompressedSolver:
             a.lam_target = C.c_void_p(self._state.data_ptr() + L.GswLoopState.lam_bits.offset)
             a.rain_kind = self._rain_kind
             a.rain = _ptr(self._rain)
+            a.rain_lookup, a.rain_ncol = _ptr(self._rain_lookup), int(self._rain_ncol)
             a.n_cls, a.n_tab, a.n_tab_len = _ptr(self._ncls), _ptr(self._ntab), int(self._ntab.numel())
             a.vcap, a.quadratic, a.keep_h = self.vcap, int(self.quad), int(self.keep_h)
             a.max_h = _ptr(self._max_h)
@@ -493,12 +618,28 @@ class CompressedSolver:
         n = self.N_stored
         return 256 if n <= 1 << 20 else (64 if n <= 1 << 24 else 16)
 
-    def run(self, t_end=None, *, dt_max=None, max_steps: int = 10 ** 9, window: int = 0, say=None, **unused):
+    def run(self, t_end=None, *, dt_max=None, max_steps: int = 10 ** 9, window: int = 0, say=None,
+            checkpoint_every_s: float = 0.0, ckpt_dir=None, resume: bool = False, **unused):
         """Step from the current time to ``t_end`` (the reference's flat loop,
         compressed_solver.py:2133-2448): dt from the previous step's wave speed, the rain
-        film limit folded into dt_max, dt = min(dt, t_end - t). Returns the number of steps."""
+        film limit folded into dt_max, dt = min(dt, t_end - t). Returns the number of steps.
+
+        Checkpoints (compressed_solver.py:1789-1936): with ``checkpoint_every_s`` and
+        ``ckpt_dir`` the state, time and step count are written in the reference's format
+        (ckpt_r00.npz + ckpt_meta.json, each replaced atomically) at the first window
+        boundary past every interval, and once more at the end; ``resume=True`` first
+        restores the checkpoint in ``ckpt_dir`` if there is one. A resumed run continues
+        the uninterrupted trajectory bit for bit (checkpoints sit on step boundaries and
+        do not clip dt)."""
         if t_end is None:
             raise TypeError("CompressedSolver.run() needs t_end, the end time in seconds")
+        if resume and ckpt_dir is not None:
+            self.load_checkpoint(ckpt_dir, missing_ok=True)
+        every = float(checkpoint_every_s or 0.0)
+        if every > 0.0 and ckpt_dir is None:
+            raise ValueError("CompressedSolver.run: checkpoint_every_s needs ckpt_dir")
+        next_ckpt = self.t + every if every > 0.0 else float("inf")
+        steps0 = self.nsteps
         if self._rain is None and self._dense_had_rain:
             warnings.warn("CompressedSolver.run: the dense Config asked for rainfall and none was attached "
                           "here. from_dense does not carry rainfall over; pass the same RainfallForcing "
@@ -542,8 +683,16 @@ class CompressedSolver:
         while True:
             g.replay()
             self.kernel_launches += per
-            if self._read_state().done:
+            st = self._read_state()
+            if st.done:
                 break
+            if every > 0.0:
+                executed = int(st.steps) + int(st.pending)
+                t_now = float(st.t_new) if st.pending else float(st.t)
+                if t_now >= next_ckpt:
+                    self._write_checkpoint(ckpt_dir, self._q[(start + executed) % 2], t_now, steps0 + executed)
+                    while next_ckpt <= t_now:
+                        next_ckpt += every
         L.call("gsw_loop_commit", _ptr(self._state), _stream())
         self.kernel_launches += 1
         st = self._read_state()
@@ -556,4 +705,112 @@ class CompressedSolver:
         if st.error == L.ERR_NONFINITE:
             raise FloatingPointError(f"cfl_dt: non-finite max wave speed at t={self.t:.3f}s "
                                      f"-- fp32 NaN/Inf in the state; check forcing/inputs")
+        if every > 0.0:
+            self._write_checkpoint(ckpt_dir, self._q[self._cur], self.t, self.nsteps)
         return steps
+
+    # ------------------------------------------------------- cache, checkpoints
+    def _canonical_of_slot(self):
+        c = torch.full((self.nslots,), -1, dtype=torch.int64, device=self.device)
+        c[self._slot] = torch.arange(self.N_stored, device=self.device)
+        return c
+
+    def _write_checkpoint(self, ckpt_dir, q, t, steps):
+        import json
+        import os
+        os.makedirs(ckpt_dir, exist_ok=True)
+        arrays = {f"q{c}": q[c][self._slot].cpu().numpy() for c in range(3)}
+        if self._max_h is not None:
+            arrays["max_h"] = self._max_h[self._slot].cpu().numpy()
+        tmp = os.path.join(ckpt_dir, "ckpt_r00_tmp")
+        np.savez(tmp, t=np.float64(t), steps=np.int64(steps), **arrays)
+        os.replace(tmp + ".npz", os.path.join(ckpt_dir, "ckpt_r00.npz"))
+        meta = dict(t=float(t), steps=int(steps), fidx=0, next_frame=0.0, nranks=1)
+        mt = os.path.join(ckpt_dir, "ckpt_meta.json.tmp")
+        with open(mt, "w") as f:
+            json.dump(meta, f)
+        os.replace(mt, os.path.join(ckpt_dir, "ckpt_meta.json"))
+
+    def load_checkpoint(self, ckpt_dir, missing_ok: bool = False):
+        """Restore state, time and step count from a checkpoint in the reference's format
+        (ckpt_meta.json + ckpt_r00.npz). Returns False when there is none and
+        `missing_ok`."""
+        import json
+        import os
+        mp = os.path.join(ckpt_dir, "ckpt_meta.json")
+        if not os.path.exists(mp):
+            if missing_ok:
+                return False
+            raise FileNotFoundError(mp)
+        meta = json.load(open(mp))
+        if int(meta.get("nranks", 1)) != 1:
+            raise RuntimeError(f"checkpoint nranks={meta['nranks']} != 1; resume with the same rank count")
+        z = np.load(os.path.join(ckpt_dir, "ckpt_r00.npz"))
+        if "t" in z.files and (abs(float(z["t"]) - float(meta["t"])) > 1e-9 or int(z["steps"]) != int(meta["steps"])):
+            raise RuntimeError("torn checkpoint: the state file and ckpt_meta.json disagree on (t, steps)")
+        for c in range(3):
+            qc = np.asarray(z[f"q{c}"], np.float32).reshape(-1)
+            if qc.size != self.N_stored:
+                raise ValueError(f"checkpoint has {qc.size} cells, the mesh {self.N_stored}")
+            self._q[self._cur][c][self._slot] = torch.from_numpy(qc).to(self.device)
+        if self._max_h is not None:
+            if "max_h" in z.files:
+                self._max_h[self._slot] = torch.from_numpy(np.asarray(z["max_h"], np.float32)).to(self.device)
+            else:
+                warnings.warn("load_checkpoint: no max_h in the checkpoint; the max-depth envelope only "
+                              "covers the resumed window", RuntimeWarning, stacklevel=2)
+        self.t = float(meta["t"])
+        self.nsteps = int(meta["steps"])
+        return True
+
+    def save_cache(self, cache_dir, *, x0: float = 0.0, y0: float = 0.0, crs_wkt: str = "",
+                   nx_glob: Optional[int] = None, ny_glob: Optional[int] = None):
+        """Write the mesh, state, Manning table and the rain / ring bundles in the
+        reference's cache format (save_cache, compressed_solver.py:2504-2560), which its
+        run_cached and from_cache here both read. Inlets are not part of the format (the
+        reference passes them to run_cached)."""
+        import json
+        import os
+        os.makedirs(cache_dir, exist_ok=True)
+        sv = lambda n, a: np.save(os.path.join(cache_dir, n + ".npy"), np.asarray(a))
+        tab = self._canonical()
+        N = self.N_stored
+        sl = self._slot
+        sv("nbr", tab["nbr"]); sv("is_active", tab["is_active"]); sv("ij_active", tab["ij"])
+        q = self._q[self._cur]
+        for c in range(3):
+            sv(f"q{c}", q[c][sl].cpu().numpy().astype(np.float32))
+        sv("bed_f", self._b[sl].cpu().numpy().astype(np.float32))
+        sv("sig_f", np.zeros(N, np.float32)); sv("inv_sig_f", np.ones(N, np.float32))
+        mc = self._ncls[sl].cpu().numpy() if self._ncls is not None else np.zeros(N, np.uint8)
+        sv("mcls_f", mc.astype(np.uint8)); sv("m_tab", self._ntab.cpu().numpy().astype(np.float32))
+        meta = dict(nxp=self.nxp, nyp=self.nyp, ngh=self.ngh, dx=self.dx, x0=float(x0), y0=float(y0),
+                    crs_wkt=str(crs_wkt), nx_glob=int(nx_glob if nx_glob is not None else self.nx),
+                    ny_glob=int(ny_glob if ny_glob is not None else self.ny), has_ring=self._ring is not None,
+                    has_sponge=False, has_rain=self._rain is not None, no_sigma=True, N=int(N), nranks=1,
+                    mpi=False)
+        if self._rain is not None:
+            table = self._rain.cpu().numpy().astype(np.float32)
+            if self._rain_kind == L.RAIN_UNIFORM:
+                table, lookup = table.reshape(-1, 1), np.zeros(N, np.int32)
+            elif self._rain_kind == L.RAIN_GRIDDED:
+                ij = tab["ij"].astype(np.int64)
+                ii, jj = ij[:, 0] - self.ngh, ij[:, 1] - self.ngh
+                inner = (ii >= 0) & (ii < self.nx) & (jj >= 0) & (jj < self.ny)
+                lookup = np.where(inner, ii * self.ny + jj, 0).astype(np.int32)
+                table = table.reshape(table.shape[0], -1)
+            else:
+                lookup = self._rain_lookup[sl].cpu().numpy().astype(np.int32)
+            sv("rain_native_rate_dev", table); sv("rain_lookup_flat", lookup)
+            sv("rain_t_s", self._rain_t.cpu().numpy())
+        if self._ring is not None:
+            r = self._ring
+            canon = self._canonical_of_slot()
+            rs = r["slots"]
+            rflat = torch.where(rs >= 0, canon[rs.clamp_min(0)], torch.full_like(rs, -1))
+            sv("ring_rflat", rflat.cpu().numpy().astype(np.int32)); sv("ring_rbed", r["bed"].cpu().numpy())
+            sv("ring_rwg", r["wg"].cpu().numpy().reshape(-1)); sv("ring_t_common", r["t"].cpu().numpy())
+            sv("ring_stage_all", r["stage"].cpu().numpy())
+            meta["ring_NG"], meta["ring_n"] = int(r["NG"]), int(r["n"])
+        with open(os.path.join(cache_dir, "meta.json"), "w") as f:
+            json.dump(meta, f)

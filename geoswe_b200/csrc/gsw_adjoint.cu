@@ -349,6 +349,7 @@ static int fill_adj(const GswFlatAdjArgs* a, AdjK<T>& k) {
         return set_error(GSW_ERR_INVALID, "adjoint: bad flat arguments");
     if (f.n_tab_len > 256) return set_error(GSW_ERR_RANGE, "adjoint: at most 256 Manning classes");
     if (f.rain_kind != GSW_RAIN_NONE && !f.rain) return set_error(GSW_ERR_INVALID, "adjoint: rain is NULL");
+    if (f.rain_kind == GSW_RAIN_LOOKUP) return set_error(GSW_ERR_INVALID, "adjoint: lookup rain is not differentiated");
     if (!a->lam_in0 || !a->lam_in1 || !a->lam_in2 || !a->lam_out0 || !a->lam_out1 || !a->lam_out2 ||
         !a->rbar0 || !a->rbar1 || !a->rbar2 || !a->n_bar)
         return set_error(GSW_ERR_INVALID, "adjoint: null adjoint buffer");
@@ -364,6 +365,7 @@ static int fill_adj(const GswFlatAdjArgs* a, AdjK<T>& k) {
     ph.linf = f.linf; ph.quad = f.quadratic; ph.keep_h = f.keep_h;
     ph.rain_kind = f.rain_kind; ph.rain = (const T*)f.rain; ph.ngh = f.ngh; ph.nx = f.nx; ph.ny = f.ny;
     ph.ntab = (const T*)f.n_tab;
+    ph.lookup = f.rain_lookup; ph.ncol = f.rain_ncol;
     k.st = f.state;
     k.li0 = (const T*)a->lam_in0; k.li1 = (const T*)a->lam_in1; k.li2 = (const T*)a->lam_in2;
     k.lo0 = (T*)a->lam_out0; k.lo1 = (T*)a->lam_out1; k.lo2 = (T*)a->lam_out2;

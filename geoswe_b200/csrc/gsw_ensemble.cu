@@ -20,7 +20,7 @@ __device__ __forceinline__ FlatPhys<float> member_phys(const GswMember& mb) {
     ph.g = mb.g; ph.h_min = mb.h_min; ph.h_min_cfl = mb.h_min_cfl; ph.vcap = mb.vcap;
     ph.linf = mb.linf; ph.quad = mb.quadratic; ph.keep_h = mb.keep_h;
     ph.rain_kind = mb.rain_kind; ph.rain = mb.rain; ph.ntab = mb.n_tab;
-    ph.ngh = 0; ph.nx = 0; ph.ny = 0;
+    ph.ngh = 0; ph.nx = 0; ph.ny = 0; ph.lookup = nullptr; ph.ncol = 0;
     return ph;
 }
 

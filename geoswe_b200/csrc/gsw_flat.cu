@@ -26,6 +26,7 @@ __global__ void __launch_bounds__(256, MINB) flat_march_kernel(FlatK<T> p) {
         dt = sizeof(T) == 4 ? (T)p.st->dt_f32 : (T)p.st->dt;
         if (p.ph.rain_kind == GSW_RAIN_UNIFORM) rate = p.ph.rain[p.st->rain_idx];
         if (p.ph.rain_kind == GSW_RAIN_GRIDDED) frame = p.ph.rain + (int64_t)p.st->rain_idx * p.ph.nx * p.ph.ny;
+        if (p.ph.rain_kind == GSW_RAIN_LOOKUP) frame = p.ph.rain + (int64_t)p.st->rain_idx * p.ph.ncol;
     }
     if (bidx < p.m.nb) lam_local = flat_brick<T, STEP>(p.m, p.ph, bidx, dt, rate, frame);
     if (STEP && p.lam != nullptr) block_max_to(lam_local, p.lam);
@@ -65,6 +66,7 @@ static int fill_flat(const GswFlatArgs* a, FlatK<T>& k, bool step) {
     ph.linf = a->linf; ph.quad = a->quadratic; ph.keep_h = a->keep_h;
     ph.rain_kind = a->rain_kind; ph.rain = (const T*)a->rain; ph.ngh = a->ngh; ph.nx = a->nx; ph.ny = a->ny;
     ph.ntab = (const T*)a->n_tab;
+    ph.lookup = a->rain_lookup; ph.ncol = a->rain_ncol;
     k.st = a->state; k.lam = (unsigned long long*)a->lam_target;
     if (step) {
         if (!a->state) return set_error(GSW_ERR_INVALID, "flat step: state is required");
@@ -72,6 +74,8 @@ static int fill_flat(const GswFlatArgs* a, FlatK<T>& k, bool step) {
         if (a->rain_kind != GSW_RAIN_NONE && !a->rain) return set_error(GSW_ERR_INVALID, "flat step: rain is NULL");
         if (a->rain_kind == GSW_RAIN_GRIDDED && (a->nx <= 0 || a->ny <= 0 || a->ngh < 0))
             return set_error(GSW_ERR_INVALID, "flat step: gridded rain needs ngh, nx, ny");
+        if (a->rain_kind == GSW_RAIN_LOOKUP && (!a->rain_lookup || a->rain_ncol < 1))
+            return set_error(GSW_ERR_INVALID, "flat step: lookup rain needs rain_lookup and rain_ncol >= 1");
         if (!m.o0 || !m.o1 || !m.o2) return set_error(GSW_ERR_INVALID, "flat step: null output");
     }
     return GSW_OK;

@@ -24,6 +24,8 @@ struct FlatPhys {
     T inv_dx, inv_dy, half_dx, half_dy, g, h_min, h_min_cfl, vcap;
     int linf, quad, keep_h, rain_kind, ngh, nx, ny;
     const T* rain; const T* ntab;
+    const int32_t* lookup;   // GSW_RAIN_LOOKUP: per-slot column of the rain row
+    int ncol;
 };
 
 // For the flat kernels' argument struct
@@ -161,6 +163,8 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
                     else if (ph.rain_kind == GSW_RAIN_GRIDDED) {
                         const int i = bi * bh + r, j = bj * GSW_BRICK_W + (lane - 1);
                         rr0 = rr0 + frame[(int64_t)(i - ph.ngh) * ph.ny + (j - ph.ngh)];
+                    } else if (ph.rain_kind == GSW_RAIN_LOOKUP) {
+                        rr0 = rr0 + frame[ph.lookup[o]];
                     }
                     T h = cur.h + dt * rr0;
                     T hu = cur.hu + dt * rhu;

@@ -263,16 +263,20 @@ typedef struct GswFlatArgs {
     double   inv_dx, inv_dy, g, h_min, h_min_cfl;     /* rounded to dtype by the kernels */
     int32_t  linf;             /* 1: CFL norm max(|u|,|v|); 0: sqrt(u^2+v^2) */
     /* step only */
-    int32_t  rain_kind;        /* GSW_RAIN_NONE / UNIFORM / GRIDDED */
+    int32_t  rain_kind;        /* GSW_RAIN_NONE / UNIFORM / GRIDDED / LOOKUP */
     const GswLoopState* state;
     uint64_t* lam_target;
-    const void* rain;          /* uniform: rates[n_frames]; gridded: frames[n_frames][nx][ny] */
+    const void* rain;          /* uniform: rates[n_frames]; gridded: frames[n_frames][nx][ny];
+                                  lookup: rows[n_frames][rain_ncol] (the reference's cached table) */
     int32_t  ngh, nx, ny;      /* dense padding and interior extents (gridded rain index) */
     int32_t  n_tab_len;
     const uint8_t* n_cls; const void* n_tab;
     double   vcap;
     int32_t  quadratic, keep_h;
     void*    max_h;            /* slot-indexed, or NULL */
+    const int32_t* rain_lookup;/* GSW_RAIN_LOOKUP: per slot, the column of rain[frame * rain_ncol + col] */
+    int32_t  rain_ncol;
+    int32_t  reserved2;
 } GswFlatArgs;
 
 /* Discharge inlet of the compressed mesh: one ghost (ring) slot per inlet cell, next to

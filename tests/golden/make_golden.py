@@ -194,6 +194,56 @@ def mesh_cases(G, out):
         out[f"mesh_{name}_covered"] = np.bool_(cs.fully_covered)
 
 
+def cache_cases(G, out_dir):
+    """A flat-mesh cache written by the reference's own save_cache (compressed_solver.py:
+    2504-2560) for a small mesh with a wet state, a two-column rain table with a per-cell
+    lookup and a two-gauge ring stage."""
+    _cupy_standin()
+    import geoswe.backend as B
+    B.raw_kernel = lambda *a, **k: None
+    B.elementwise_kernel = lambda *a, **k: None     # module-level kernels, never launched here
+    from geoswe.mesh import Mesh2D
+    from geoswe.compressed_rhs import CompressedSWE
+    import geoswe.compressed_solver as CSol
+    rng = np.random.default_rng(23)
+    nx, ny, ngh, dx = 44, 50, 2, 5.0
+    z = _fractal(nx, ny, dx, 23)[:, :] * 0.25
+    inside_int = z < np.quantile(z, 0.7)
+    inside_int[:3, :] = inside_int[-3:, :] = False
+    inside_int[:, :3] = inside_int[:, -3:] = False
+    nxp, nyp = nx + 2 * ngh, ny + 2 * ngh
+    inside = np.zeros((nxp, nyp), bool)
+    inside[ngh:-ngh, ngh:-ngh] = inside_int
+    bp = np.pad(z, ngh, mode="edge").astype(np.float32)
+    cs = CompressedSWE(Mesh2D(nx=nxp, ny=nyp, dx=1.0, dy=1.0, ngh=0), inside, ring=2)
+    ij = np.asarray(cs.cm.ij_active)
+    N = ij.shape[0]
+    bed_f = bp[ij[:, 0], ij[:, 1]].astype(np.float32)
+    eta = np.float32(np.quantile(z, 0.45))
+    q0 = np.maximum(eta - bed_f, 0.0).astype(np.float32)
+    q0 += (rng.random(N) * 0.02 * (q0 > 0)).astype(np.float32)
+    q1 = ((rng.random(N) - 0.5) * 0.05 * (q0 > 0)).astype(np.float32)
+    q2 = ((rng.random(N) - 0.5) * 0.05 * (q0 > 0)).astype(np.float32)
+    act = np.asarray(cs.is_active)
+    mcls = rng.integers(0, 3, N).astype(np.uint8)
+    m_tab = np.array([0.03, 0.05, 0.08], np.float32)
+    rain = dict(native_rate_dev=(np.array([[20.0, 60.0], [5.0, 40.0], [0.0, 10.0]]) / 3.6e6).astype(np.float32),
+                lookup_flat=((ij[:, 1] // 10) % 2).astype(np.int32), t_s=np.array([0.0, 120.0, 400.0]))
+    ring_ids = np.nonzero((act == 0) & (ij[:, 0] < nxp // 2))[0]
+    w = rng.random((ring_ids.size, 2)).astype(np.float32)
+    w /= w.sum(axis=1, keepdims=True)
+    t_c = np.arange(0.0, 1200.0, 100.0)
+    stage = np.stack([eta + 0.2 * np.sin(2 * np.pi * t_c / 600.0),
+                      eta + 0.1 * np.cos(2 * np.pi * t_c / 900.0)]).astype(np.float32)
+    ring = dict(rflat=ring_ids.astype(np.int32), rbed=bed_f[ring_ids], rwg=w.reshape(-1), t_common=t_c,
+                stage_all=stage, NG=2, n=int(ring_ids.size))
+    os.makedirs(out_dir, exist_ok=True)
+    CSol.save_cache(str(out_dir), nbr=np.asarray(cs.nbr), is_active=act, ij_active=ij, nxp=nxp, nyp=nyp, ngh=ngh,
+                    dx=dx, x0=0.0, y0=0.0, crs_wkt="", nx_glob=nx, ny_glob=ny, q0=q0, q1=q1, q2=q2, bed_f=bed_f,
+                    sig_f=np.zeros(N, np.float32), mcls_f=mcls, m_tab=m_tab, inv_sig_f=np.ones(N, np.float32),
+                    ring=ring, sponge=None, rain=rain, no_sigma=True, say=lambda *a, **k: None)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
@@ -206,6 +256,7 @@ def main():
     mesh_out = {}
     mesh_cases(G, mesh_out)
     np.savez_compressed(HERE / "reference_mesh.npz", **mesh_out)
+    cache_cases(G, HERE / "reference_cache")
     for f in ("reference_dense.npz", "reference_mesh.npz"):
         print(f, (HERE / f).stat().st_size, "bytes")
 

@@ -56,3 +56,21 @@ def test_bricks_cover_stored_cells(bh):
         for d, (da, dc) in enumerate([(-1, 0), (1, 0), (0, -1), (0, 1)]):
             exp = idx.get((a + da, c + dc), nb)
             assert bnbr[n, d] == exp
+
+
+def test_reference_cache_tables_match_builder():
+    """The golden cache written by the reference's save_cache holds the canonical tables
+    this package's host builder produces for the same active set."""
+    import json
+    from pathlib import Path
+    from geoswe_b200.compressed import build_tables
+    d = Path(__file__).resolve().parent / "golden" / "reference_cache"
+    meta = json.load(open(d / "meta.json"))
+    ij = np.load(d / "ij_active.npy")
+    act = np.load(d / "is_active.npy")
+    inside = np.zeros((meta["nxp"], meta["nyp"]), np.uint8)
+    inside[ij[act != 0, 0], ij[act != 0, 1]] = 1
+    t = build_tables(inside, ring=2)
+    assert t["N"] == meta["N"]
+    assert np.array_equal(t["ij"], ij) and np.array_equal(t["nbr"], np.load(d / "nbr.npy"))
+    assert np.array_equal(t["is_active"], act)
