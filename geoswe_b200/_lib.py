@@ -112,6 +112,15 @@ class GswFlatRingArgs(C.Structure):
                 ("reserved0", i32), ("stage_all", vp), ("state", vp)]
 
 
+class GswFlatForcingArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("phase", i32), ("q0", vp), ("q1", vp), ("q2", vp), ("flags", vp),
+                ("nslots", i64), ("h_min", C.c_float), ("reserved0", i32), ("state", vp), ("n_cls", vp),
+                ("infil_tab", vp), ("sp_slots", vp), ("sp_keep", vp), ("sp_amb", vp), ("sp_n", i32),
+                ("ga_mode", i32), ("ga_cls", vp), ("Ks_t", vp), ("psi_t", vp), ("dth_t", vp), ("F", vp),
+                ("Fmax", vp), ("inv_tau", vp), ("cl_slots", vp), ("cl_hmax", vp), ("cl_n", i32), ("dr_n", i32),
+                ("dr_slots", vp), ("dr_htgt", vp)]
+
+
 class GswMember(C.Structure):
     _fields_ = [("dt", GswDtParams), ("inv_dx", C.c_float), ("g", C.c_float), ("h_min", C.c_float),
                 ("h_min_cfl", C.c_float), ("vcap", C.c_float), ("linf", i32), ("quadratic", i32),
@@ -138,6 +147,7 @@ _PROTOS = {
     "gsw_dt_finalize": [C.POINTER(GswDtParams), vp, vp],
     "gsw_loop_commit": [vp, vp],
     "gsw_flat_inflow_apply": [C.POINTER(GswFlatInflowArgs), vp],
+    "gsw_flat_forcings": [C.POINTER(GswFlatForcingArgs), vp],
     "gsw_flat_ring_stage": [C.POINTER(GswFlatRingArgs), vp],
     "gsw_adj_flat_step": [C.POINTER(GswFlatAdjArgs), vp],
     "gsw_adj_flat_inflow": [C.POINTER(GswFlatInflowArgs), vp, vp, vp, vp, vp],

@@ -337,6 +337,7 @@ class CompressedSolver:
         self._rain_ncol = 0
         self._inflows = []
         self._ring = None
+        self._forcing = {}
         self.warps, self.min_blocks = 0, 0
         from . import autotune
         best = autotune.load("flat", self.nslots)
@@ -468,6 +469,122 @@ class CompressedSolver:
                           stage=torch.from_numpy(np.ascontiguousarray(st)).to(dev))
         self._graph_cache.clear()
         return self
+
+    # ----------------------------------------------- per-step coastal forcings
+    def _slots_of_padded(self, rows, cols):
+        """Slots of padded (i, j) cells (-1 where the cell is not stored)."""
+        i = torch.as_tensor(np.asarray(rows, np.int64), device=self.device)
+        j = torch.as_tensor(np.asarray(cols, np.int64), device=self.device)
+        lut = torch.full((self.nxp * self.nyp,), -1, dtype=torch.int64, device=self.device)
+        lut[self._lin_of_slot.to(torch.int64)] = self._slot_cells.to(torch.int64)
+        return lut[i * self.nyp + j].contiguous()
+
+    def _pack_padded(self, field, dtype):
+        f = torch.as_tensor(np.ascontiguousarray(np.asarray(field)), device=self.device).reshape(-1)
+        out = torch.zeros(self.nslots, dtype=dtype, device=self.device)
+        out[self._slot_cells] = f[self._lin_of_slot].to(dtype)
+        return out
+
+    def set_sponge(self, sponge):
+        """Open-boundary sponge (compressed_solver.py:3148-3156): {"keep": k, "amb": a} on
+        the padded grid; each step h <- keep*h + amb, hu, hv <- keep*hu, keep*hv over the
+        band where keep != 1 or amb != 0."""
+        self._forcing.pop("sponge", None)
+        if sponge is not None:
+            keep = np.asarray(sponge["keep"], np.float32)
+            amb = np.asarray(sponge["amb"], np.float32)
+            if keep.shape != (self.nxp, self.nyp) or amb.shape != keep.shape:
+                raise ValueError(f"set_sponge: keep and amb must be padded ({self.nxp}, {self.nyp}) fields")
+            ii, jj = np.nonzero((keep != 1.0) | (amb != 0.0))
+            slots = self._slots_of_padded(ii, jj)
+            ok = (slots >= 0).cpu().numpy()
+            self._forcing["sponge"] = dict(slots=slots[torch.from_numpy(ok).to(self.device)].contiguous(),
+                                           keep=torch.from_numpy(keep[ii[ok], jj[ok]].copy()).to(self.device),
+                                           amb=torch.from_numpy(amb[ii[ok], jj[ok]].copy()).to(self.device))
+        self._graph_cache.clear()
+        return self
+
+    def set_infil(self, infil):
+        """Landcover infiltration (compressed_solver.py:3212, infiltrate_flat): {"tab":
+        rate (m/s) per Manning class}; each step h <- max(h - tab[class] dt, 0) with the
+        velocity kept."""
+        self._forcing.pop("infil", None)
+        if infil is not None:
+            self._forcing["infil"] = torch.from_numpy(np.asarray(infil["tab"], np.float32).reshape(-1).copy()
+                                                      ).to(self.device)
+        self._graph_cache.clear()
+        return self
+
+    def set_ga_drain(self, b):
+        """Green-Ampt infiltration and linear-reservoir drain (compressed_solver.py:3214,
+        3284-3292): {cls_pad, Ks_t, psi_t, dth_t, F_pad, Fmax_pad?, inv_tau_pad?, mode}
+        with padded per-cell fields and per-class tables; mode "fused", "ga" or "drain"."""
+        self._forcing.pop("ga", None)
+        if b is not None:
+            mode = {"fused": 1, "ga": 2, "drain": 3}[b.get("mode", "fused")]
+            t = lambda k: torch.from_numpy(np.asarray(b[k], np.float32).reshape(-1).copy()).to(self.device)
+            self._forcing["ga"] = dict(
+                mode=mode, cls=self._pack_padded(b["cls_pad"], torch.uint8),
+                Ks=t("Ks_t"), psi=t("psi_t"), dth=t("dth_t"), F=self._pack_padded(b["F_pad"], torch.float32),
+                Fmax=(self._pack_padded(b["Fmax_pad"], torch.float32) if b.get("Fmax_pad") is not None else None),
+                inv_tau=(self._pack_padded(b["inv_tau_pad"], torch.float32)
+                         if b.get("inv_tau_pad") is not None else None))
+            if mode != 2 and self._forcing["ga"]["inv_tau"] is None:
+                raise ValueError("set_ga_drain: the drain needs inv_tau_pad")
+        self._graph_cache.clear()
+        return self
+
+    def set_clamp(self, b):
+        """Stage clamp (compressed_solver.py:3216, 3294-3299): {rows, cols, hmax} padded
+        cells where h is capped at hmax with the velocity kept."""
+        self._forcing.pop("clamp", None)
+        if b is not None and len(b["rows"]) > 0:
+            self._forcing["clamp"] = dict(slots=self._slots_of_padded(b["rows"], b["cols"]),
+                                          hmax=torch.from_numpy(np.asarray(b["hmax"], np.float32).copy()
+                                                                ).to(self.device))
+        self._graph_cache.clear()
+        return self
+
+    def set_drain(self, drain):
+        """Karst drain cap (compressed_solver.py:3211, drain_cap): {idx (canonical flat
+        ids), h_tgt or h_tgt_arr}; h is capped at the target with the velocity kept."""
+        self._forcing.pop("drain", None)
+        if drain is not None:
+            idx = torch.from_numpy(np.asarray(drain["idx"], np.int64).reshape(-1)).to(self.device)
+            ht = (np.asarray(drain["h_tgt_arr"], np.float32) if "h_tgt_arr" in drain
+                  else np.full(idx.numel(), np.float32(drain.get("h_tgt", 0.5)), np.float32))
+            self._forcing["drain"] = dict(slots=self._slot[idx].contiguous(),
+                                          htgt=torch.from_numpy(ht.reshape(-1).copy()).to(self.device))
+        self._graph_cache.clear()
+        return self
+
+    def _forcing_args(self, q, phase):
+        f = self._forcing
+        a = L.GswFlatForcingArgs()
+        a.abi_version = L.ABI_VERSION
+        a.phase = phase
+        a.q0, a.q1, a.q2, a.flags = _ptr(q[0]), _ptr(q[1]), _ptr(q[2]), _ptr(self._flags)
+        a.nslots, a.h_min, a.state = self.nslots, self.h_min, _ptr(self._state)
+        if phase == 0:
+            if "infil" in f:
+                a.n_cls, a.infil_tab = _ptr(self._ncls), _ptr(f["infil"])
+            if "sponge" in f:
+                sp = f["sponge"]
+                a.sp_slots, a.sp_keep, a.sp_amb, a.sp_n = (_ptr(sp["slots"]), _ptr(sp["keep"]), _ptr(sp["amb"]),
+                                                           int(sp["slots"].numel()))
+        else:
+            if "ga" in f:
+                g = f["ga"]
+                a.ga_mode, a.ga_cls, a.Ks_t, a.psi_t, a.dth_t = (g["mode"], _ptr(g["cls"]), _ptr(g["Ks"]),
+                                                                 _ptr(g["psi"]), _ptr(g["dth"]))
+                a.F, a.Fmax, a.inv_tau = _ptr(g["F"]), _ptr(g["Fmax"]), _ptr(g["inv_tau"])
+            if "clamp" in f:
+                a.cl_slots, a.cl_hmax, a.cl_n = (_ptr(f["clamp"]["slots"]), _ptr(f["clamp"]["hmax"]),
+                                                 int(f["clamp"]["slots"].numel()))
+            if "drain" in f:
+                a.dr_slots, a.dr_htgt, a.dr_n = (_ptr(f["drain"]["slots"]), _ptr(f["drain"]["htgt"]),
+                                                 int(f["drain"]["slots"].numel()))
+        return a
 
     def _ring_args(self, q):
         r = self._ring
@@ -655,6 +772,8 @@ class CompressedSolver:
         start = self._cur
         _host_lib()
 
+        forced = bool(self._forcing)
+
         def one_window():
             s = _stream()
             for k in range(K):
@@ -662,13 +781,22 @@ class CompressedSolver:
                 src, dst = self._q[(start + k) % 2], self._q[(start + k + 1) % 2]
                 for f in self._inflows:             # inlet ghosts at t_n, before the step
                     L.call("gsw_flat_inflow_apply", C.byref(self._inflow_args(f, src)), s)
-                L.call("gsw_flat_step", C.byref(self._args(src, dst)), s)
+                a = self._args(src, dst)
+                if forced:                          # the wave speed is taken after the forcings
+                    a.lam_target = None
+                L.call("gsw_flat_step", C.byref(a), s)
+                if forced:
+                    L.call("gsw_flat_forcings", C.byref(self._forcing_args(dst, 0)), s)
                 if self._ring is not None:          # ring stage at t_n, after the step
                     L.call("gsw_flat_ring_stage", C.byref(self._ring_args(dst)), s)
-            return (2 + len(self._inflows) + (self._ring is not None)) * K
+                if forced:
+                    L.call("gsw_flat_forcings", C.byref(self._forcing_args(dst, 1)), s)
+                    L.call("gsw_flat_lammax", C.byref(self._args(dst, dst, step=False)),
+                           C.c_void_p(self._state.data_ptr() + L.GswLoopState.lam_bits.offset), s)
+            return (2 + len(self._inflows) + (self._ring is not None) + 3 * forced) * K
 
         key = (K, start, float(t_end), p.dt_max, int(max_steps), self._rain_kind, len(self._inflows),
-               self._ring is not None, self.warps, self.min_blocks)
+               self._ring is not None, self.warps, self.min_blocks, tuple(sorted(self._forcing)))
         if key not in self._graph_cache:
             self._graph_cache.clear()
             side = torch.cuda.Stream(device=self.device)
@@ -722,6 +850,8 @@ class CompressedSolver:
         arrays = {f"q{c}": q[c][self._slot].cpu().numpy() for c in range(3)}
         if self._max_h is not None:
             arrays["max_h"] = self._max_h[self._slot].cpu().numpy()
+        if "ga" in self._forcing:                  # Green-Ampt's cumulative infiltration is state
+            arrays["F"] = self._forcing["ga"]["F"][self._slot].cpu().numpy()
         tmp = os.path.join(ckpt_dir, "ckpt_r00_tmp")
         np.savez(tmp, t=np.float64(t), steps=np.int64(steps), **arrays)
         os.replace(tmp + ".npz", os.path.join(ckpt_dir, "ckpt_r00.npz"))
@@ -759,6 +889,11 @@ class CompressedSolver:
             else:
                 warnings.warn("load_checkpoint: no max_h in the checkpoint; the max-depth envelope only "
                               "covers the resumed window", RuntimeWarning, stacklevel=2)
+        if "ga" in self._forcing:
+            if "F" not in z.files:
+                raise RuntimeError("resume: Green-Ampt is active but the checkpoint has no F array; resuming "
+                                   "would reset cumulative infiltration to zero")
+            self._forcing["ga"]["F"][self._slot] = torch.from_numpy(np.asarray(z["F"], np.float32)).to(self.device)
         self.t = float(meta["t"])
         self.nsteps = int(meta["steps"])
         return True

@@ -183,6 +183,110 @@ __global__ void flat_ring_kernel(GswFlatRingArgs a) {
     ((T*)a.q2)[idx] = (T)0;
 }
 
+// ---- per-step forcings of the flat loop (compressed_solver.py:2330-2366) ----
+// Landcover infiltration, infiltrate_flat (:143-158).
+__global__ void flat_infiltrate_kernel(GswFlatForcingArgs a) {
+    if (a.state->done) return;
+    const float dt = a.state->dt_f32;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < a.nslots;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        if (!(a.flags[k] & GSW_SLOT_ACTIVE)) continue;
+        const float h = a.q0[k];
+        if (h < a.h_min) continue;
+        const float dh = a.infil_tab[a.n_cls ? a.n_cls[k] : 0] * dt;
+        float hn = h - dh;
+        if (hn < 0.0f) hn = 0.0f;
+        const float r = hn / h;
+        a.q0[k] = hn; a.q1[k] = a.q1[k] * r; a.q2[k] = a.q2[k] * r;
+    }
+}
+
+// Open-boundary sponge over its band, sponge_band (:1320-1328).
+__global__ void flat_sponge_kernel(GswFlatForcingArgs a) {
+    if (a.state->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.sp_n) return;
+    const int64_t k = a.sp_slots[i];
+    const float kp = a.sp_keep[i];
+    a.q0[k] = __fadd_rn(__fmul_rn(a.q0[k], kp), a.sp_amb[i]);
+    a.q1[k] = a.q1[k] * kp;
+    a.q2[k] = a.q2[k] * kp;
+}
+
+// Green-Ampt infiltration and the linear-reservoir drain, ga_drain_flat / ga_flat /
+// drain_tau_flat (:313-420): one momentum scale accumulated over both, as the reference.
+__global__ void flat_ga_drain_kernel(GswFlatForcingArgs a) {
+    if (a.state->done) return;
+    const float dt = a.state->dt_f32;
+    const bool ga = a.ga_mode == 1 || a.ga_mode == 2;
+    const bool drain = a.ga_mode == 1 || a.ga_mode == 3;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < a.nslots;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        if (!(a.flags[k] & GSW_SLOT_ACTIVE)) continue;
+        float h = a.q0[k];
+        if (h <= 0.0f) continue;
+        float scale = 1.0f;
+        if (ga) {
+            const int c = a.ga_cls[k];
+            const float K = a.Ks_t[c];
+            if (K > 0.0f) {
+                const float KsDt = K * dt;
+                const float head = a.psi_t[c] + h;
+                const float F0 = a.F[k];
+                const float A = F0 + KsDt;
+                const float disc = A * A + 4.0f * KsDt * head * a.dth_t[c];
+                const float F1 = 0.5f * (A + sqrtf(fmaxf(disc, 0.0f)));
+                const float dF_raw = F1 - F0;
+                float dF = (dF_raw > 0.0f) ? dF_raw : 0.0f;
+                if (dF > h) dF = h;
+                const float room = (a.Fmax ? a.Fmax[k] : 3.0e38f) - F0;
+                if (dF > room) dF = (room > 0.0f) ? room : 0.0f;
+                const float hn = h - dF;
+                if (drain) {
+                    scale = scale * (hn / h);
+                } else {
+                    scale = hn / h;
+                }
+                h = hn;
+                a.F[k] = F0 + dF;
+            } else if (!drain) {
+                continue;
+            }
+        }
+        if (drain) {
+            const float it = a.inv_tau[k];
+            if (it > 0.0f && h > 0.0f) {
+                const float decay = __expf(-dt * it);
+                scale = scale * decay;
+                h = h * decay;
+            } else if (!ga) {
+                continue;
+            }
+        }
+        a.q0[k] = h;
+        a.q1[k] = a.q1[k] * scale;
+        a.q2[k] = a.q2[k] * scale;
+    }
+}
+
+// Stage clamp, stage_clamp_flat (:422-437), then the karst drain cap, drain_cap (:268-283).
+__global__ void flat_clamp_kernel(GswFlatForcingArgs a, bool cap) {
+    if (a.state->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = cap ? a.dr_n : a.cl_n;
+    if (i >= n) return;
+    const int64_t k = cap ? a.dr_slots[i] : a.cl_slots[i];
+    if (k < 0) return;
+    const float h = a.q0[k];
+    const float ht = cap ? a.dr_htgt[i] : a.cl_hmax[i];
+    if (h > ht) {
+        const float r = cap ? ((h > 1e-12f) ? ht / h : 0.0f) : ht / h;
+        a.q0[k] = ht;
+        a.q1[k] = a.q1[k] * r;
+        a.q2[k] = a.q2[k] * r;
+    }
+}
+
 }  // namespace gsw
 
 using namespace gsw;
@@ -225,4 +329,44 @@ extern "C" int gsw_flat_ring_stage(const GswFlatRingArgs* a, void* stream) {
     else if (a->dtype == GSW_F64) flat_ring_kernel<double><<<grid, 256, 0, s>>>(*a);
     else return set_error(GSW_ERR_INVALID, "ring stage: bad dtype");
     return check_launch("flat_ring");
+}
+
+extern "C" int gsw_flat_forcings(const GswFlatForcingArgs* a, void* stream) {
+    GSW_CHECK_ABI(a);
+    if (!a->q0 || !a->q1 || !a->q2 || !a->flags || !a->state || a->nslots < 0)
+        return set_error(GSW_ERR_INVALID, "flat forcings: null state or flags");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int grid_all = (int)std::max<int64_t>(1, std::min<int64_t>(sm_count() * 8, (a->nslots + 255) / 256));
+    if (a->phase == 0) {
+        if (a->infil_tab) {
+            flat_infiltrate_kernel<<<grid_all, 256, 0, s>>>(*a);
+            if (int rc = check_launch("flat_infiltrate")) return rc;
+        }
+        if (a->sp_n > 0) {
+            if (!a->sp_slots || !a->sp_keep || !a->sp_amb) return set_error(GSW_ERR_INVALID, "sponge: null arrays");
+            flat_sponge_kernel<<<(a->sp_n + 255) / 256, 256, 0, s>>>(*a);
+            if (int rc = check_launch("flat_sponge")) return rc;
+        }
+        return GSW_OK;
+    }
+    if (a->phase != 1) return set_error(GSW_ERR_INVALID, "flat forcings: phase must be 0 or 1");
+    if (a->ga_mode != 0) {
+        if (a->ga_mode < 0 || a->ga_mode > 3) return set_error(GSW_ERR_INVALID, "Green-Ampt: bad mode");
+        if ((a->ga_mode != 3 && (!a->ga_cls || !a->Ks_t || !a->psi_t || !a->dth_t || !a->F)) ||
+            (a->ga_mode != 2 && !a->inv_tau))
+            return set_error(GSW_ERR_INVALID, "Green-Ampt / drain: null arrays");
+        flat_ga_drain_kernel<<<grid_all, 256, 0, s>>>(*a);
+        if (int rc = check_launch("flat_ga_drain")) return rc;
+    }
+    if (a->cl_n > 0) {
+        if (!a->cl_slots || !a->cl_hmax) return set_error(GSW_ERR_INVALID, "stage clamp: null arrays");
+        flat_clamp_kernel<<<(a->cl_n + 63) / 64, 64, 0, s>>>(*a, false);
+        if (int rc = check_launch("flat_clamp")) return rc;
+    }
+    if (a->dr_n > 0) {
+        if (!a->dr_slots || !a->dr_htgt) return set_error(GSW_ERR_INVALID, "drain cap: null arrays");
+        flat_clamp_kernel<<<(a->dr_n + 255) / 256, 256, 0, s>>>(*a, true);
+        if (int rc = check_launch("flat_drain_cap")) return rc;
+    }
+    return GSW_OK;
 }

@@ -328,6 +328,40 @@ typedef struct GswFlatRingArgs {
 } GswFlatRingArgs;
 GSW_API int gsw_flat_ring_stage(const GswFlatRingArgs* a, void* stream);
 
+/* Per-step forcings of the flat loop, applied after the step in the reference's order
+ * (geoswe/compressed_solver.py:2330-2366): phase 0 = landcover infiltration
+ * (infiltrate_flat, :143-158), then the open-boundary sponge band (sponge_band,
+ * :1320-1328); the ring stage (gsw_flat_ring_stage) comes between; phase 1 = Green-Ampt
+ * infiltration with the linear-reservoir drain (ga_drain_flat / ga_flat / drain_tau_flat,
+ * :313-420), the stage clamp (stage_clamp_flat, :422-437), then the karst drain cap
+ * (drain_cap, :268-283). Each part is skipped when its pointers are NULL. dt is the
+ * step's state->dt_f32; nothing runs when state->done. fp32 only, as the reference. */
+typedef struct GswFlatForcingArgs {
+    uint32_t abi_version;
+    int32_t  phase;                 /* 0 or 1 (above) */
+    float* q0; float* q1; float* q2;/* brick storage */
+    const uint8_t* flags;           /* slot flags; forcings over all slots touch active slots only */
+    int64_t  nslots;
+    float    h_min;
+    int32_t  reserved0;
+    const GswLoopState* state;
+    /* landcover infiltration: rate infil_tab[n_cls[slot]] (m/s) */
+    const uint8_t* n_cls; const float* infil_tab;
+    /* sponge band: q0 = q0*keep + amb, q1, q2 *= keep on the listed slots */
+    const int64_t* sp_slots; const float* sp_keep; const float* sp_amb; int32_t sp_n;
+    /* Green-Ampt / drain: 1 fused, 2 Green-Ampt only, 3 drain only (0 off); per-slot
+       class, cumulative infiltration F (state, updated), cap Fmax, drain rate inv_tau */
+    int32_t  ga_mode;
+    const uint8_t* ga_cls; const float* Ks_t; const float* psi_t; const float* dth_t;
+    float* F; const float* Fmax; const float* inv_tau;
+    /* stage clamp: h <= h_max on the listed slots, momentum scaled */
+    const int64_t* cl_slots; const float* cl_hmax; int32_t cl_n;
+    /* karst drain cap: h <= h_tgt on the listed slots, momentum scaled */
+    int32_t  dr_n;
+    const int64_t* dr_slots; const float* dr_htgt;
+} GswFlatForcingArgs;
+GSW_API int gsw_flat_forcings(const GswFlatForcingArgs* a, void* stream);
+
 /* Fused step on the compressed mesh: active cells get the SRM-HLLC residual, rain,
  * Euler, wet/dry and Manning (table); stored ring cells are carried unchanged.
  * Replaces the flat fused step + CFL launch (geoswe/compressed_rhs.py:673-865, 990-1118;

@@ -388,6 +388,81 @@ class OracleFlat:
                          t=np.asarray(t_common, np.float64), st=np.asarray(stage_all, np.float32))
         return self
 
+    def set_forcings(self, *, infil_tab=None, sponge=None, ga=None, clamp=None, drain=None):
+        """Per-step forcings on canonical ids, restated from the flat loop's kernels
+        (compressed_solver.py:143-158, 268-283, 313-437, 1320-1328), applied in its order
+        (:2330-2366): infiltration, sponge, ring, Green-Ampt / drain, clamp, drain cap.
+        sponge = (ids, keep, amb); ga = dict(mode, cls, Ks, psi, dth, F, Fmax, inv_tau)
+        (mode "ga" only: the drain's __expf has no exact CPU restatement); clamp = (ids,
+        hmax); drain = (ids, h_tgt)."""
+        self.forcings = dict(infil=infil_tab, sponge=sponge, ga=ga, clamp=clamp, drain=drain)
+        return self
+
+    def _apply_forcings(self, phase):
+        f = getattr(self, "forcings", None)
+        if not f:
+            return
+        q0, q1, q2 = self.q
+        act = self.act != 0
+        f32 = np.float32
+        dt = f32(self._dt32)
+        if phase == 0:
+            if f["infil"] is not None:
+                tab = np.asarray(f["infil"], np.float32)
+                ncls = self.ncls if self.ncls is not None else np.zeros(len(self.act), np.uint8)
+                m = act & (q0 >= f32(self.h_min))
+                h = q0[m]
+                hn = (h - (tab[ncls[m]] * dt).astype(np.float32)).astype(np.float32)
+                hn = np.where(hn < 0, f32(0), hn).astype(np.float32)
+                r = (hn / h).astype(np.float32)
+                q0[m] = hn
+                q1[m] = (q1[m] * r).astype(np.float32)
+                q2[m] = (q2[m] * r).astype(np.float32)
+            if f["sponge"] is not None:
+                ids, keep, amb = f["sponge"]
+                q0[ids] = ((q0[ids] * keep).astype(np.float32) + amb).astype(np.float32)
+                q1[ids] = (q1[ids] * keep).astype(np.float32)
+                q2[ids] = (q2[ids] * keep).astype(np.float32)
+            return
+        g = f["ga"]
+        if g is not None:
+            if g["mode"] != "ga":
+                raise NotImplementedError("the oracle restates the Green-Ampt-only mode")
+            K = np.asarray(g["Ks"], np.float32)[g["cls"]]
+            m = act & (K > 0) & (q0 > 0)
+            h = q0[m]
+            KsDt = (K[m] * dt).astype(np.float32)
+            head = (np.asarray(g["psi"], np.float32)[g["cls"][m]] + h).astype(np.float32)
+            F0 = g["F"][m]
+            A = (F0 + KsDt).astype(np.float32)
+            disc = ((A * A).astype(np.float32)
+                    + ((f32(4.0) * KsDt).astype(np.float32) * head).astype(np.float32)
+                    * np.asarray(g["dth"], np.float32)[g["cls"][m]]).astype(np.float32)
+            F1 = (f32(0.5) * (A + np.sqrt(np.maximum(disc, f32(0))).astype(np.float32)).astype(np.float32)
+                  ).astype(np.float32)
+            dF = np.maximum((F1 - F0).astype(np.float32), f32(0)).astype(np.float32)
+            dF = np.where(dF > h, h, dF)
+            Fmax = g["Fmax"][m] if g["Fmax"] is not None else np.full(h.size, f32(3.0e38), np.float32)
+            room = (Fmax - F0).astype(np.float32)
+            dF = np.where(dF > room, np.where(room > 0, room, f32(0)), dF).astype(np.float32)
+            hn = (h - dF).astype(np.float32)
+            al = (hn / h).astype(np.float32)
+            q0[m] = hn
+            q1[m] = (q1[m] * al).astype(np.float32)
+            q2[m] = (q2[m] * al).astype(np.float32)
+            g["F"][m] = (F0 + dF).astype(np.float32)
+        for key, guard in (("clamp", False), ("drain", True)):
+            if f[key] is None:
+                continue
+            ids, ht = f[key]
+            for i, k in enumerate(ids):
+                h = q0[k]
+                if h > ht[i]:
+                    r = (np.float32(ht[i] / h) if (not guard or h > np.float32(1e-12)) else np.float32(0.0))
+                    q0[k] = ht[i]
+                    q1[k] = np.float32(q1[k] * r)
+                    q2[k] = np.float32(q2[k] * r)
+
     def _apply_ring(self):
         r = getattr(self, "ring", None)
         if r is None:
@@ -457,7 +532,12 @@ class OracleFlat:
             C.c_int(int(self.quad)), C.c_int(int(self.keep_h)), _p(qn[0]), _p(qn[1]), _p(qn[2]), _p(self.max_h))
         self.q = qn
         self._lam = float(lam)
+        self._dt32 = np.float32(dt)
+        self._apply_forcings(0)
         self._apply_ring()                      # at the step's start time, after the step
+        self._apply_forcings(1)
+        if getattr(self, "forcings", None):
+            self._lam = None                    # the wave speed of the forced state
         self.t += dt
         self.nsteps += 1
 

@@ -8,6 +8,8 @@ This recipe imports the reference package with a recording stand-in for CuPy, so
 exact text the reference would hand to NVRTC is captured, and compiles it with nvcc:
 
   oracle/_ref/ref_kernels.cu          the captured reference text + C launch wrappers
+                                      (the dense fused step, the residual, lammax, and
+                                      the flat loop's per-step forcing kernels)
   oracle/_ref/libref_fma.so           nvcc defaults (FMA contraction on, as NVRTC)
   oracle/_ref/libref_strict.so        --fmad=false (every operation rounded separately)
 
@@ -76,8 +78,14 @@ def capture(ref_src):
     k2d = R.build_dense_fstep2d_kernel(True, 1)                         # no sigma, keep-h
     kres = R._build_srm_hllc_ns("float", "fused_rhs_wb_srm_hllc_2d_ns_fp32")
     kres64 = R._build_srm_hllc_ns("double", "fused_rhs_wb_srm_hllc_2d_ns_fp64")
+    from geoswe import compressed_solver as CS
     return {k2d.name: k2d.code, kres.name: kres.code, kres64.name: kres64.code,
-            "lammax_fp32_lean": S._CFL_LAMMAX_SRC_LEAN}
+            "lammax_fp32_lean": S._CFL_LAMMAX_SRC_LEAN,
+            # the flat loop's per-step forcings (compressed_solver.py:143-158, 268-283, 313-437, 1320-1328)
+            "infiltrate_flat": CS._INFILTRATE_SRC, "drain_cap": CS._DRAIN_CAP_SRC,
+            "ga_drain_flat": CS._GA_DRAIN_FLAT_SRC, "ga_flat": CS._GA_FLAT_SRC,
+            "drain_tau_flat": CS._DRAIN_TAU_FLAT_SRC, "stage_clamp_flat": CS._STAGE_CLAMP_FLAT_SRC,
+            "sponge_band": CS._SPONGE_BAND_SRC}
 
 
 # C launch wrappers around the captured kernels (signatures of the reference text:
@@ -110,6 +118,24 @@ extern "C" int ref_rhs_f64(const double* q0, const double* q1, const double* q2,
     dim3 block(16, 16), grid((nxp + 15) / 16, (nyp + 15) / 16);
     fused_rhs_wb_srm_hllc_2d_ns_fp64<<<grid, block, 0, (cudaStream_t)stream>>>(
         q0, q1, q2, dummy_sigma, b, r0, r1, r2, nxp, nyp, inv_dx, inv_dy, g, h_min, mask);
+    return (int)cudaGetLastError();
+}
+extern "C" int ref_forcing(int which, float* q0, float* q1, float* q2, const unsigned char* cls,
+    const float* t0, const float* t1, const float* t2, float* F, const float* Fmax, const float* inv_tau,
+    const unsigned char* act, const int* idx, const float* a0, const float* a1, int n, float dt, float h_min,
+    void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int grid = (n + 255) / 256;
+    switch (which) {
+    case 0: infiltrate_flat<<<grid, 256, 0, s>>>(q0, q1, q2, cls, t0, act, n, dt, h_min); break;
+    case 1: sponge_band<<<grid, 256, 0, s>>>(idx, a0, a1, q0, q1, q2, n); break;
+    case 2: ga_drain_flat<<<grid, 256, 0, s>>>(q0, q1, q2, cls, t0, t1, t2, F, Fmax, inv_tau, act, dt, n); break;
+    case 3: ga_flat<<<grid, 256, 0, s>>>(q0, q1, q2, cls, t0, t1, t2, F, Fmax, act, dt, n); break;
+    case 4: drain_tau_flat<<<grid, 256, 0, s>>>(q0, q1, q2, inv_tau, act, dt, n); break;
+    case 5: stage_clamp_flat<<<grid, 256, 0, s>>>(idx, q0, q1, q2, a0, n); break;
+    case 6: drain_cap<<<grid, 256, 0, s>>>(idx, q0, q1, q2, a0, n); break;
+    default: return -1;
+    }
     return (int)cudaGetLastError();
 }
 extern "C" int ref_lammax(const float* q0, const float* q1, const float* q2, int nx, int ny,

@@ -175,3 +175,22 @@ class RefDenseGPU:
             self.step(dt)
             steps += 1
         return steps
+
+
+_FORCING = {"infiltrate": 0, "sponge": 1, "ga_drain": 2, "ga": 3, "drain_tau": 4, "clamp": 5, "drain_cap": 6}
+
+
+def ref_forcing(which, q, *, cls=None, t0=None, t1=None, t2=None, F=None, Fmax=None, inv_tau=None, act=None,
+                idx=None, a0=None, a1=None, n=None, dt=0.0, h_min=1e-6, variant="fma"):
+    """Apply one of the reference's flat-loop forcing kernels (captured text, compiled by
+    oracle/ref_build.py) in place on CUDA tensors in canonical flat order: q is a list
+    of three float32 tensors; the other arrays as the kernel takes them."""
+    L = _lib(variant)
+    L.ref_forcing.restype = C.c_int
+    if n is None:
+        n = int(q[0].numel()) if idx is None else int(idx.numel())
+    rc = L.ref_forcing(_FORCING[which], _p(q[0]), _p(q[1]), _p(q[2]), _p(cls), _p(t0), _p(t1), _p(t2), _p(F),
+                       _p(Fmax), _p(inv_tau), _p(act), _p(idx), _p(a0), _p(a1), C.c_int(n),
+                       C.c_float(dt), C.c_float(h_min), _stream())
+    if rc != 0:
+        raise RuntimeError(f"ref_forcing({which}): CUDA error {rc}")
