@@ -145,6 +145,8 @@ _PROTOS = {
     "gsw_lam_cells": [C.POINTER(GswStageArgs), vp],
     "gsw_inflow_apply": [C.POINTER(GswInflowArgs), vp],
     "gsw_dt_finalize": [C.POINTER(GswDtParams), vp, vp],
+    "gsw_dt_params_upload": [C.POINTER(GswDtParams), vp, vp],
+    "gsw_dt_finalize_dev": [vp, vp, vp],
     "gsw_loop_commit": [vp, vp],
     "gsw_flat_inflow_apply": [C.POINTER(GswFlatInflowArgs), vp],
     "gsw_flat_forcings": [C.POINTER(GswFlatForcingArgs), vp],

@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from . import _lib as L
-from .solver import Solver2D, _ptr, _stream
+from .solver import Solver2D, _cached_graph, _ptr, _stream
 
 BRICK_W, BRICK_PITCH = L.BRICK_W, L.BRICK_PITCH
 SLOT_STORED, SLOT_ACTIVE = 1, 2
@@ -344,6 +344,7 @@ class CompressedSolver:
         if best:
             self.warps, self.min_blocks = int(best["warps"]), int(best["min_blocks"])
         self._graph_cache = {}
+        self._dtp_dev = None
         self.t = 0.0
         self.nsteps = 0
         self.kernel_launches = 0
@@ -763,50 +764,54 @@ class CompressedSolver:
                           "to set_rain().", stacklevel=2)
         dm = dt_max if dt_max is not None else self.dt_max_user
         K = int(window) if window else self._window_size()
-        if max_steps and max_steps < K:
+        if max_steps and max_steps < K and not window:
             K = int(max_steps)
         K += K % 2
         self._write_state()
         self._lammax_into_state()
         p = self._dt_params(t_end, dm, max_steps)
+        # the dt rule is read from device memory, so one captured window serves every
+        # t_end / dt_max / max_steps
+        if self._dtp_dev is None:
+            self._dtp_dev = torch.zeros(C.sizeof(L.GswDtParams), dtype=torch.uint8, device=self.device)
+        L.call("gsw_dt_params_upload", C.byref(p), _ptr(self._dtp_dev), _stream())
         start = self._cur
         _host_lib()
 
         forced = bool(self._forcing)
+        per_step = 2 + len(self._inflows) + (self._ring is not None) + 3 * forced
+
+        def one_step(k_parity):
+            s = _stream()
+            L.call("gsw_dt_finalize_dev", _ptr(self._dtp_dev), _ptr(self._state), s)
+            src, dst = self._q[k_parity], self._q[1 - k_parity]
+            for f in self._inflows:             # inlet ghosts at t_n, before the step
+                L.call("gsw_flat_inflow_apply", C.byref(self._inflow_args(f, src)), s)
+            a = self._args(src, dst)
+            if forced:                          # the wave speed is taken after the forcings
+                a.lam_target = None
+            L.call("gsw_flat_step", C.byref(a), s)
+            if forced:
+                L.call("gsw_flat_forcings", C.byref(self._forcing_args(dst, 0)), s)
+            if self._ring is not None:          # ring stage at t_n, after the step
+                L.call("gsw_flat_ring_stage", C.byref(self._ring_args(dst)), s)
+            if forced:
+                L.call("gsw_flat_forcings", C.byref(self._forcing_args(dst, 1)), s)
+                L.call("gsw_flat_lammax", C.byref(self._args(dst, dst, step=False)),
+                       C.c_void_p(self._state.data_ptr() + L.GswLoopState.lam_bits.offset), s)
 
         def one_window():
-            s = _stream()
             for k in range(K):
-                L.call("gsw_dt_finalize", C.byref(p), _ptr(self._state), s)
-                src, dst = self._q[(start + k) % 2], self._q[(start + k + 1) % 2]
-                for f in self._inflows:             # inlet ghosts at t_n, before the step
-                    L.call("gsw_flat_inflow_apply", C.byref(self._inflow_args(f, src)), s)
-                a = self._args(src, dst)
-                if forced:                          # the wave speed is taken after the forcings
-                    a.lam_target = None
-                L.call("gsw_flat_step", C.byref(a), s)
-                if forced:
-                    L.call("gsw_flat_forcings", C.byref(self._forcing_args(dst, 0)), s)
-                if self._ring is not None:          # ring stage at t_n, after the step
-                    L.call("gsw_flat_ring_stage", C.byref(self._ring_args(dst)), s)
-                if forced:
-                    L.call("gsw_flat_forcings", C.byref(self._forcing_args(dst, 1)), s)
-                    L.call("gsw_flat_lammax", C.byref(self._args(dst, dst, step=False)),
-                           C.c_void_p(self._state.data_ptr() + L.GswLoopState.lam_bits.offset), s)
-            return (2 + len(self._inflows) + (self._ring is not None) + 3 * forced) * K
+                one_step(k % 2)
+            return per_step * K
 
-        key = (K, start, float(t_end), p.dt_max, int(max_steps), self._rain_kind, len(self._inflows),
-               self._ring is not None, self.warps, self.min_blocks, tuple(sorted(self._forcing)))
-        if key not in self._graph_cache:
-            self._graph_cache.clear()
-            side = torch.cuda.Stream(device=self.device)
-            side.wait_stream(torch.cuda.current_stream())
-            g = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g, stream=side):
-                per = one_window()
-            torch.cuda.current_stream().wait_stream(side)
-            self._graph_cache[key] = (g, per)
-        g, per = self._graph_cache[key]
+        if start == 1:
+            # one step outside the window, so every captured window starts on buffer 0
+            one_step(1)
+            self.kernel_launches += per_step
+        key = (K, self._rain_kind, len(self._inflows), self._ring is not None, self.warps, self.min_blocks,
+               tuple(sorted(self._forcing)))
+        g, per = _cached_graph(self._graph_cache, key, one_window, self.device)
         self.kernel_launches += 1
         while True:
             g.replay()

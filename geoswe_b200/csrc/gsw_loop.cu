@@ -45,6 +45,11 @@ int sm_count() {
 }
 
 __global__ void dt_finalize_kernel(GswDtParams p, GswLoopState* s) { dt_finalize_one(p, s, s->lam_bits); }
+// The same with the parameters read from device memory: a captured launch then follows
+// whatever t_end / dt_max / max_steps the last gsw_dt_params_upload wrote.
+__global__ void dt_finalize_dev_kernel(const GswDtParams* p, GswLoopState* s) {
+    dt_finalize_one(*p, s, s->lam_bits);
+}
 
 __global__ void loop_commit_kernel(GswLoopState* s) { loop_commit(s); }
 
@@ -52,14 +57,38 @@ __global__ void loop_commit_kernel(GswLoopState* s) { loop_commit(s); }
 
 using namespace gsw;
 
+static int check_dt_params(const GswDtParams* p) {
+    if (p->mode == 0 && !(p->cfl_dmin > 0.0)) return set_error(GSW_ERR_INVALID, "dt_finalize: cfl_dmin must be > 0");
+    if (p->mode == 1 && !(p->fixed_dt > 0.0)) return set_error(GSW_ERR_INVALID, "dt_finalize: fixed_dt must be > 0");
+    if (p->mode == 2 && !p->dt_table) return set_error(GSW_ERR_INVALID, "dt_finalize: dt_table is NULL");
+    if (p->mode < 0 || p->mode > 2) return set_error(GSW_ERR_INVALID, "dt_finalize: mode %d", p->mode);
+    if (p->n_rain > 0 && !p->rain_t) return set_error(GSW_ERR_INVALID, "dt_finalize: rain_t is NULL");
+    return GSW_OK;
+}
+
 extern "C" int gsw_dt_finalize(const GswDtParams* p, GswLoopState* state, void* stream) {
     GSW_CHECK_ABI(p);
     if (!state) return set_error(GSW_ERR_INVALID, "dt_finalize: null state");
-    if (p->mode == 0 && !(p->cfl_dmin > 0.0)) return set_error(GSW_ERR_INVALID, "dt_finalize: cfl_dmin must be > 0");
-    if (p->mode == 1 && !(p->fixed_dt > 0.0)) return set_error(GSW_ERR_INVALID, "dt_finalize: fixed_dt must be > 0");
-    if (p->n_rain > 0 && !p->rain_t) return set_error(GSW_ERR_INVALID, "dt_finalize: rain_t is NULL");
+    if (int rc = check_dt_params(p)) return rc;
     dt_finalize_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(*p, state);
     return check_launch("dt_finalize");
+}
+
+extern "C" int gsw_dt_params_upload(const GswDtParams* p, GswDtParams* dev, void* stream) {
+    GSW_CHECK_ABI(p);
+    if (!dev) return set_error(GSW_ERR_INVALID, "dt_params_upload: null destination");
+    if (int rc = check_dt_params(p)) return rc;
+    // pageable source: the copy is staged before the call returns, so *p may be reused
+    const cudaError_t e = cudaMemcpyAsync(dev, p, sizeof(GswDtParams), cudaMemcpyHostToDevice,
+                                          (cudaStream_t)stream);
+    if (e != cudaSuccess) return set_error(GSW_ERR_CUDA, "dt_params_upload: %s", cudaGetErrorString(e));
+    return GSW_OK;
+}
+
+extern "C" int gsw_dt_finalize_dev(const GswDtParams* dev, GswLoopState* state, void* stream) {
+    if (!dev || !state) return set_error(GSW_ERR_INVALID, "dt_finalize_dev: null pointer");
+    dt_finalize_dev_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(dev, state);
+    return check_launch("dt_finalize_dev");
 }
 
 extern "C" int gsw_loop_commit(GswLoopState* state, void* stream) {

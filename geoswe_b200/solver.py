@@ -49,6 +49,23 @@ class _Tables:
     """Device copies of the forcing tables, in the solver's dtype."""
 
 
+def _cached_graph(cache, key, capture, device, keep=4):
+    """The CUDA graph of `capture()` for `key`, captured on first use on a side stream
+    (the captured kernels read the loop's `done` flag first, so a replay after the loop
+    has finished is a no-op). At most `keep` graphs are kept."""
+    if key not in cache:
+        while len(cache) >= keep:
+            cache.pop(next(iter(cache)))
+        side = torch.cuda.Stream(device=device)
+        side.wait_stream(torch.cuda.current_stream())
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            per = capture()
+        torch.cuda.current_stream().wait_stream(side)
+        cache[key] = (g, per)
+    return cache[key]
+
+
 class Solver2D:
     """Two-dimensional shallow-water solver on the dense padded grid.
 
@@ -137,6 +154,7 @@ class Solver2D:
         self._state_host = torch.zeros(128, dtype=torch.uint8).pin_memory()
         self._lam_scratch = torch.zeros(1, dtype=torch.int64, device=dev)
         self._graph_cache = {}
+        self._dtp_dev = None
         self._dev_tables = None
         self._tables_key = None
         self.kernel_launches = 0        # libgsw kernels enqueued or replayed by this solver
@@ -665,43 +683,46 @@ class Solver2D:
     def _run_device(self, t_end, max_steps, dt_max, window=0):
         T = self._tables()
         K = int(window) if window else self._window_size()
-        if max_steps and max_steps < K:
+        if max_steps and max_steps < K and not window:
             K = int(max_steps)
         K += K % 2
         self._write_state()
         self._lammax_into_state(T.ghost_skip)
         p = self._dt_params(t_end=t_end, dt_max=dt_max, max_steps=max_steps)
+        # the dt rule is read from device memory, so one captured window serves every
+        # t_end / dt_max / max_steps
+        if self._dtp_dev is None:
+            self._dtp_dev = torch.zeros(C.sizeof(L.GswDtParams), dtype=torch.uint8, device=self.device)
+        L.call("gsw_dt_params_upload", C.byref(p), _ptr(self._dtp_dev), _stream())
         start_cur = self._cur
 
+        def one_step(k_parity):
+            L.call("gsw_dt_finalize_dev", _ptr(self._dtp_dev), _ptr(self._state), _stream())
+            self._counting += 1
+            self._launch_step(k_parity, T)
+
         def one_window():
-            s = _stream()
             self._counting = 0
             for k in range(K):
-                L.call("gsw_dt_finalize", C.byref(p), _ptr(self._state), s)
-                self._counting += 1
-                self._launch_step((start_cur + k) % 2, T)
+                one_step(k % 2)
             return self._counting
 
+        lead = 0
+        if start_cur == 1:
+            # one step outside the window, so every captured window starts on buffer 0
+            self._counting = 0
+            one_step(1)
+            lead = self._counting
         if self._use_graphs:
-            key = (K, start_cur, float(t_end), None if dt_max is None else float(dt_max), int(max_steps))
-            if key not in self._graph_cache:
-                self._graph_cache.clear()
-                side = torch.cuda.Stream(device=self.device)
-                side.wait_stream(torch.cuda.current_stream())
-                g = torch.cuda.CUDAGraph()
-                # capture on a side stream; the captured kernels read `done` first, so a
-                # replay after the loop has finished is a no-op
-                with torch.cuda.graph(g, stream=side):
-                    per = one_window()
-                torch.cuda.current_stream().wait_stream(side)
-                self._graph_cache[key] = (g, per)
-            g, per = self._graph_cache[key]
+            g, per = _cached_graph(self._graph_cache, (K, self._tile_rows, self._warps, self._min_blocks),
+                                   one_window, self.device)
 
             def run_window():
                 g.replay()
                 return per
         else:
             run_window = one_window
+        self.kernel_launches += lead
         self.kernel_launches += 1            # the initial wave-speed pass
         while True:
             self.kernel_launches += run_window()

@@ -500,6 +500,13 @@ GSW_API int gsw_ensemble_step_static(const GswEnsembleArgs* a, void* stream);
 /* Commit the pending t/steps, test the loop condition, and compute this step's dt
  * and rain frame from state->lam_bits (then zeroed for the step's reduction). */
 GSW_API int gsw_dt_finalize(const GswDtParams* p, GswLoopState* state, void* stream);
+/* Device-resident parameters, for loops captured once in a CUDA graph and replayed
+ * for any t_end / dt_max / max_steps: gsw_dt_params_upload validates *p on the host
+ * and copies it to `dev` (device memory, sizeof(GswDtParams) bytes) on `stream`;
+ * gsw_dt_finalize_dev is gsw_dt_finalize reading the parameters from `dev` when it
+ * runs. Replaces the same host-side dt computation as gsw_dt_finalize. */
+GSW_API int gsw_dt_params_upload(const GswDtParams* p, GswDtParams* dev, void* stream);
+GSW_API int gsw_dt_finalize_dev(const GswDtParams* dev, GswLoopState* state, void* stream);
 /* Commit a pending t_new/steps (call once after the last step). */
 GSW_API int gsw_loop_commit(GswLoopState* state, void* stream);
 

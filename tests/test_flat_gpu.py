@@ -76,9 +76,17 @@ def test_flat_run_bitwise_oracle(linf):
     o = oracle.OracleFlat(cs.nbr, cs.is_active, q, b, dx, ncls=ncls, ntab=MANNING_CLASSES, linf=linf,
                           rain_times=rf.time_s, rain_table=(np.asarray(rf.rate_mm_h) / 3.6e6).astype(np.float32)[:, None],
                           rain_lookup=np.zeros(cs.n_stored, np.int64))
-    n_g = cs.run(t_end=1500.0)
-    n_o = o.run(t_end=1500.0)
-    assert n_g == n_o and n_g > 10
+    if linf:
+        n_g = cs.run(t_end=1500.0)
+        n_o = o.run(t_end=1500.0)
+        assert n_g == n_o and n_g > 10
+    else:
+        # interval by interval: a new t_end per call, calls starting on either buffer,
+        # one captured window replayed throughout
+        n_g = [cs.run(t_end=t) for t in (250.0, 700.0, 1100.0, 1500.0)]
+        n_o = [o.run(t_end=t) for t in (250.0, 700.0, 1100.0, 1500.0)]
+        assert n_g == n_o and sum(n_g) > 10 and any(k % 2 for k in n_g)
+        assert len(cs._graph_cache) == 1
     assert cs.t == o.t
     for c in range(3):
         assert same(cs.flat(c).cpu().numpy(), o.q[c]), c
