@@ -108,12 +108,12 @@ def build_case(n, dtype="float32", seed=0):
     return z, cls
 
 
-def make_solver(z, cls, n, dtype="float32"):
+def make_solver(z, cls, n, dtype="float32", arith="exact"):
     from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
     from geoswe_b200.synthetic import MANNING_CLASSES
     mesh = Mesh2D(nx=n, ny=n, dx=3.0, dy=3.0, ngh=2)
     cfg = Config(bc_x="wall", bc_y="wall", bc={"x+": "fall"}, cfl=0.5, dtype=dtype,
-                 friction="manning",
+                 friction="manning", arith=arith,
                  rainfall_forcing=RainfallForcing(time_s=[0.0, 1e9], rate_mm_h=[50.0, 50.0]))
     q0 = np.zeros((3, n, n), np.float32)
     s = Solver2D(mesh, cfg, q0, z)
@@ -150,15 +150,13 @@ def bytes_per_cell(track_max=True):
     return 16 + 1 + 12 + (8 if track_max else 0)
 
 
-def run_gsw(args, rank, world):
+def measure_dense(args, z, cls, n, world, arith="exact"):
+    """Device-resident throughput of the dense rain-on-terrain run with one arithmetic:
+    warm-up, launch-shape tuning, a warm-up of the timed window (its graph is captured
+    there), then exactly `steps` timed steps between CUDA events; then the step
+    kernel alone (CUDA events, same launch shape) for the roofline."""
     import torch
-    from geoswe_b200 import _lib
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    n = args.n
-    z, cls = build_case(n)
-    cells = n * n
-    # ---------------- device-resident throughput (value) ----------------
-    s = make_solver(z, cls, n)
+    s = make_solver(z, cls, n, arith=arith)
     s.run(t_end=1e12, max_steps=args.warmup)
     tune = None
     if not args.no_tune:
@@ -184,15 +182,27 @@ def run_gsw(args, rank, world):
     ms = e0.elapsed_time(e1)
     launches = s.kernel_launches - l0
     assert steps == args.steps, (steps, args.steps)
-    # ---------------- dominant kernel alone (roofline) ----------------
     kern_ms = time_step_kernel(s, reps=args.kernel_reps)
     shape = {"tile_rows": s._tile_rows or 32, "warps": s._warps or 4, "min_blocks": s._min_blocks}
-    # ---------------- end to end through the public API ----------------
-    e2e = run_e2e(args, z, cls, n)
     del s
     torch.cuda.empty_cache()
     if world > 1:
         ms = max_over_ranks(ms, "cuda")
+    return dict(ms=ms, launches=launches, kern_ms=kern_ms, clocks=clocks, shape=shape, tune=tune)
+
+
+def run_gsw(args, rank, world):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    n = args.n
+    z, cls = build_case(n)
+    cells = n * n
+    # ---------------- device-resident throughput (value), exact arithmetic ----------------
+    m = measure_dense(args, z, cls, n, world, "exact")
+    ms, kern_ms = m["ms"], m["kern_ms"]
+    # ---------------- end to end through the public API ----------------
+    e2e = run_e2e(args, z, cls, n)
+    torch.cuda.empty_cache()
     value = cells * args.steps * world / (ms / 1e3)
     peak, peak_kind = _peaks()
     bpc = bytes_per_cell(True)
@@ -203,17 +213,31 @@ def run_gsw(args, rank, world):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": dense_config(n, world),
         "e2e": e2e,
-        "gpu_launches": int(launches),
+        "gpu_launches": int(m["launches"]),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": DRAM_BYTES_PER_CELL["dense"] * cells / 1e9,
                      "traffic_unit": "GB per launch (ncu, 4096x4096 capture scaled by cells)",
                      "kernel": "dense_march_kernel<float,true>", "kernel_ms": kern_ms,
                      "bytes_per_cell": bpc, "peak_source": peak_kind},
-        "clocks": clocks,
-        "launch_shape": shape,
+        "clocks": m["clocks"],
+        "arith": "exact (IEEE, bit-identical to the reference kernel without FMA contraction)",
+        "launch_shape": m["shape"],
     }
-    if tune is not None:
-        out["autotune"] = tune
+    if m["tune"] is not None:
+        out["autotune"] = m["tune"]
+    # ---------------- the opt-in fast arithmetic, same workload ----------------
+    if not args.no_fast:
+        f = measure_dense(args, z, cls, n, world, "fast")
+        f_ach = bpc * cells / (f["kern_ms"] / 1e3) / 1e9
+        out["fast_arith"] = {
+            "what": "Config(arith='fast'): FMA contraction, approximate binary32 sqrt/div; same workload and "
+                    "step count; held to a depth tolerance, not bit equality (depth error in cpu_baseline)",
+            "value": cells * args.steps * world / (f["ms"] / 1e3), "unit": UNIT,
+            "ms_per_step": f["ms"] / args.steps, "gpu_launches": int(f["launches"]),
+            "roofline": {"bound": "hbm", "achieved": f_ach, "peak": peak, "unit": "GB/s", "frac": f_ach / peak,
+                         "kernel": "gsw_fast::dense_march_kernel<float,true>", "kernel_ms": f["kern_ms"],
+                         "peak_source": peak_kind},
+            "clocks": f["clocks"], "launch_shape": f["shape"]}
     if rank == 0 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
@@ -534,6 +558,12 @@ def fp64_depth_error(n, t_end):
     torch.cuda.synchronize()
     h32 = s.depth().astype(np.float64)
     h64 = ref.q[0][2:-2, 2:-2]
+    cfg_f = Config(bc_x="wall", bc_y="wall", bc={"x+": "fall"}, friction="manning", arith="fast",
+                   rainfall_forcing=RainfallForcing(time_s=[0.0, 1e9], rate_mm_h=[50.0, 50.0]))
+    sf = Solver2D(Mesh2D(nx=n, ny=n, dx=3.0, dy=3.0, ngh=2), cfg_f, np.zeros((3, n, n), np.float32), z)
+    sf.set_manning_table(np.pad(cls, 2, mode="edge"), MANNING_CLASSES)
+    steps_f = sf.run(t_end=t_end)
+    df = sf.depth().astype(np.float64) - h64
     # the reference's NumPy fp32 path (it accumulates the bed source in float64)
     ref32 = numpy_ref._rain_on_terrain_solver(n, dtype=np.float32)
     steps_r32 = ref32.run(t_end=t_end)
@@ -544,6 +574,8 @@ def fp64_depth_error(n, t_end):
             "steps_fp32_gpu": int(steps32), "steps_fp64_cpu": int(steps64),
             "reference_numpy_fp32_vs_fp64": {"max_m": float(np.abs(dr).max()),
                                            "rmse_m": float(np.sqrt(np.mean(dr * dr))), "steps": int(steps_r32)},
+            "fast_arith_vs_fp64": {"max_m": float(np.abs(df).max()), "rmse_m": float(np.sqrt(np.mean(df * df))),
+                                   "steps": int(steps_f)},
             "seconds": time.perf_counter() - t0}
 
 
@@ -558,6 +590,7 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=512)
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fast", action="store_true", help="skip the fast-arithmetic measurement")
     ap.add_argument("--err-n", type=int, default=96, help="fp64 depth-error sample size (0: skip)")
     ap.add_argument("--err-t-end", type=float, default=600.0)
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")

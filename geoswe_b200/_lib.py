@@ -22,6 +22,7 @@ BC_EXTRAPOLATE, BC_WALL, BC_FALL, BC_PERIODIC, BC_NONE = 0, 1, 2, 3, 4
 BC_CODES = {"extrapolate": BC_EXTRAPOLATE, "wall": BC_WALL, "fall": BC_FALL,
             "periodic": BC_PERIODIC, "none": BC_NONE}
 RAIN_NONE, RAIN_UNIFORM, RAIN_GRIDDED, RAIN_LOOKUP = 0, 1, 2, 3
+ARITH_EXACT, ARITH_FAST = 0, 1
 FRICTION_NONE, FRICTION_TABLE, FRICTION_FIELD = 0, 1, 2
 NORM_LINF, NORM_L2 = 0, 1
 BRICK_W, BRICK_PITCH = 30, 32
@@ -53,7 +54,7 @@ class GswDenseArgs(C.Structure):
                 ("friction_kind", i32), ("n_cls", vp), ("n_cls_pitch", i64), ("n_tab", vp),
                 ("n_tab_len", i32), ("n_field", vp), ("vcap", f64), ("quadratic", i32),
                 ("keep_h", i32), ("max_h", vp), ("cfl_skip", vp), ("h_cfl", f64),
-                ("tile_rows", i32), ("warps", i32), ("min_blocks", i32), ("reserved", i32)]
+                ("tile_rows", i32), ("warps", i32), ("min_blocks", i32), ("arith", i32)]
 
 
 class GswBcArgs(C.Structure):
@@ -78,7 +79,7 @@ class GswInflowArgs(C.Structure):
 
 class GswFlatArgs(C.Structure):
     _fields_ = [("abi_version", u32), ("dtype", i32), ("brick_h", i32), ("warps", i32), ("min_blocks", i32),
-                ("reserved1", i32), ("n_bricks", i64),
+                ("arith", i32), ("n_bricks", i64),
                 ("brick_ij", vp), ("brick_nbr", vp), ("flags", vp),
                 ("q0", vp), ("q1", vp), ("q2", vp), ("qn0", vp), ("qn1", vp), ("qn2", vp), ("bed", vp),
                 ("inv_dx", f64), ("inv_dy", f64), ("g", f64), ("h_min", f64), ("h_min_cfl", f64),
@@ -129,7 +130,8 @@ class GswMember(C.Structure):
 
 class GswEnsembleArgs(C.Structure):
     _fields_ = [("abi_version", u32), ("brick_h", i32), ("n_bricks", i64), ("n_members", i32),
-                ("warps", i32), ("grid", i32), ("min_blocks", i32), ("brick_ij", vp), ("brick_nbr", vp),
+                ("warps", i32), ("grid", i32), ("min_blocks", i32), ("arith", i32), ("reserved0", i32),
+                ("brick_ij", vp), ("brick_nbr", vp),
                 ("brick_member", vp), ("flags", vp), ("n_cls", vp), ("q0", vp), ("q1", vp), ("q2", vp),
                 ("qn0", vp), ("qn1", vp), ("qn2", vp), ("bed", vp), ("max_h", vp), ("members", vp),
                 ("states", vp), ("scratch", vp), ("all_done", vp)]

@@ -165,6 +165,9 @@ class FlatAdjoint:
             raise ValueError("window must be in [1, n_steps]")
         if dtype not in ("float32", "float64"):
             raise ValueError("dtype must be float32 or float64")
+        if cs.arith != L.ARITH_EXACT:
+            raise ValueError("FlatAdjoint: the adjoint differentiates the exact step; build the solver "
+                             "with arith='exact'")
         self.cs = cs
         self.dev = cs.device
         self.code = L.F32 if dtype == "float32" else L.F64

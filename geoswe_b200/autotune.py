@@ -29,6 +29,11 @@ def _cache_path() -> Path:
     return Path(p) if p else Path.home() / ".cache" / "geoswe_b200" / "autotune.json"
 
 
+def kind(base, arith=0):
+    """Cache kind of a kernel family: the fast-arithmetic kernels tune separately."""
+    return base if int(arith) == L.ARITH_EXACT else base + "-fast"
+
+
 def _key(kind, cells):
     dev = torch.cuda.get_device_name()
     drv = torch.version.cuda or ""
@@ -116,7 +121,7 @@ def tune_dense(s, reps=8, space=None, store=True, verbose=False):
     best = min(table, key=lambda e: e["ms"])
     cells = s.mesh.nx * s.mesh.ny
     if store:
-        _store("dense", cells, best)
+        _store(kind("dense", s.arith), cells, best)
     return best, table
 
 
@@ -139,7 +144,7 @@ def tune_ensemble(ens, t_end, reps=6, space=None, store=True, verbose=False):
     best = min(table, key=lambda e: e["ms"])
     ens.warps, ens.grid, ens.min_blocks = best["warps"], best["grid"], best["min_blocks"]
     if store:
-        _store("ensemble", ens.nslots, best)
+        _store(kind("ensemble", ens.arith), ens.nslots, best)
     return best, table
 
 
@@ -194,5 +199,5 @@ def tune_flat(cs, reps=6, space=None, store=True, verbose=False):
     cs.warps, cs.min_blocks = best["warps"], best["min_blocks"]
     cs._graph_cache.clear()
     if store:
-        _store("flat", cs.nslots, best)
+        _store(kind("flat", cs.arith), cs.nslots, best)
     return best, table

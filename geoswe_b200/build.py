@@ -5,7 +5,9 @@
 
 The library is compiled with ``--fmad=false``: every multiply and add of the step is
 rounded separately, in the reference's operand order, so the C oracle reproduces the
-kernels' values exactly. Only nvcc is needed; no GPU is touched.
+kernels' values exactly. The one exception is gsw_fast.cu, the opt-in fast-arithmetic
+compilation of the binary32 step kernels (FMA contraction, flush-to-zero). Only nvcc
+is needed; no GPU is touched.
 """
 from __future__ import annotations
 
@@ -23,6 +25,11 @@ LIB = PKG / "libgsw.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
+# The fast-arithmetic compilation of the binary32 step kernels (gsw_fast.cu): FMA
+# contraction and flush-to-zero; its square root and division are the approximate
+# instructions named in gsw_core.cuh.
+FAST_SOURCES = {"gsw_fast.cu"}
+FAST_FLAGS = [f for f in NVCC_FLAGS if f != "--fmad=false"] + ["--fmad=true", "-ftz=true"]
 
 
 def sources():
@@ -56,7 +63,8 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> Path:
     nvcc = _nvcc()
     for src in sources():
         obj = build_dir / (src.stem + ".o")
-        cmd = [nvcc, *ARCH, *NVCC_FLAGS, *extra, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+        flags = FAST_FLAGS if src.name in FAST_SOURCES else NVCC_FLAGS
+        cmd = [nvcc, *ARCH, *flags, *extra, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
         if src.suffix == ".cpp":
             cmd = [nvcc, "-x", "c++", "-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
                    "-Xcompiler", "-fvisibility=hidden", *extra, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]

@@ -125,7 +125,7 @@ class CompressedSolver:
                            h_min=max(float(cfg.h_min), 1.0e-6) if h_min is None else float(h_min),
                            cfl_linf=cfl_linf, vcap=float(cfg.friction_velocity_cap_ms),
                            quad=bool(cfg.friction_quadratic_alpha), keep_h=bool(cfg.wetdry_keep_h),
-                           dt_max=dt_max, brick_h=brick_h)
+                           dt_max=dt_max, brick_h=brick_h, arith=cfg.arith)
         self._dense_had_rain = cfg.rainfall_forcing is not None or cfg.rainfall > 0.0
         t0 = time.perf_counter()
         dev = self.device
@@ -174,7 +174,7 @@ class CompressedSolver:
     @classmethod
     def from_cache(cls, cache_dir, *, cfl: float = 0.5, h_min: float = 1e-6, g: float = 9.81, dt_max=None,
                    cfl_linf: bool = False, brick_h: Optional[int] = None, track_max_depth: bool = True,
-                   device=None, say=None):
+                   device=None, say=None, arith: str = "exact"):
         """Load a flat-mesh cache in the reference's format (save_cache /
         run_cached, compressed_solver.py:2504-2560, 2616-2780): meta.json plus .npy files
         (nbr int16 deltas, is_active, ij_active, q0..q2, bed_f, mcls_f, m_tab, and the
@@ -207,7 +207,8 @@ class CompressedSolver:
         dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self._init_physics(device=dev, nxp=nxp, nyp=nyp, ngh=ngh, nx=nxp - 2 * ngh, ny=nyp - 2 * ngh,
                            dx=float(meta["dx"]), g=g, cfl=cfl, h_min=max(float(h_min), 1.0e-6),
-                           cfl_linf=cfl_linf, vcap=15.0, quad=True, keep_h=True, dt_max=dt_max, brick_h=brick_h)
+                           cfl_linf=cfl_linf, vcap=15.0, quad=True, keep_h=True, dt_max=dt_max, brick_h=brick_h,
+                           arith=arith)
         self.cache_meta = meta
         inside = np.zeros((nxp, nyp), np.uint8)
         act = is_active != 0
@@ -262,7 +263,10 @@ class CompressedSolver:
 
     # ------------------------------------------------------------- construction
     def _init_physics(self, *, device, nxp, nyp, ngh, nx, ny, dx, g, cfl, h_min, cfl_linf, vcap, quad, keep_h,
-                      dt_max, brick_h):
+                      dt_max, brick_h, arith="exact"):
+        if arith not in ("exact", "fast"):
+            raise ValueError(f"CompressedSolver: arith={arith!r} invalid; expected 'exact' or 'fast'")
+        self.arith = L.ARITH_FAST if arith == "fast" else L.ARITH_EXACT
         self.brick_h = int(brick_h or type(self).brick_h)
         self.device = torch.device(device)
         self.nxp, self.nyp, self.ngh = int(nxp), int(nyp), int(ngh)
@@ -340,7 +344,7 @@ class CompressedSolver:
         self._forcing = {}
         self.warps, self.min_blocks = 0, 0
         from . import autotune
-        best = autotune.load("flat", self.nslots)
+        best = autotune.load(autotune.kind("flat", self.arith), self.nslots)
         if best:
             self.warps, self.min_blocks = int(best["warps"]), int(best["min_blocks"])
         self._graph_cache = {}
@@ -676,6 +680,7 @@ class CompressedSolver:
         a.linf = int(self.cfl_linf)
         a.ngh, a.nx, a.ny = self.ngh, self.nx, self.ny
         a.warps, a.min_blocks = self.warps, self.min_blocks
+        a.arith = self.arith
         if step:
             a.state = _ptr(self._state)
             a.lam_target = C.c_void_p(self._state.data_ptr() + L.GswLoopState.lam_bits.offset)

@@ -62,9 +62,13 @@ def check_numeric_inputs(where="Config", **vals):
 class Config:
     """Solver configuration; ``Config()`` is the production flood scheme.
 
-    Extension over the reference: ``bc`` takes an optional per-face mapping
+    Extensions over the reference: ``bc`` takes an optional per-face mapping
     ``{"x-": kind, "x+": kind, "y-": kind, "y+": kind}`` that overrides ``bc_x``/``bc_y``
     face by face (for example one open outflow edge on an otherwise walled domain).
+    ``arith`` selects the step's arithmetic: ``"exact"`` (default; separately rounded
+    IEEE operations, bit-identical to the reference kernel compiled without FMA
+    contraction) or ``"fast"`` (binary32 only: FMA contraction, approximate square root
+    and division; held to a depth tolerance against ``"exact"``, not to bit equality).
     """
     pde: str = "baseline"
     flux: str = "hllc"
@@ -92,6 +96,7 @@ class Config:
     dtype: Optional[str] = None
     wetdry_keep_h: bool = True
     bc: Optional[dict] = None
+    arith: str = "exact"
 
     def __post_init__(self):
         if self.dtype is None:
@@ -113,13 +118,15 @@ class Config:
                    "recon": {"first", "muscl", "linear2", "linear3", "linear5", "weno5"},
                    "wb_method": {"audusse", "srm"}, "pde": {"igr", "baseline"},
                    "dtype": {"float32", "float64"}, "bc_x": _BC_OK, "bc_y": _BC_OK,
-                   "friction": {"manning_implicit"}}
+                   "friction": {"manning_implicit"}, "arith": {"exact", "fast"}}
         for k, ok in enum_ok.items():
             v = getattr(self, k, None)
             if v is None and k == "friction":
                 continue
             if not isinstance(v, str) or v not in ok:
                 raise ValueError(f"Config.{k}={v!r} invalid; expected one of {sorted(ok)}")
+        if self.arith == "fast" and self.dtype != "float32":
+            raise ValueError("Config.arith='fast' is binary32 only; use dtype='float32' or arith='exact'")
         if self.friction is None and (self.manning_n > 0.0 or self.manning_field is not None):
             warnings.warn("Config: a Manning roughness is set but friction is off, so the run is "
                           "frictionless; pass friction='manning' to apply it", stacklevel=3)

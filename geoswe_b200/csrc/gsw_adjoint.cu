@@ -350,6 +350,7 @@ static int fill_adj(const GswFlatAdjArgs* a, AdjK<T>& k) {
     if (f.n_tab_len > 256) return set_error(GSW_ERR_RANGE, "adjoint: at most 256 Manning classes");
     if (f.rain_kind != GSW_RAIN_NONE && !f.rain) return set_error(GSW_ERR_INVALID, "adjoint: rain is NULL");
     if (f.rain_kind == GSW_RAIN_LOOKUP) return set_error(GSW_ERR_INVALID, "adjoint: lookup rain is not differentiated");
+    if (f.arith != GSW_ARITH_EXACT) return set_error(GSW_ERR_INVALID, "adjoint: the exact step is differentiated (arith)");
     if (!a->lam_in0 || !a->lam_in1 || !a->lam_in2 || !a->lam_out0 || !a->lam_out1 || !a->lam_out2 ||
         !a->rbar0 || !a->rbar1 || !a->rbar2 || !a->n_bar)
         return set_error(GSW_ERR_INVALID, "adjoint: null adjoint buffer");

@@ -8,13 +8,22 @@
 #include "../../include/gsw.h"
 #include "gsw_core.cuh"
 
-namespace gsw {
-
-// Thread-local message behind gsw_last_error(); defined in gsw_loop.cu.
+// Library runtime, defined once in gsw_loop.cu: the thread-local message behind
+// gsw_last_error(), the launch counter, the SM count. Kept out of namespace gsw, which
+// a second compilation of the step kernels renames (gsw_fast.cu).
+namespace gsw_rt {
 int set_error(int code, const char* fmt, ...);
 int check_launch(const char* what);
 int sm_count();
 void count_launch(int n = 1);
+}  // namespace gsw_rt
+
+namespace gsw {
+
+using gsw_rt::set_error;
+using gsw_rt::check_launch;
+using gsw_rt::sm_count;
+using gsw_rt::count_launch;
 
 // Max of a non-negative IEEE-bits value over the block, then one atomicMax.
 // Every thread of the block must call it (it holds a block barrier).

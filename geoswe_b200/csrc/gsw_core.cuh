@@ -4,7 +4,9 @@
 // (geoswe/rhs_cuda.py:900-1207 for the residual, :1757-1796 for the update tail) and
 // is evaluated with separately rounded IEEE operations: the library is compiled with
 // --fmad=false and uses no fast-math intrinsics, so the C oracle (oracle/gsw_oracle.c)
-// reproduces every value.
+// reproduces every value. gsw_fast.cu compiles the binary32 step kernels a second time
+// with GSW_FAST_ARITH (FMA contraction, approximate square root and division): the
+// opt-in fast arithmetic, held to a stated depth tolerance instead of bit equality.
 //
 // Face sharing. The reference evaluates the four faces of every cell, so each
 // interior face is computed twice, once from each side. From the right-hand cell
@@ -27,10 +29,15 @@ __device__ __forceinline__ float  gmax(float a, float b)   { return fmaxf(a, b);
 __device__ __forceinline__ float  gmin(float a, float b)   { return fminf(a, b); }
 __device__ __forceinline__ double gmax(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ double gmin(double a, double b) { return fmin(a, b); }
-__device__ __forceinline__ float  gsqrt(float a)  { return sqrtf(a); }
 __device__ __forceinline__ double gsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ double gdiv(double a, double b) { return a / b; }
 __device__ __forceinline__ float  gabs(float a)   { return fabsf(a); }
 __device__ __forceinline__ double gabs(double a)  { return fabs(a); }
+
+#ifndef GSW_FAST_ARITH
+// Exact arithmetic (the default compilation): IEEE square root and division.
+__device__ __forceinline__ float gsqrt(float a) { return sqrtf(a); }
+__device__ __forceinline__ float gdiv(float a, float b) { return a / b; }
 
 // Exact-zero operands take the IEEE square root's and division's out-of-range path,
 // which is a subroutine call; dry faces (sqrt(g * 0)) and fluid at rest (0 / h) hit it
@@ -49,6 +56,26 @@ __device__ __forceinline__ T div_z(T a, T b) {
     const T q = (zr ? (T)1 : a) / b;
     return zr ? a * b : q;
 }
+#else
+// Fast arithmetic (gsw_fast.cu, compiled with FMA contraction and flush-to-zero):
+// binary32 square root and division by the hardware approximations, sqrt.approx
+// (relative error about 2^-23) and div.full (at most 2 ulp, full range); no slow path,
+// so no zero guards. Binary64 keeps the IEEE operations.
+__device__ __forceinline__ float gsqrt(float a) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+__device__ __forceinline__ float gdiv(float a, float b) {
+    float r;
+    asm("div.full.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float  sqrt_z(float x) { return gsqrt(x); }
+__device__ __forceinline__ float  div_z(float a, float b) { return gdiv(a, b); }
+__device__ __forceinline__ double sqrt_z(double x) { return x == 0.0 ? x : sqrt(x); }
+__device__ __forceinline__ double div_z(double a, double b) { return a / b; }
+#endif
 
 // Primitive state of one cell (PRIMS macro, rhs_cuda.py:931-938) plus what the
 // faces need: free surface and the central bed gradients.
@@ -89,7 +116,7 @@ __device__ __forceinline__ float pow_m43(float x) {
         t = t * third;
         r = r + t;
     }
-    return r / x;
+    return gdiv(r, x);
 }
 // fp64: the same iteration in double, six steps from the binary32 guess; r/x is within
 // ~6 double ulp of x^(-4/3).
@@ -122,7 +149,7 @@ __device__ __forceinline__ void hllc(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
     const T aR = sqrt_z(g * (hR > z ? hR : z));
     const T u_st = half * (uNL + uNR) + aL - aR;
     const T h_rt = half * (aL + aR) + quarter * (uNL - uNR);
-    const T h_st = (h_rt > z) ? (h_rt * h_rt) / g : z;
+    const T h_st = (h_rt > z) ? gdiv(h_rt * h_rt, g) : z;
     const T a_st = sqrt_z(g * (h_st > z ? h_st : z));
     const T SL_w = gmin(uNL - aL, u_st - a_st);
     const T SR_w = gmax(uNR + aR, u_st + a_st);
@@ -156,7 +183,7 @@ __device__ __forceinline__ void hllc(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
     const T hK = left ? hL : hR, uNK = left ? uNL : uNR, uTK = left ? uTL : uTR;
     const T huNK = left ? huNL : huNR, huTK = left ? huTL : huTR;
     const T FK_h = left ? FL_h : FR_h, FK_N = left ? FL_N : FR_N, FK_T = left ? FL_T : FR_T;
-    const T fac = (S - uNK) / (S - SM + (T)1.0e-30);
+    const T fac = gdiv(S - uNK, S - SM + (T)1.0e-30);
     const T hKs = hK * fac;
     const T huNKs = hKs * SM;
     const T huTKs = hKs * uTK;
@@ -257,16 +284,16 @@ __device__ __forceinline__ void wetdry_friction(T& h, T& hu, T& hv, bool frictio
     const T modU = sqrt_z(u * u + v * v);
     const T h43 = pow_m43(hs);
     if (modU > vcap) {
-        const T n_cri = gsqrt((T)1.0 / (((T)1.0e-10 + dt) * g * h43 * (modU + (T)1.0e-30)));
+        const T n_cri = gsqrt(gdiv((T)1.0, ((T)1.0e-10 + dt) * g * h43 * (modU + (T)1.0e-30)));
         if (n_cri > n) n = n_cri;
     }
     const T Cf = g * n * n * h43;
     T alpha;
     if (quadratic) {
         const T twodtCfU = (T)2.0 * dt * Cf * modU;
-        alpha = (T)2.0 / (gsqrt((T)1.0 + (T)2.0 * twodtCfU) + (T)1.0);
+        alpha = gdiv((T)2.0, gsqrt((T)1.0 + (T)2.0 * twodtCfU) + (T)1.0);
     } else {
-        alpha = (T)1.0 / ((T)1.0 + dt * Cf * modU);
+        alpha = gdiv((T)1.0, (T)1.0 + dt * Cf * modU);
     }
     hu = hu * alpha;
     hv = hv * alpha;
@@ -284,7 +311,7 @@ __device__ __forceinline__ unsigned long long lam_dense_bits(float h, float hu, 
     const float u = div_z(hu, h);
     const float v = div_z(hv, h);
     const float au = fabsf(u), av = fabsf(v);
-    const float lam = ((au > av) ? au : av) + sqrtf(g * h);
+    const float lam = ((au > av) ? au : av) + gsqrt(g * h);
     const bool fin = (lam <= 3.0e38f) && (au <= 3.0e38f) && (av <= 3.0e38f);
     return fin ? (unsigned long long)__double_as_longlong((double)lam) : 0x7ff0000000000000ull;
 }
@@ -315,7 +342,7 @@ __device__ __forceinline__ unsigned long long lam_flat_bits(float h, float hu, f
     if (h < h_min) return 0ull;
     const float hs = h > h_min_cfl ? h : h_min_cfl;
     const float u = div_z(hu, hs), v = div_z(hv, hs);
-    const float c = sqrtf(g * (h > 0.0f ? h : 0.0f));
+    const float c = gsqrt(g * (h > 0.0f ? h : 0.0f));
     const float speed = linf ? fmaxf(fabsf(u), fabsf(v)) : sqrt_z(u * u + v * v);
     const float l = speed + c;
     return (unsigned long long)__double_as_longlong((double)l);

@@ -1,206 +1,10 @@
-// gsw_dense.cu -- dense-grid kernels of the GeoSWE step for sm_100a and their C ABI.
-//
-// Column march. A warp owns a strip of 32 adjacent columns (lane = column, so every
-// load of a row is one coalesced 128-byte access) and walks it down `tile_rows` rows.
-// Lanes 1..30 are output columns, lanes 0 and 31 are the strip's halo columns.
-//   * x-faces (between rows i and i+1) are computed once per row and carried down the
-//     column in registers: the face below row i is the face above row i+1;
-//   * y-faces (between columns) are computed once by the left lane and handed to the
-//     right lane with one warp shuffle;
-// so each face is evaluated once instead of twice, and no shared memory or block
-// barrier is needed on the step path. The new state's wave speed is reduced in
-// registers, then per block, then with one 64-bit atomicMax.
-#include "gsw_common.cuh"
+// gsw_dense.cu -- dense-grid kernels of the GeoSWE step for sm_100a and their C ABI:
+// the fused step and residual (the column march of gsw_dense_march.cuh), the standalone
+// wave speed, the ghost fill, the stage boundary.
+#include "gsw_dense_march.cuh"
+#include "gsw_fast.h"
 
 namespace gsw {
-
-template <typename T>
-struct DenseK {
-    const T* q0; const T* q1; const T* q2;
-    T* o0; T* o1; T* o2;
-    const T* b;
-    const uint8_t* mask; int64_t mpitch;
-    int nxp, nyp, lo;            // cells [lo, n-lo) are computed (lo = ngh, or 2 for the residual)
-    int ngh;
-    int64_t pitch;
-    T inv_dx, inv_dy, half_dx, half_dy, g, h_min;
-    const GswLoopState* st;
-    unsigned long long* lam;
-    int rain_kind; const T* rain;
-    int friction_kind; const uint8_t* ncls; int64_t cpitch; const T* ntab; const T* nfield;
-    T vcap; int quad; int keep_h;
-    T* max_h;
-    const uint8_t* cfl_skip;
-    T h_cfl;
-    int tile_rows;
-};
-
-template <typename T>
-__device__ __forceinline__ T ldg_at(const T* a, int64_t pitch, int i, int j) {
-    return __ldg(a + (int64_t)i * pitch + j);
-}
-
-// Central y-gradient of the bed at (row, lane column): neighbours come from the
-// adjacent lanes; the strip's edge lanes read their outer neighbour directly.
-template <typename T>
-__device__ __forceinline__ T grad_y(const DenseK<T>& p, T bc, int row, int c, int lane) {
-    T bl = __shfl_up_sync(0xffffffffu, bc, 1);
-    T br = __shfl_down_sync(0xffffffffu, bc, 1);
-    if (lane == 0)  bl = ldg_at(p.b, p.pitch, row, max(c - 1, 0));
-    if (lane == 31) br = ldg_at(p.b, p.pitch, row, min(c + 1, p.nyp - 1));
-    return (T)0.5 * (br - bl) * p.inv_dy;
-}
-
-template <typename T>
-__device__ __forceinline__ void load_cell(const DenseK<T>& p, Cell<T>& c, int row, int col) {
-    c.h = ldg_at(p.q0, p.pitch, row, col);
-    c.hu = ldg_at(p.q1, p.pitch, row, col);
-    c.hv = ldg_at(p.q2, p.pitch, row, col);
-}
-
-template <typename T>
-__device__ __forceinline__ Cell<T> shfl_cell_down(const Cell<T>& c) {
-    Cell<T> r;
-    r.h = __shfl_down_sync(0xffffffffu, c.h, 1);
-    r.u = __shfl_down_sync(0xffffffffu, c.u, 1);
-    r.v = __shfl_down_sync(0xffffffffu, c.v, 1);
-    r.eta = __shfl_down_sync(0xffffffffu, c.eta, 1);
-    r.b = __shfl_down_sync(0xffffffffu, c.b, 1);
-    r.gy = __shfl_down_sync(0xffffffffu, c.gy, 1);
-    r.gx = r.gy; r.hu = r.h; r.hv = r.h;   // unused by a y-face
-    return r;
-}
-
-template <typename T>
-__device__ __forceinline__ Face<T> shfl_face_up(const Face<T>& f) {
-    Face<T> r;
-    r.Fh = __shfl_up_sync(0xffffffffu, f.Fh, 1);
-    r.Fn = __shfl_up_sync(0xffffffffu, f.Fn, 1);
-    r.Ft = __shfl_up_sync(0xffffffffu, f.Ft, 1);
-    r.srcR = __shfl_up_sync(0xffffffffu, f.srcR, 1);
-    r.srcL = r.srcR;
-    r.wet = __shfl_up_sync(0xffffffffu, (int)f.wet, 1) != 0;
-    return r;
-}
-
-template <typename T>
-__device__ __forceinline__ T dt_of(const GswLoopState* st);
-template <> __device__ __forceinline__ float  dt_of<float>(const GswLoopState* st)  { return st->dt_f32; }
-template <> __device__ __forceinline__ double dt_of<double>(const GswLoopState* st) { return st->dt; }
-
-// STEP = false: residual into o0..o2. STEP = true: updated state into o0..o2.
-template <typename T, bool STEP, int MINB>
-__global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
-    if (STEP && p.st->done) return;                       // grid-uniform
-    const int lane = threadIdx.x;
-    const int strip = blockIdx.x * blockDim.y + threadIdx.y;
-    const int jend = p.nyp - p.lo;
-    const int col0 = p.lo + strip * 30;
-    const bool warp_active = col0 < jend;
-    const int c = col0 - 1 + lane;
-    const int cl = min(c, p.nyp - 1);
-    const bool out_lane = warp_active && lane >= 1 && lane <= 30 && c < jend;
-    const int i0 = p.lo + blockIdx.y * p.tile_rows;
-    const int i1 = min(i0 + p.tile_rows, p.nxp - p.lo);
-    unsigned long long lam_local = 0ull;
-
-    T dt = (T)0;
-    T rate = (T)0;
-    const T* frame = nullptr;
-    if (STEP) {
-        dt = dt_of<T>(p.st);
-        if (p.rain_kind == GSW_RAIN_UNIFORM) rate = p.rain[p.st->rain_idx];
-        if (p.rain_kind == GSW_RAIN_GRIDDED)
-            frame = p.rain + (int64_t)p.st->rain_idx * (int64_t)(p.nxp - 2 * p.ngh) * (p.nyp - 2 * p.ngh);
-    }
-
-    if (warp_active && i0 < i1) {
-        Cell<T> cur, nx;
-        const T b_m2 = ldg_at(p.b, p.pitch, i0 - 2, cl);
-        load_cell(p, cur, i0 - 1, cl);
-        cur.b = ldg_at(p.b, p.pitch, i0 - 1, cl);
-        load_cell(p, nx, i0, cl);
-        nx.b = ldg_at(p.b, p.pitch, i0, cl);
-        T b_next = ldg_at(p.b, p.pitch, i0 + 1, cl);
-        // prefetch of the row after next: its loads are in flight during this row's faces
-        T pf_h = ldg_at(p.q0, p.pitch, i0 + 1, cl);
-        T pf_hu = ldg_at(p.q1, p.pitch, i0 + 1, cl);
-        T pf_hv = ldg_at(p.q2, p.pitch, i0 + 1, cl);
-        T pf_b = ldg_at(p.b, p.pitch, i0 + 2, cl);
-        make_prims(cur, p.h_min);
-        make_prims(nx, p.h_min);
-        cur.gx = (T)0.5 * (nx.b - b_m2) * p.inv_dx;
-        cur.gy = (T)0;
-        nx.gx = (T)0.5 * (b_next - cur.b) * p.inv_dx;
-        nx.gy = grad_y(p, nx.b, i0, c, lane);
-        Face<T> Wf;
-        srm_face<T, true>(cur, nx, p.half_dx, p.inv_dx, p.g, p.h_min, Wf);
-        cur = nx;
-
-        for (int r = i0; r < i1; ++r) {
-            nx.h = pf_h; nx.hu = pf_hu; nx.hv = pf_hv;
-            nx.b = b_next;
-            const T b_p2 = pf_b;
-            if (r + 1 < i1) {           // rows r+2 / r+3 exist: the strip ends at i1 <= nxp - lo
-                pf_h = ldg_at(p.q0, p.pitch, r + 2, cl);
-                pf_hu = ldg_at(p.q1, p.pitch, r + 2, cl);
-                pf_hv = ldg_at(p.q2, p.pitch, r + 2, cl);
-                pf_b = ldg_at(p.b, p.pitch, r + 3, cl);
-            }
-            make_prims(nx, p.h_min);
-            nx.gx = (T)0.5 * (b_p2 - cur.b) * p.inv_dx;
-            nx.gy = grad_y(p, nx.b, r + 1, c, lane);
-
-            Face<T> Ef;
-            srm_face<T, true>(cur, nx, p.half_dx, p.inv_dx, p.g, p.h_min, Ef);
-            const Cell<T> rn = shfl_cell_down(cur);
-            Face<T> Nf;
-            srm_face<T, false>(cur, rn, p.half_dy, p.inv_dy, p.g, p.h_min, Nf);
-            const Face<T> Sf = shfl_face_up(Nf);
-
-            if (out_lane) {
-                T rh, rhu, rhv;
-                accumulate(Ef, Wf, Nf, Sf, rh, rhu, rhv);
-                const bool inside = (p.mask == nullptr) || (p.mask[(int64_t)r * p.mpitch + c] != 0);
-                if (!inside) { rh = (T)0; rhu = (T)0; rhv = (T)0; }
-                const int64_t o = (int64_t)r * p.pitch + c;
-                if (!STEP) {
-                    p.o0[o] = rh; p.o1[o] = rhu; p.o2[o] = rhv;
-                } else {
-                    T rr0 = rh;
-                    if (inside) {
-                        if (p.rain_kind == GSW_RAIN_UNIFORM) rr0 = rh + rate;
-                        else if (p.rain_kind == GSW_RAIN_GRIDDED)
-                            rr0 = rh + frame[(int64_t)(r - p.ngh) * (p.nyp - 2 * p.ngh) + (c - p.ngh)];
-                    }
-                    T h = cur.h + dt * rr0;
-                    T hu = cur.hu + dt * rhu;
-                    T hv = cur.hv + dt * rhv;
-                    T n = (T)0;
-                    if (p.friction_kind == GSW_FRICTION_TABLE)
-                        n = p.ncls ? p.ntab[p.ncls[(int64_t)r * p.cpitch + c]] : p.ntab[0];
-                    else if (p.friction_kind == GSW_FRICTION_FIELD) n = p.nfield[o];
-                    wetdry_friction<T>(h, hu, hv, p.friction_kind != GSW_FRICTION_NONE, n, dt, p.g,
-                                       p.h_min, p.vcap, p.quad != 0, p.keep_h != 0);
-                    p.o0[o] = h; p.o1[o] = hu; p.o2[o] = hv;
-                    if (p.max_h != nullptr && h > p.max_h[o]) p.max_h[o] = h;
-                    if (p.lam != nullptr) {
-                        const bool skip = (p.cfl_skip != nullptr) &&
-                            p.cfl_skip[(int64_t)(r - p.ngh) * (p.nyp - 2 * p.ngh) + (c - p.ngh)] != 0;
-                        if (!skip) {
-                            const unsigned long long lb = lam_dense_bits(h, hu, hv, p.g, p.h_cfl);
-                            lam_local = lb > lam_local ? lb : lam_local;
-                        }
-                    }
-                }
-            }
-            Wf = Ef;
-            cur = nx;
-            b_next = b_p2;
-        }
-    }
-    if (STEP && p.lam != nullptr) block_max_to(lam_local, p.lam);
-}
 
 // Standalone wave speed of the current state over the interior (lammax_fp32_lean).
 template <typename T>
@@ -354,71 +158,19 @@ __global__ void lam_cells_kernel(const T* q0, const T* q1, const T* q2, const in
 
 using namespace gsw;
 
-template <typename T>
-static int fill_dense(const GswDenseArgs* a, DenseK<T>& k, bool step) {
-    if (a->nxp < 5 || a->nyp < 5 || a->ngh < 2 || 2 * a->ngh >= a->nxp || 2 * a->ngh >= a->nyp)
-        return set_error(GSW_ERR_INVALID, "dense: need ngh >= 2 and a non-empty interior (nxp=%d nyp=%d ngh=%d)",
-                         a->nxp, a->nyp, a->ngh);
-    if (a->pitch < a->nyp) return set_error(GSW_ERR_INVALID, "dense: pitch %lld < nyp %d", (long long)a->pitch, a->nyp);
-    if (!a->q0 || !a->q1 || !a->q2 || !a->qn0 || !a->qn1 || !a->qn2 || !a->bed)
-        return set_error(GSW_ERR_INVALID, "dense: null state/output/bed pointer");
-    if (a->inside_mask && a->mask_pitch < a->nyp) return set_error(GSW_ERR_INVALID, "dense: mask_pitch < nyp");
-    k.q0 = (const T*)a->q0; k.q1 = (const T*)a->q1; k.q2 = (const T*)a->q2;
-    k.o0 = (T*)a->qn0; k.o1 = (T*)a->qn1; k.o2 = (T*)a->qn2;
-    k.b = (const T*)a->bed;
-    k.mask = a->inside_mask; k.mpitch = a->mask_pitch;
-    k.nxp = a->nxp; k.nyp = a->nyp; k.ngh = a->ngh; k.pitch = a->pitch;
-    k.lo = step ? a->ngh : 2;
-    k.inv_dx = (T)a->inv_dx; k.inv_dy = (T)a->inv_dy;
-    {   // dx = 1/inv_dx evaluated in T, as the reference kernel does (rhs_cuda.py:925-926)
-        const T dx = (T)1 / k.inv_dx, dy = (T)1 / k.inv_dy;
-        k.half_dx = (T)0.5 * dx; k.half_dy = (T)0.5 * dy;
-    }
-    k.g = (T)a->g; k.h_min = (T)a->h_min;
-    k.st = a->state; k.lam = (unsigned long long*)a->lam_target;
-    k.rain_kind = a->rain_kind; k.rain = (const T*)a->rain;
-    k.friction_kind = a->friction_kind; k.ncls = a->n_cls; k.cpitch = a->n_cls_pitch;
-    k.ntab = (const T*)a->n_tab; k.nfield = (const T*)a->n_field;
-    k.vcap = (T)a->vcap; k.quad = a->quadratic; k.keep_h = a->keep_h;
-    k.max_h = (T*)a->max_h; k.cfl_skip = a->cfl_skip; k.h_cfl = (T)a->h_cfl;
-    k.tile_rows = a->tile_rows > 0 ? a->tile_rows : 32;
-    if (step) {
-        if (!a->state) return set_error(GSW_ERR_INVALID, "dense step: state (GswLoopState*) is required");
-        if (a->rain_kind != GSW_RAIN_NONE && a->rain_kind != GSW_RAIN_UNIFORM && a->rain_kind != GSW_RAIN_GRIDDED)
-            return set_error(GSW_ERR_INVALID, "dense step: bad rain_kind %d", a->rain_kind);
-        if (a->rain_kind != GSW_RAIN_NONE && !a->rain) return set_error(GSW_ERR_INVALID, "dense step: rain is NULL");
-        if (a->friction_kind == GSW_FRICTION_TABLE && (!a->n_tab || a->n_tab_len < 1 ||
-                                                        (a->n_cls && a->n_cls_pitch < a->nyp)))
-            return set_error(GSW_ERR_INVALID, "dense step: table friction needs n_tab (and n_cls pitch >= nyp)");
-        if (a->friction_kind == GSW_FRICTION_FIELD && !a->n_field)
-            return set_error(GSW_ERR_INVALID, "dense step: field friction needs n_field");
-        if (a->friction_kind < 0 || a->friction_kind > 2) return set_error(GSW_ERR_INVALID, "dense step: bad friction_kind");
-    }
+// Exact or fast arithmetic; fast is binary32 only.
+static int check_arith(const GswDenseArgs* a) {
+    if (a->arith != GSW_ARITH_EXACT && a->arith != GSW_ARITH_FAST)
+        return set_error(GSW_ERR_INVALID, "dense: bad arith %d", a->arith);
+    if (a->arith == GSW_ARITH_FAST && a->dtype != GSW_F32)
+        return set_error(GSW_ERR_INVALID, "dense: fast arithmetic is binary32 only");
     return GSW_OK;
-}
-
-template <typename T, bool STEP>
-static int launch_march(const GswDenseArgs* a, cudaStream_t s) {
-    DenseK<T> k;
-    int rc = fill_dense<T>(a, k, STEP);
-    if (rc) return rc;
-    const int W = a->warps > 0 ? a->warps : 4;
-    const int minb = a->min_blocks;
-    if (minb != 0 && minb != 4 && minb != 5) return set_error(GSW_ERR_INVALID, "dense: min_blocks must be 0, 4 or 5");
-    if (W < 1 || W > 8) return set_error(GSW_ERR_INVALID, "dense: warps must be in [1, 8]");
-    const int ncols = k.nyp - 2 * k.lo, nrows = k.nxp - 2 * k.lo;
-    const int strips = (ncols + 29) / 30;
-    dim3 block(32, W);
-    dim3 grid((strips + W - 1) / W, (nrows + k.tile_rows - 1) / k.tile_rows);
-    if (grid.y > 65535u) return set_error(GSW_ERR_INVALID, "dense: too many row tiles (%u); raise tile_rows", grid.y);
-    if (minb == 0) dense_march_kernel<T, STEP, 1><<<grid, block, 0, s>>>(k);
-    else if (minb == 4) dense_march_kernel<T, STEP, 4><<<grid, block, 0, s>>>(k);
-    else dense_march_kernel<T, STEP, 5><<<grid, block, 0, s>>>(k);
-    return check_launch("dense_march");
 }
 
 extern "C" int gsw_dense_step(const GswDenseArgs* a, void* stream) {
     GSW_CHECK_ABI(a);
+    if (int rc = check_arith(a)) return rc;
+    if (a->arith == GSW_ARITH_FAST) return gsw_fast_dense_launch(a, true, (cudaStream_t)stream);
     if (a->dtype == GSW_F32) return launch_march<float, true>(a, (cudaStream_t)stream);
     if (a->dtype == GSW_F64) return launch_march<double, true>(a, (cudaStream_t)stream);
     return set_error(GSW_ERR_INVALID, "dense step: bad dtype %d", a->dtype);
@@ -433,11 +185,13 @@ static int launch_rhs(const GswDenseArgs* a, cudaStream_t s) {
         if (cudaMemset2DAsync(o, (size_t)a->pitch * sizeof(T), 0, rowb, (size_t)a->nxp, s) != cudaSuccess)
             return set_error(GSW_ERR_CUDA, "dense rhs: cudaMemset2DAsync failed");
     }
+    if (a->arith == GSW_ARITH_FAST) return gsw_fast_dense_launch(a, false, s);
     return launch_march<T, false>(a, s);
 }
 
 extern "C" int gsw_dense_rhs(const GswDenseArgs* a, void* stream) {
     GSW_CHECK_ABI(a);
+    if (int rc = check_arith(a)) return rc;
     if (a->dtype == GSW_F32) return launch_rhs<float>(a, (cudaStream_t)stream);
     if (a->dtype == GSW_F64) return launch_rhs<double>(a, (cudaStream_t)stream);
     return set_error(GSW_ERR_INVALID, "dense rhs: bad dtype %d", a->dtype);

@@ -1,78 +1,11 @@
-// gsw_ensemble.cu -- a batch of compressed meshes advanced by one persistent kernel per step.
-//
-// All members' bricks sit in one brick storage. A step is one launch of a persistent
-// grid (a few blocks per SM): warps stride over the global brick list, look up the
-// brick's member, and advance it with that member's dt, rain rate and Manning table
-// (gsw_flat.cu's per-brick march). Each member's new wave speed is reduced into its own
-// GswLoopState. The block that finishes last (a ticket counter in scratch memory)
-// then evaluates every member's time-step rule for the next launch, so members keep
-// their own CFL dt with no grid-wide barrier and no host round trip; a member that
-// reaches its end time drops out while the others continue.
-#include "gsw_flat_brick.cuh"
+// gsw_ensemble.cu -- a batch of compressed meshes advanced by one persistent kernel per
+// step (gsw_ensemble_march.cuh): the step, the initial wave speed and dt rule, and
+// their C ABI.
+#include "gsw_ensemble_march.cuh"
+#include "gsw_fast.h"
 #include <mutex>
 
 namespace gsw {
-
-__device__ __forceinline__ FlatPhys<float> member_phys(const GswMember& mb) {
-    FlatPhys<float> ph;
-    ph.inv_dx = mb.inv_dx; ph.inv_dy = mb.inv_dx;
-    ph.half_dx = 0.5f * (1.0f / mb.inv_dx); ph.half_dy = ph.half_dx;
-    ph.g = mb.g; ph.h_min = mb.h_min; ph.h_min_cfl = mb.h_min_cfl; ph.vcap = mb.vcap;
-    ph.linf = mb.linf; ph.quad = mb.quadratic; ph.keep_h = mb.keep_h;
-    ph.rain_kind = mb.rain_kind; ph.rain = mb.rain; ph.ntab = mb.n_tab;
-    ph.ngh = 0; ph.nx = 0; ph.ny = 0; ph.lookup = nullptr; ph.ncol = 0;
-    return ph;
-}
-
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArgs a, FlatMesh<float> m) {
-    if (*a.all_done) return;
-    const int lane = threadIdx.x;
-    const int W = blockDim.y;
-    for (int64_t b = (int64_t)blockIdx.x * W + threadIdx.y; b < a.n_bricks; b += (int64_t)gridDim.x * W) {
-        const int mi = a.brick_member[b];
-        const GswLoopState* st = a.states + mi;
-        if (st->done) continue;                                   // warp-uniform
-        const GswMember& mb = a.members[mi];
-        const FlatPhys<float> ph = member_phys(mb);
-        const float dt = st->dt_f32;
-        const float rate = (mb.rain_kind == GSW_RAIN_UNIFORM) ? mb.rain[st->rain_idx] : 0.0f;
-        unsigned long long lam = flat_brick<float, true>(m, ph, b, dt, rate, nullptr);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long w = __shfl_xor_sync(0xffffffffu, lam, o);
-            lam = w > lam ? w : lam;
-        }
-        if (lane == 0 && lam != 0ull) atomicMax((unsigned long long*)&a.states[mi].lam_bits, lam);
-    }
-    // the last block to arrive evaluates every member's rule for the next step
-    __shared__ int s_last;
-    __syncthreads();
-    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-    if (tid == 0) {
-        __threadfence();
-        const unsigned int ticket = atomicAdd(&a.scratch[0], 1u);
-        s_last = (ticket == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    const int nth = blockDim.x * blockDim.y;
-    __shared__ int s_open;
-    if (tid == 0) s_open = 0;
-    __syncthreads();
-    for (int mi = tid; mi < a.n_members; mi += nth) {
-        GswLoopState* st = a.states + mi;
-        const unsigned long long lb = atomicAdd((unsigned long long*)&st->lam_bits, 0ull);  // coherent read
-        dt_finalize_one(a.members[mi].dt, st, lb);
-        if (!st->done) atomicAdd(&s_open, 1);
-    }
-    __syncthreads();
-    if (tid == 0) {
-        a.scratch[0] = 0u;
-        *a.all_done = (s_open == 0) ? 1 : 0;
-    }
-}
 
 __global__ void ensemble_finalize_kernel(GswEnsembleArgs a) {
     __shared__ int s_open;
@@ -140,20 +73,9 @@ extern "C" int gsw_ensemble_step(const GswEnsembleArgs* a, void* stream) {
     int rc = check_ens(a);
     if (rc) return rc;
     if (!a->qn0 || !a->qn1 || !a->qn2) return set_error(GSW_ERR_INVALID, "ensemble step: null output");
-    const int W = a->warps > 0 ? a->warps : 4;
-    if (W < 1 || W > 8) return set_error(GSW_ERR_INVALID, "ensemble: warps must be in [1, 8]");
-    const int grid = a->grid > 0 ? a->grid : 2 * sm_count();
-    FlatMesh<float> m;
-    m.q0 = a->q0; m.q1 = a->q1; m.q2 = a->q2;
-    m.o0 = a->qn0; m.o1 = a->qn1; m.o2 = a->qn2;
-    m.b = a->bed; m.flags = a->flags; m.ncls = a->n_cls; m.max_h = a->max_h;
-    m.bij = a->brick_ij; m.bnbr = a->brick_nbr; m.nb = a->n_bricks; m.bh = a->brick_h;
-    cudaStream_t st = (cudaStream_t)stream;
-    if (a->min_blocks == 4) ensemble_step_kernel<4><<<grid, dim3(32, W), 0, st>>>(*a, m);
-    else if (a->min_blocks == 5) ensemble_step_kernel<5><<<grid, dim3(32, W), 0, st>>>(*a, m);
-    else if (a->min_blocks == 0) ensemble_step_kernel<1><<<grid, dim3(32, W), 0, st>>>(*a, m);
-    else return set_error(GSW_ERR_INVALID, "ensemble: min_blocks must be 0, 4 or 5");
-    return check_launch("ensemble_step");
+    if (a->arith == GSW_ARITH_FAST) return gsw_fast_ensemble_launch(a, (cudaStream_t)stream);
+    if (a->arith != GSW_ARITH_EXACT) return set_error(GSW_ERR_INVALID, "ensemble step: bad arith %d", a->arith);
+    return launch_ensemble_step(a, (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------------------

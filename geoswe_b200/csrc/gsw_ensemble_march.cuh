@@ -1,0 +1,97 @@
+// gsw_ensemble_march.cuh -- the persistent ensemble step kernel and its launcher.
+//
+// All members' bricks sit in one brick storage. A step is one launch of a persistent
+// grid (a few blocks per SM): warps stride over the global brick list, look up the
+// brick's member, and advance it with that member's dt, rain rate and Manning table
+// (the per-brick march of gsw_flat_brick.cuh). Each member's new wave speed is reduced
+// into its own GswLoopState. The block that finishes last (a ticket counter in scratch
+// memory) then evaluates every member's time-step rule for the next launch, so members
+// keep their own CFL dt with no grid-wide barrier and no host round trip; a member that
+// reaches its end time drops out while the others continue.
+//
+// Included by gsw_ensemble.cu (exact arithmetic) and gsw_fast.cu (fast arithmetic,
+// with namespace gsw renamed).
+#pragma once
+#include "gsw_flat_brick.cuh"
+
+namespace gsw {
+
+__device__ __forceinline__ FlatPhys<float> member_phys(const GswMember& mb) {
+    FlatPhys<float> ph;
+    ph.inv_dx = mb.inv_dx; ph.inv_dy = mb.inv_dx;
+    ph.half_dx = 0.5f * (1.0f / mb.inv_dx); ph.half_dy = ph.half_dx;
+    ph.g = mb.g; ph.h_min = mb.h_min; ph.h_min_cfl = mb.h_min_cfl; ph.vcap = mb.vcap;
+    ph.linf = mb.linf; ph.quad = mb.quadratic; ph.keep_h = mb.keep_h;
+    ph.rain_kind = mb.rain_kind; ph.rain = mb.rain; ph.ntab = mb.n_tab;
+    ph.ngh = 0; ph.nx = 0; ph.ny = 0; ph.lookup = nullptr; ph.ncol = 0;
+    return ph;
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArgs a, FlatMesh<float> m) {
+    if (*a.all_done) return;
+    const int lane = threadIdx.x;
+    const int W = blockDim.y;
+    for (int64_t b = (int64_t)blockIdx.x * W + threadIdx.y; b < a.n_bricks; b += (int64_t)gridDim.x * W) {
+        const int mi = a.brick_member[b];
+        const GswLoopState* st = a.states + mi;
+        if (st->done) continue;                                   // warp-uniform
+        const GswMember& mb = a.members[mi];
+        const FlatPhys<float> ph = member_phys(mb);
+        const float dt = st->dt_f32;
+        const float rate = (mb.rain_kind == GSW_RAIN_UNIFORM) ? mb.rain[st->rain_idx] : 0.0f;
+        unsigned long long lam = flat_brick<float, true>(m, ph, b, dt, rate, nullptr);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long w = __shfl_xor_sync(0xffffffffu, lam, o);
+            lam = w > lam ? w : lam;
+        }
+        if (lane == 0 && lam != 0ull) atomicMax((unsigned long long*)&a.states[mi].lam_bits, lam);
+    }
+    // the last block to arrive evaluates every member's rule for the next step
+    __shared__ int s_last;
+    __syncthreads();
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    if (tid == 0) {
+        __threadfence();
+        const unsigned int ticket = atomicAdd(&a.scratch[0], 1u);
+        s_last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const int nth = blockDim.x * blockDim.y;
+    __shared__ int s_open;
+    if (tid == 0) s_open = 0;
+    __syncthreads();
+    for (int mi = tid; mi < a.n_members; mi += nth) {
+        GswLoopState* st = a.states + mi;
+        const unsigned long long lb = atomicAdd((unsigned long long*)&st->lam_bits, 0ull);  // coherent read
+        dt_finalize_one(a.members[mi].dt, st, lb);
+        if (!st->done) atomicAdd(&s_open, 1);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        a.scratch[0] = 0u;
+        *a.all_done = (s_open == 0) ? 1 : 0;
+    }
+}
+
+// Launch of the step over checked arguments (outputs non-null).
+inline int launch_ensemble_step(const GswEnsembleArgs* a, cudaStream_t st) {
+    const int W = a->warps > 0 ? a->warps : 4;
+    if (W < 1 || W > 8) return set_error(GSW_ERR_INVALID, "ensemble: warps must be in [1, 8]");
+    const int grid = a->grid > 0 ? a->grid : 2 * sm_count();
+    FlatMesh<float> m;
+    m.q0 = a->q0; m.q1 = a->q1; m.q2 = a->q2;
+    m.o0 = a->qn0; m.o1 = a->qn1; m.o2 = a->qn2;
+    m.b = a->bed; m.flags = a->flags; m.ncls = a->n_cls; m.max_h = a->max_h;
+    m.bij = a->brick_ij; m.bnbr = a->brick_nbr; m.nb = a->n_bricks; m.bh = a->brick_h;
+    if (a->min_blocks == 4) ensemble_step_kernel<4><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else if (a->min_blocks == 5) ensemble_step_kernel<5><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else if (a->min_blocks == 0) ensemble_step_kernel<1><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else return set_error(GSW_ERR_INVALID, "ensemble: min_blocks must be 0, 4 or 5");
+    return check_launch("ensemble_step");
+}
+
+}  // namespace gsw

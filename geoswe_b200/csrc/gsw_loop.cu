@@ -9,7 +9,7 @@
 #include <atomic>
 #include <string.h>
 
-namespace gsw {
+namespace gsw_rt {
 
 static thread_local char g_err[512] = "";
 static std::atomic<unsigned long long> g_launches{0};
@@ -43,6 +43,10 @@ int sm_count() {
     }
     return cached;
 }
+
+}  // namespace gsw_rt
+
+namespace gsw {
 
 __global__ void dt_finalize_kernel(GswDtParams p, GswLoopState* s) { dt_finalize_one(p, s, s->lam_bits); }
 // The same with the parameters read from device memory: a captured launch then follows
@@ -97,6 +101,6 @@ extern "C" int gsw_loop_commit(GswLoopState* state, void* stream) {
     return check_launch("loop_commit");
 }
 
-extern "C" const char* gsw_last_error(void) { return g_err; }
+extern "C" const char* gsw_last_error(void) { return gsw_rt::g_err; }
 extern "C" uint32_t gsw_abi_version(void) { return GSW_ABI_VERSION; }
-extern "C" uint64_t gsw_launch_count(void) { return (uint64_t)g_launches.load(); }
+extern "C" uint64_t gsw_launch_count(void) { return (uint64_t)gsw_rt::g_launches.load(); }

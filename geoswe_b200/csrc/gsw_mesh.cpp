@@ -26,8 +26,8 @@
 #include <algorithm>
 #include "../../include/gsw.h"
 
-namespace gsw { int set_error(int code, const char* fmt, ...); }
-using gsw::set_error;
+namespace gsw_rt { int set_error(int code, const char* fmt, ...); }
+using gsw_rt::set_error;
 
 namespace {
 

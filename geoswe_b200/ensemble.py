@@ -38,6 +38,10 @@ class Ensemble:
         bh = {m.brick_h for m in members}
         if len(bh) != 1:
             raise ValueError(f"Ensemble: members must share brick_h (got {sorted(bh)})")
+        ar = {m.arith for m in members}
+        if len(ar) != 1:
+            raise ValueError("Ensemble: members must share their arithmetic (all 'exact' or all 'fast')")
+        self.arith = ar.pop()
         _protos()
         self.members = list(members)
         self.brick_h = bh.pop()
@@ -117,6 +121,7 @@ class Ensemble:
         a.abi_version = L.ABI_VERSION
         a.brick_h, a.n_bricks, a.n_members = self.brick_h, self.n_bricks, len(self.members)
         a.warps, a.grid, a.min_blocks = self.warps, self.grid, self.min_blocks
+        a.arith = self.arith
         a.brick_ij, a.brick_nbr, a.brick_member = _ptr(self._bij), _ptr(self._bnbr), _ptr(self._bmem)
         a.flags, a.n_cls = _ptr(self._flags), _ptr(self._ncls)
         a.q0, a.q1, a.q2 = _ptr(src[0]), _ptr(src[1]), _ptr(src[2])

@@ -120,10 +120,11 @@ class Solver2D:
         self.code = L.F32 if self.np_dtype == np.float32 else L.F64
         self.nxp, self.nyp = mesh.padded_shape
         self.pitch = _pitch(self.nyp, self.np_dtype.itemsize)
+        self.arith = L.ARITH_FAST if cfg.arith == "fast" else L.ARITH_EXACT
         self._tile_rows, self._warps, self._min_blocks = int(tile_rows), int(warps), int(min_blocks)
         if autotuned and not (tile_rows or warps or min_blocks):
             from . import autotune
-            best = autotune.load("dense", mesh.nx * mesh.ny)
+            best = autotune.load(autotune.kind("dense", self.arith), mesh.nx * mesh.ny)
             if best and self.np_dtype == np.float32:
                 self._tile_rows, self._warps = int(best["tile_rows"]), int(best["warps"])
                 self._min_blocks = int(best["min_blocks"])
@@ -447,6 +448,7 @@ class Solver2D:
         a.g, a.h_min = cfg.g, cfg.h_min
         a.h_cfl = self._h_cfl()
         a.tile_rows, a.warps, a.min_blocks = self._tile_rows, self._warps, self._min_blocks
+        a.arith = self.arith
         if step:
             T = T or self._tables()
             a.state = _ptr(self._state)

@@ -67,6 +67,15 @@ extern "C" {
 #define GSW_RAIN_GRIDDED  2    /* rain + frame*nx*ny is an interior (nx, ny) frame (m/s) */
 #define GSW_RAIN_LOOKUP   3    /* flat: rate_table[frame*ncol + lookup[cell]] */
 
+/* step arithmetic (the `arith` field of the step argument structs)
+ *   EXACT: separately rounded IEEE operations in the reference kernel's operand order;
+ *          bit-identical to the reference kernel text compiled without FMA contraction.
+ *   FAST:  binary32 only; FMA contraction, flush-to-zero, approximate square root and
+ *          division. Held to a depth tolerance against EXACT (stated by the tests and
+ *          the benchmark), not to bit equality. */
+#define GSW_ARITH_EXACT 0
+#define GSW_ARITH_FAST  1
+
 /* friction kinds */
 #define GSW_FRICTION_NONE  0
 #define GSW_FRICTION_TABLE 1   /* n = n_tab[n_cls[cell]] */
@@ -159,7 +168,7 @@ typedef struct GswDenseArgs {
     int32_t  tile_rows;        /* rows per warp strip (0: default 32) */
     int32_t  warps;            /* warps per block (0: default 4) */
     int32_t  min_blocks;       /* register cap: 0 (compiler's choice), 4 (64 regs) or 5 (51 regs) */
-    int32_t  reserved;
+    int32_t  arith;            /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST (GSW_F32 step only) */
 } GswDenseArgs;
 
 /* One fused step over the interior: SRM-HLLC residual, rain, forward Euler,
@@ -252,7 +261,7 @@ typedef struct GswFlatArgs {
     int32_t  brick_h;          /* rows per brick (>= 2) */
     int32_t  warps;            /* warps per block (0: 4) */
     int32_t  min_blocks;       /* fp32 step register cap: 0 (compiler's choice), 4 (64 regs) or 5 (48 regs) */
-    int32_t  reserved1;
+    int32_t  arith;            /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST (GSW_F32 step only) */
     int64_t  n_bricks;         /* brick n_bricks is the all-zero brick (a missing neighbour) */
     const int32_t* brick_ij;   /* (n_bricks, 2) brick row, brick column */
     const int32_t* brick_nbr;  /* (n_bricks, 4) up, down, left, right */
@@ -452,6 +461,8 @@ typedef struct GswEnsembleArgs {
     int32_t  warps;              /* warps per block (0: 4) */
     int32_t  grid;               /* persistent blocks (0: 2 per SM) */
     int32_t  min_blocks;         /* register cap: 0 (compiler's choice), 4 (64 regs) or 5 (48 regs) */
+    int32_t  arith;              /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST */
+    int32_t  reserved0;
     const int32_t* brick_ij;     /* (n_bricks, 2) */
     const int32_t* brick_nbr;    /* (n_bricks, 4) global brick ids */
     const int32_t* brick_member; /* (n_bricks) */

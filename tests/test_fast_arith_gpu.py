@@ -1,0 +1,134 @@
+"""The opt-in fast arithmetic (Config(arith="fast"): FMA contraction, approximate binary32
+square root and division, compiled separately in gsw_fast.cu) against the exact step.
+
+Fast results are not bit-identical to the reference's, so they are held to stated
+tolerances instead:
+  * residual at a fixed state: max |r_fast - r_exact| <= 2e-6 * max |r_exact| per field;
+  * runs: the same step count as the exact run; on the compressed mesh depth RMSE
+    <= 1e-5 m and max <= 1e-4 m against the exact run; on the dense dry-start
+    rain-on-terrain run (where binary32 itself drifts from binary64 by millimetres)
+    the fast run's depth error against the binary64 run is at most 1.25 x the exact
+    binary32 run's, in RMSE and in max;
+  * the fast ensemble equals its members run one by one with fast arithmetic (step
+    counts equal, depth within 1e-6 m).
+"""
+import warnings
+
+import numpy as np
+import pytest
+
+from tests._cases import flowing
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _rmse(a, b):
+    return float(np.sqrt(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2)))
+
+
+def _dense(q0, bed, arith, dtype="float32", dx=2.0, **kw):
+    from geoswe_b200 import Config, Mesh2D, Solver2D
+    nx, ny = bed.shape
+    c = dict(bc_x="wall", bc_y="wall", dtype=dtype, h_min=1e-6, arith=arith)
+    c.update(kw)
+    return Solver2D(Mesh2D(nx=nx, ny=ny, dx=dx, dy=dx, ngh=2), Config(**c), q0, bed)
+
+
+def test_fast_residual_close_to_exact():
+    q0, bed = flowing(70, 97, seed=11, dtype=np.float32)
+    r = {}
+    for ar in ("exact", "fast"):
+        s = _dense(q0, bed, ar)
+        s.apply_bc()
+        r[ar] = s.residual().cpu().numpy()[:, 2:-2, 2:-2]
+    for c in range(3):
+        scale = np.abs(r["exact"][c]).max()
+        assert scale > 0
+        assert np.abs(r["fast"][c] - r["exact"][c]).max() <= 2e-6 * scale, c
+
+
+def _rain_on_terrain(arith, dtype):
+    from geoswe_b200 import RainfallForcing
+    from geoswe_b200.synthetic import fractal_bed, voronoi_classes
+    nx, ny, dx = 80, 100, 3.0
+    z = fractal_bed(nx, ny, dx, seed=4)
+    cls = voronoi_classes(nx, ny, n_seeds=16, seed=4)
+    s = _dense(np.zeros((3, nx, ny)), z, arith, dtype=dtype, dx=dx, bc={"x+": "fall"}, friction="manning",
+               rainfall_forcing=RainfallForcing(time_s=[0.0, 1e9], rate_mm_h=[50.0, 50.0]))
+    s.set_manning(np.array([0.025, 0.04, 0.06, 0.1])[cls])
+    n = s.run(t_end=3000.0)
+    return n, s.t, np.asarray(s.depth(), np.float64)
+
+
+def test_fast_dense_run_error_vs_fp64_no_worse_than_exact():
+    n_e, t_e, h_e = _rain_on_terrain("exact", "float32")
+    n_f, t_f, h_f = _rain_on_terrain("fast", "float32")
+    n_64, _, h_64 = _rain_on_terrain("exact", "float64")
+    assert n_f == n_e == n_64 and t_f == t_e == 3000.0
+    assert _rmse(h_f, h_64) <= 1.25 * _rmse(h_e, h_64)
+    assert np.abs(h_f - h_64).max() <= 1.25 * np.abs(h_e - h_64).max()
+
+
+def _flat(arith, seed=6):
+    from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
+    from geoswe_b200.compressed import CompressedSolver
+    from geoswe_b200.synthetic import MANNING_CLASSES, fractal_bed, voronoi_classes
+    nx, ny, dx = 72, 90, 3.0
+    z = fractal_bed(nx, ny, dx, seed=seed).astype(np.float32)
+    mask = z < np.percentile(z, 60)
+    mask[:3, :] = mask[-3:, :] = False
+    mask[:, :3] = mask[:, -3:] = False
+    cls = voronoi_classes(nx, ny, n_seeds=16, seed=seed)
+    s = Solver2D(Mesh2D(nx=nx, ny=ny, dx=dx, dy=dx, ngh=2),
+                 Config(bc_x="fall", bc_y="fall", friction="manning", arith=arith),
+                 np.zeros((3, nx, ny), np.float32), z)
+    s.set_inside_mask(mask)
+    s.set_manning_table(np.pad(cls, 2, mode="edge"), MANNING_CLASSES)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        cs = CompressedSolver.from_dense(s)
+    cs.set_rain(RainfallForcing(time_s=[0.0, 600.0, 1e9], rate_mm_h=[50.0, 20.0, 20.0]))
+    return cs
+
+
+def test_fast_flat_run_close_to_exact():
+    runs = {}
+    for ar in ("exact", "fast"):
+        cs = _flat(ar)
+        n = cs.run(t_end=1500.0)
+        runs[ar] = (n, cs.t, cs.depth())
+    assert runs["fast"][0] == runs["exact"][0] > 10
+    assert runs["fast"][1] == runs["exact"][1] == 1500.0
+    he, hf = runs["exact"][2], runs["fast"][2]
+    assert he.max() > 0.1
+    assert _rmse(hf, he) <= 1e-5
+    assert np.abs(hf.astype(np.float64) - he).max() <= 1e-4
+
+
+def test_fast_ensemble_matches_fast_members():
+    from geoswe_b200.ensemble import Ensemble
+    seeds = (6, 7, 8)
+    alone = []
+    for sd in seeds:
+        cs = _flat("fast", seed=sd)
+        n = cs.run(t_end=900.0)
+        alone.append((n, cs.depth()))
+    ens = Ensemble([_flat("fast", seed=sd) for sd in seeds])
+    steps = ens.run(t_end=900.0)
+    for k in range(len(seeds)):
+        assert steps[k] == alone[k][0]
+        assert np.abs(ens.depth(k).astype(np.float64) - alone[k][1]).max() <= 1e-6
+
+
+def test_fast_refusals():
+    from geoswe_b200 import Config
+    from geoswe_b200.adjoint import FlatAdjoint
+    with pytest.raises(ValueError):
+        Config(arith="fast", dtype="float64")
+    with pytest.raises(ValueError):
+        Config(arith="approximate")
+    cs = _flat("fast")
+    act = np.nonzero(cs.is_active != 0)[0]
+    with pytest.raises(ValueError):
+        FlatAdjoint(cs, gauges=[int(act[0])], n_steps=4, window=2)
