@@ -157,9 +157,12 @@ def measure_dense(args, z, cls, n, world, arith="exact"):
     kernel alone (CUDA events, same launch shape) for the roofline."""
     import torch
     s = make_solver(z, cls, n, arith=arith)
+    forced = args.fast_shape if arith == "fast" else args.exact_shape
+    if forced:
+        s._tile_rows, s._warps, s._min_blocks = (int(v) for v in forced.split(","))
     s.run(t_end=1e12, max_steps=args.warmup)
     tune = None
-    if not args.no_tune:
+    if not forced and not args.no_tune:
         from geoswe_b200 import autotune
         best, table = autotune.tune_dense(s, reps=4)
         s._tile_rows, s._warps, s._min_blocks = best["tile_rows"], best["warps"], best["min_blocks"]
@@ -591,6 +594,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fast", action="store_true", help="skip the fast-arithmetic measurement")
+    ap.add_argument("--exact-shape", default="", help="dense launch shape 'tile_rows,warps,min_blocks' (no tuning)")
+    ap.add_argument("--fast-shape", default="", help="the same for the fast arithmetic")
     ap.add_argument("--err-n", type=int, default=96, help="fp64 depth-error sample size (0: skip)")
     ap.add_argument("--err-t-end", type=float, default=600.0)
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")

@@ -21,7 +21,7 @@ import torch
 
 from . import _lib as L
 
-DENSE_SPACE = dict(tile_rows=(16, 32, 64), warps=(2, 4, 8), min_blocks=(0, 4, 5))
+DENSE_SPACE = dict(tile_rows=(16, 32, 64), warps=(2, 4, 8), min_blocks=(0, 3, 4, 5))
 
 
 def _cache_path() -> Path:
@@ -125,8 +125,8 @@ def tune_dense(s, reps=8, space=None, store=True, verbose=False):
     return best, table
 
 
-ENSEMBLE_SPACE = dict(warps=(4, 8), blocks_per_sm=(1, 2, 4, 8), min_blocks=(0, 4, 5))
-FLAT_SPACE = dict(warps=(2, 4, 8), min_blocks=(0, 4, 5))
+ENSEMBLE_SPACE = dict(warps=(4, 8), blocks_per_sm=(1, 2, 4, 8), min_blocks=(0, 3, 4, 5))
+FLAT_SPACE = dict(warps=(2, 4, 8), min_blocks=(0, 3, 4, 5))
 
 
 def tune_ensemble(ens, t_end, reps=6, space=None, store=True, verbose=False):

@@ -256,16 +256,19 @@ inline int launch_march(const GswDenseArgs* a, cudaStream_t s) {
     if (rc) return rc;
     const int W = a->warps > 0 ? a->warps : 4;
     const int minb = a->min_blocks;
-    if (minb != 0 && minb != 4 && minb != 5) return set_error(GSW_ERR_INVALID, "dense: min_blocks must be 0, 4 or 5");
+    if (minb != 0 && (minb < 3 || minb > 5)) return set_error(GSW_ERR_INVALID, "dense: min_blocks must be 0, 3, 4 or 5");
     if (W < 1 || W > 8) return set_error(GSW_ERR_INVALID, "dense: warps must be in [1, 8]");
     const int ncols = k.nyp - 2 * k.lo, nrows = k.nxp - 2 * k.lo;
     const int strips = (ncols + 29) / 30;
     dim3 block(32, W);
     dim3 grid((strips + W - 1) / W, (nrows + k.tile_rows - 1) / k.tile_rows);
     if (grid.y > 65535u) return set_error(GSW_ERR_INVALID, "dense: too many row tiles (%u); raise tile_rows", grid.y);
-    if (minb == 0) dense_march_kernel<T, STEP, 1><<<grid, block, 0, s>>>(k);
-    else if (minb == 4) dense_march_kernel<T, STEP, 4><<<grid, block, 0, s>>>(k);
-    else dense_march_kernel<T, STEP, 5><<<grid, block, 0, s>>>(k);
+    // register caps apply to the binary32 step; the residual and binary64 use the compiler's choice
+    constexpr bool capped = STEP && sizeof(T) == 4;
+    if (capped && minb == 3) dense_march_kernel<T, STEP, capped ? 3 : 1><<<grid, block, 0, s>>>(k);
+    else if (capped && minb == 4) dense_march_kernel<T, STEP, capped ? 4 : 1><<<grid, block, 0, s>>>(k);
+    else if (capped && minb == 5) dense_march_kernel<T, STEP, capped ? 5 : 1><<<grid, block, 0, s>>>(k);
+    else dense_march_kernel<T, STEP, 1><<<grid, block, 0, s>>>(k);
     return check_launch("dense_march");
 }
 

@@ -87,10 +87,11 @@ inline int launch_ensemble_step(const GswEnsembleArgs* a, cudaStream_t st) {
     m.o0 = a->qn0; m.o1 = a->qn1; m.o2 = a->qn2;
     m.b = a->bed; m.flags = a->flags; m.ncls = a->n_cls; m.max_h = a->max_h;
     m.bij = a->brick_ij; m.bnbr = a->brick_nbr; m.nb = a->n_bricks; m.bh = a->brick_h;
-    if (a->min_blocks == 4) ensemble_step_kernel<4><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    if (a->min_blocks == 3) ensemble_step_kernel<3><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else if (a->min_blocks == 4) ensemble_step_kernel<4><<<grid, dim3(32, W), 0, st>>>(*a, m);
     else if (a->min_blocks == 5) ensemble_step_kernel<5><<<grid, dim3(32, W), 0, st>>>(*a, m);
     else if (a->min_blocks == 0) ensemble_step_kernel<1><<<grid, dim3(32, W), 0, st>>>(*a, m);
-    else return set_error(GSW_ERR_INVALID, "ensemble: min_blocks must be 0, 4 or 5");
+    else return set_error(GSW_ERR_INVALID, "ensemble: min_blocks must be 0, 3, 4 or 5");
     return check_launch("ensemble_step");
 }
 

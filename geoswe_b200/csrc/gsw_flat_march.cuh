@@ -74,9 +74,11 @@ inline int launch_flat(const GswFlatArgs* a, cudaStream_t s) {
     const int64_t blocks = (k.m.nb + W - 1) / W;
     if (blocks > 0x7fffffffLL) return set_error(GSW_ERR_INVALID, "flat: too many bricks");
     const int mb = a->min_blocks;
-    if (mb != 0 && mb != 4 && mb != 5) return set_error(GSW_ERR_INVALID, "flat: min_blocks must be 0, 4 or 5");
-    if (STEP && sizeof(T) == 4 && mb == 4) flat_march_kernel<T, STEP, 4><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
-    else if (STEP && sizeof(T) == 4 && mb == 5) flat_march_kernel<T, STEP, 5><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
+    if (mb != 0 && (mb < 3 || mb > 5)) return set_error(GSW_ERR_INVALID, "flat: min_blocks must be 0, 3, 4 or 5");
+    constexpr bool capped = STEP && sizeof(T) == 4;   // register caps apply to the binary32 step
+    if (capped && mb == 3) flat_march_kernel<T, STEP, capped ? 3 : 1><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
+    else if (capped && mb == 4) flat_march_kernel<T, STEP, capped ? 4 : 1><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
+    else if (capped && mb == 5) flat_march_kernel<T, STEP, capped ? 5 : 1><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
     else flat_march_kernel<T, STEP, 1><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
     return check_launch("flat_march");
 }

@@ -167,7 +167,7 @@ typedef struct GswDenseArgs {
     double   h_cfl;            /* wave-speed wet threshold (and divisor) */
     int32_t  tile_rows;        /* rows per warp strip (0: default 32) */
     int32_t  warps;            /* warps per block (0: default 4) */
-    int32_t  min_blocks;       /* register cap: 0 (compiler's choice), 4 (64 regs) or 5 (51 regs) */
+    int32_t  min_blocks;       /* register cap: 0 (compiler's choice), 3 (80 regs), 4 (64 regs) or 5 (48 regs) */
     int32_t  arith;            /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST (GSW_F32 step only) */
 } GswDenseArgs;
 
@@ -260,7 +260,7 @@ typedef struct GswFlatArgs {
     int32_t  dtype;            /* GSW_F32 or GSW_F64: q*, qn*, bed, rain, n_tab and max_h */
     int32_t  brick_h;          /* rows per brick (>= 2) */
     int32_t  warps;            /* warps per block (0: 4) */
-    int32_t  min_blocks;       /* fp32 step register cap: 0 (compiler's choice), 4 (64 regs) or 5 (48 regs) */
+    int32_t  min_blocks;       /* fp32 step register cap: 0 (compiler's choice), 3 (80 regs), 4 (64 regs) or 5 (48 regs) */
     int32_t  arith;            /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST (GSW_F32 step only) */
     int64_t  n_bricks;         /* brick n_bricks is the all-zero brick (a missing neighbour) */
     const int32_t* brick_ij;   /* (n_bricks, 2) brick row, brick column */
@@ -460,7 +460,7 @@ typedef struct GswEnsembleArgs {
     int32_t  n_members;
     int32_t  warps;              /* warps per block (0: 4) */
     int32_t  grid;               /* persistent blocks (0: 2 per SM) */
-    int32_t  min_blocks;         /* register cap: 0 (compiler's choice), 4 (64 regs) or 5 (48 regs) */
+    int32_t  min_blocks;         /* register cap: 0 (compiler's choice), 3 (80 regs), 4 (64 regs) or 5 (48 regs) */
     int32_t  arith;              /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST */
     int32_t  reserved0;
     const int32_t* brick_ij;     /* (n_bricks, 2) */
