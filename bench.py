@@ -276,7 +276,7 @@ def run_e2e(args, z, cls, n):
             "what": "Solver2D(host arrays) + run(steps) + depth(); bytes per step = total / steps"}
 
 
-def build_member(spec, brick_h=16, device="cuda"):
+def build_member(spec, brick_h=16, device="cuda", arith="exact"):
     """One member of the uneven ensemble as a CompressedSolver (inputs generated on the GPU)."""
     import torch
     from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
@@ -290,7 +290,8 @@ def build_member(spec, brick_h=16, device="cuda"):
     mask[:3, :] = mask[-3:, :] = False
     mask[:, :3] = mask[:, -3:] = False
     cls = voronoi_classes_device(nx, ny, seed=spec["seed"], device=device).cpu().numpy()
-    s = Solver2D(Mesh2D(nx=nx, ny=ny, dx=3.0, dy=3.0, ngh=2), Config(bc_x="fall", bc_y="fall", friction="manning"),
+    s = Solver2D(Mesh2D(nx=nx, ny=ny, dx=3.0, dy=3.0, ngh=2),
+                 Config(bc_x="fall", bc_y="fall", friction="manning", arith=arith),
                  np.zeros((3, nx, ny), np.float32), z.cpu().numpy(), track_max_depth=False)
     s.set_inside_mask(mask)
     s.set_manning_table(np.pad(cls, 2, mode="edge"), MANNING_CLASSES * spec["scale"])
@@ -314,11 +315,12 @@ def run_ensemble(args):
     t_end = args.ens_t_end
     # warm-up: context, library and capture paths on the smallest member
     small = min(specs, key=lambda sp: sp["nx"] * sp["ny"])
-    build_member(small).run(t_end=t_end, max_steps=max(args.warmup, 3))
-    Ensemble([build_member(small), build_member(small)]).run(t_end=t_end, max_steps=max(args.warmup, 3), window=8)
+    build_member(small, arith=args.arith).run(t_end=t_end, max_steps=max(args.warmup, 3))
+    Ensemble([build_member(small, arith=args.arith), build_member(small, arith=args.arith)]).run(
+        t_end=t_end, max_steps=max(args.warmup, 3), window=8)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    loop_members = [build_member(sp) for sp in specs]
+    loop_members = [build_member(sp, arith=args.arith) for sp in specs]
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
     loop_shape = None
@@ -326,7 +328,7 @@ def run_ensemble(args):
         big = max(loop_members, key=lambda m: m.nslots)
         best, _ = autotune.tune_flat(big, store=False)
         for m in loop_members:
-            m.warps, m.min_blocks = best["warps"], best["min_blocks"]
+            m.warps, m.min_blocks, m.segments = best["warps"], best["min_blocks"], best["segments"]
         loop_shape = best
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -338,7 +340,7 @@ def run_ensemble(args):
     work = sum(m.N_active * n for m, n in zip(loop_members, steps_loop))
     del loop_members
     torch.cuda.empty_cache()
-    ens = Ensemble([build_member(sp) for sp in specs], warps=args.ens_warps, grid=args.ens_grid)
+    ens = Ensemble([build_member(sp, arith=args.arith) for sp in specs], warps=args.ens_warps, grid=args.ens_grid)
     tune = None
     if not args.no_tune and args.ens_warps == 0 and args.ens_grid == 0:
         best, table = autotune.tune_ensemble(ens, t_end)
@@ -360,8 +362,9 @@ def run_ensemble(args):
            "identical_steps_to_plain": bool(steps_ens == steps_loop),
            "gpu_launches": int(ens.kernel_launches - n0), "gpu_launches_plain_loop": loop_launches,
            "schedule": {"warps": ens.warps or 4, "grid": ens.grid, "min_blocks": ens.min_blocks,
+                        "segments": ens.segments or 1,
                         "brick_h": ens.brick_h}, "autotune": tune, "plain_loop_shape": loop_shape,
-           "build_s": build_s, "dtype": "f32", "data": "synthetic"}
+           "build_s": build_s, "dtype": "f32", "arith": args.arith, "data": "synthetic"}
     return out
 
 
@@ -469,7 +472,7 @@ def run_tidal(args):
     zh = z.cpu().numpy()
     del h, z, x, y
     torch.cuda.empty_cache()
-    cfg = Config(bc_x="wall", bc_y="wall", friction="manning", manning_n=0.03, cfl=0.5)
+    cfg = Config(bc_x="wall", bc_y="wall", friction="manning", manning_n=0.03, cfl=0.5, arith=args.arith)
     s = Solver2D(Mesh2D(nx=nx, ny=ny, dx=dx, dy=dx, ngh=2), cfg, q0, zh, track_max_depth=False)
     del q0, zh
     s.apply_bc()
@@ -512,7 +515,7 @@ def run_tidal(args):
     stored_bytes = 29.0 * cs.nslots                      # q in + bed + flag + q out per slot
     return {"metric": METRIC + " [compressed, everywhere wet]", "value": cells * steps / (ms / 1e3), "unit": UNIT,
             "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
-            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "higher_is_better": True, "dtype": "f32", "arith": args.arith, "data": "synthetic",
             "config": {"workload": f"tidal everywhere-wet compressed {nx}x{ny}, dx=1 m, sinusoidal bed, "
                                    f"n=0.03, tidal stage on the x- ring, CFL 0.5, fp32",
                        "active_cells": cells, "stored_slots": int(cs.nslots), "bricks": int(cs.n_bricks),
@@ -524,7 +527,8 @@ def run_tidal(args):
                          "kernel_ms": kern_ms, "bytes_per_cell": 38, "peak_source": peak_kind,
                          "brick_bytes_GBs": stored_bytes / (kern_ms / 1e3) / 1e9},
             "gpu_launches": int(launches), "clocks": clocks, "build_s": build_s, "simulated_s": cs.t,
-            "launch_shape": {"warps": cs.warps or 4, "min_blocks": cs.min_blocks}, "autotune": tune}
+            "launch_shape": {"warps": cs.warps or 4, "min_blocks": cs.min_blocks, "segments": cs.segments or 1},
+            "autotune": tune}
 
 
 def cpu_baseline(args):
@@ -594,6 +598,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fast", action="store_true", help="skip the fast-arithmetic measurement")
+    ap.add_argument("--arith", default="exact", choices=["exact", "fast"],
+                    help="step arithmetic of the tidal and ensemble cases")
     ap.add_argument("--exact-shape", default="", help="dense launch shape 'tile_rows,warps,min_blocks' (no tuning)")
     ap.add_argument("--fast-shape", default="", help="the same for the fast arithmetic")
     ap.add_argument("--err-n", type=int, default=96, help="fp64 depth-error sample size (0: skip)")

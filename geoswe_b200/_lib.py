@@ -86,7 +86,7 @@ class GswFlatArgs(C.Structure):
                 ("linf", i32), ("rain_kind", i32), ("state", vp), ("lam_target", vp), ("rain", vp),
                 ("ngh", i32), ("nx", i32), ("ny", i32), ("n_tab_len", i32), ("n_cls", vp), ("n_tab", vp),
                 ("vcap", f64), ("quadratic", i32), ("keep_h", i32), ("max_h", vp), ("rain_lookup", vp),
-                ("rain_ncol", i32), ("reserved2", i32)]
+                ("rain_ncol", i32), ("segments", i32)]
 
 
 class GswFlatInflowArgs(C.Structure):
@@ -130,11 +130,11 @@ class GswMember(C.Structure):
 
 class GswEnsembleArgs(C.Structure):
     _fields_ = [("abi_version", u32), ("brick_h", i32), ("n_bricks", i64), ("n_members", i32),
-                ("warps", i32), ("grid", i32), ("min_blocks", i32), ("arith", i32), ("reserved0", i32),
+                ("warps", i32), ("grid", i32), ("min_blocks", i32), ("arith", i32), ("segments", i32),
                 ("brick_ij", vp), ("brick_nbr", vp),
                 ("brick_member", vp), ("flags", vp), ("n_cls", vp), ("q0", vp), ("q1", vp), ("q2", vp),
                 ("qn0", vp), ("qn1", vp), ("qn2", vp), ("bed", vp), ("max_h", vp), ("members", vp),
-                ("states", vp), ("scratch", vp), ("all_done", vp)]
+                ("states", vp), ("scratch", vp), ("all_done", vp), ("member_brick_off", vp), ("run", vp)]
 
 
 # entry point -> argtypes

@@ -252,6 +252,7 @@ class FlatAdjoint:
         a.n_cls, a.n_tab, a.n_tab_len = _ptr(cs._ncls), _ptr(self._ntab), self.n_classes
         a.vcap, a.quadratic, a.keep_h = cs.vcap, int(cs.quad), int(cs.keep_h)
         a.warps, a.min_blocks = cs.warps, (cs.min_blocks if self.code == L.F32 else 0)
+        a.segments = cs.segments
         return a
 
     def _inflow_args(self, q):

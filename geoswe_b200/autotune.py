@@ -125,8 +125,8 @@ def tune_dense(s, reps=8, space=None, store=True, verbose=False):
     return best, table
 
 
-ENSEMBLE_SPACE = dict(warps=(4, 8), blocks_per_sm=(1, 2, 4, 8), min_blocks=(0, 3, 4, 5))
-FLAT_SPACE = dict(warps=(2, 4, 8), min_blocks=(0, 3, 4, 5))
+ENSEMBLE_SPACE = dict(warps=(4, 8), blocks_per_sm=(2, 4, 8), min_blocks=(0, 3, 4), segments=(0, 1))
+FLAT_SPACE = dict(warps=(2, 4, 8), min_blocks=(0, 3, 4, 5), segments=(0, 1, 2, 4))
 
 
 def tune_ensemble(ens, t_end, reps=6, space=None, store=True, verbose=False):
@@ -136,22 +136,25 @@ def tune_ensemble(ens, t_end, reps=6, space=None, store=True, verbose=False):
     space = space or ENSEMBLE_SPACE
     sms = torch.cuda.get_device_properties(ens.device).multi_processor_count
     table = []
-    for w, bps, mb in itertools.product(space["warps"], space["blocks_per_sm"], space.get("min_blocks", (0,))):
-        ms = ens.time_step(t_end, warps=w, grid=bps * sms, min_blocks=mb, reps=reps)
-        table.append(dict(warps=w, blocks_per_sm=bps, grid=bps * sms, min_blocks=mb, ms=ms))
+    segs = [g for g in space.get("segments", (1,)) if g == 0 or ens.brick_h % g == 0]
+    for w, bps, mb, g in itertools.product(space["warps"], space["blocks_per_sm"], space.get("min_blocks", (0,)),
+                                           segs):
+        ms = ens.time_step(t_end, warps=w, grid=bps * sms, min_blocks=mb, segments=g, reps=reps)
+        table.append(dict(warps=w, blocks_per_sm=bps, grid=bps * sms, min_blocks=mb, segments=g, ms=ms))
         if verbose:
-            print(f"  warps={w} blocks/SM={bps} min_blocks={mb}: {ms:.4f} ms", flush=True)
+            print(f"  warps={w} blocks/SM={bps} min_blocks={mb} segments={g}: {ms:.4f} ms", flush=True)
     best = min(table, key=lambda e: e["ms"])
     ens.warps, ens.grid, ens.min_blocks = best["warps"], best["grid"], best["min_blocks"]
+    ens.segments = best["segments"]
     if store:
         _store(kind("ensemble", ens.arith), ens.nslots, best)
     return best, table
 
 
-def time_flat_step(cs, reps=10, dt=None, warps=None, min_blocks=None):
+def time_flat_step(cs, reps=10, dt=None, warps=None, min_blocks=None, segments=None):
     """Mean duration (ms) of one fused flat-step launch of compressed solver `cs` on
     scratch copies of its state (the solver is not advanced), with the solver's own
-    launch shape unless `warps` / `min_blocks` are given."""
+    launch shape unless `warps` / `min_blocks` / `segments` are given."""
     from .solver import _ptr, _stream
     if dt is None:
         dt = getattr(cs, "last_dt", None) or 0.01
@@ -172,6 +175,8 @@ def time_flat_step(cs, reps=10, dt=None, warps=None, min_blocks=None):
             a.warps = int(warps)
         if min_blocks is not None:
             a.min_blocks = int(min_blocks)
+        if segments is not None:
+            a.segments = int(segments)
         args.append(a)
     for k in range(2):
         L.call("gsw_flat_step", C.byref(args[k % 2]), _stream())
@@ -186,17 +191,19 @@ def time_flat_step(cs, reps=10, dt=None, warps=None, min_blocks=None):
 
 
 def tune_flat(cs, reps=6, space=None, store=True, verbose=False):
-    """Time the fused flat step for every (warps, register cap) of `space` on scratch
-    copies of `cs`'s state; set the winner on `cs` and cache it. Returns (best, table)."""
+    """Time the fused flat step for every (warps, register cap, row segments per brick)
+    of `space` on scratch copies of `cs`'s state; set the winner on `cs` and cache it.
+    Returns (best, table)."""
     space = space or FLAT_SPACE
     table = []
-    for w, mb in itertools.product(space["warps"], space["min_blocks"]):
-        ms = time_flat_step(cs, reps=reps, warps=w, min_blocks=mb)
-        table.append(dict(warps=w, min_blocks=mb, ms=ms))
+    segs = [g for g in space.get("segments", (1,)) if g == 0 or cs.brick_h % g == 0]
+    for w, mb, g in itertools.product(space["warps"], space["min_blocks"], segs):
+        ms = time_flat_step(cs, reps=reps, warps=w, min_blocks=mb, segments=g)
+        table.append(dict(warps=w, min_blocks=mb, segments=g, ms=ms))
         if verbose:
-            print(f"  warps={w} min_blocks={mb}: {ms:.4f} ms", flush=True)
+            print(f"  warps={w} min_blocks={mb} segments={g}: {ms:.4f} ms", flush=True)
     best = min(table, key=lambda e: e["ms"])
-    cs.warps, cs.min_blocks = best["warps"], best["min_blocks"]
+    cs.warps, cs.min_blocks, cs.segments = best["warps"], best["min_blocks"], best["segments"]
     cs._graph_cache.clear()
     if store:
         _store(kind("flat", cs.arith), cs.nslots, best)

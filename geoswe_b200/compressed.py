@@ -342,11 +342,13 @@ class CompressedSolver:
         self._inflows = []
         self._ring = None
         self._forcing = {}
-        self.warps, self.min_blocks = 0, 0
+        self.warps, self.min_blocks, self.segments = 0, 0, 0
         from . import autotune
         best = autotune.load(autotune.kind("flat", self.arith), self.nslots)
         if best:
             self.warps, self.min_blocks = int(best["warps"]), int(best["min_blocks"])
+            g = int(best.get("segments", 0))
+            self.segments = g if g == 0 or self.brick_h % g == 0 else 0
         self._graph_cache = {}
         self._dtp_dev = None
         self.t = 0.0
@@ -679,7 +681,7 @@ class CompressedSolver:
         a.g, a.h_min, a.h_min_cfl = self.g, self.h_min, self.h_min_cfl
         a.linf = int(self.cfl_linf)
         a.ngh, a.nx, a.ny = self.ngh, self.nx, self.ny
-        a.warps, a.min_blocks = self.warps, self.min_blocks
+        a.warps, a.min_blocks, a.segments = self.warps, self.min_blocks, self.segments
         a.arith = self.arith
         if step:
             a.state = _ptr(self._state)
@@ -814,7 +816,7 @@ class CompressedSolver:
             # one step outside the window, so every captured window starts on buffer 0
             one_step(1)
             self.kernel_launches += per_step
-        key = (K, self._rain_kind, len(self._inflows), self._ring is not None, self.warps, self.min_blocks,
+        key = (K, self._rain_kind, len(self._inflows), self._ring is not None, self.warps, self.min_blocks, self.segments,
                tuple(sorted(self._forcing)))
         g, per = _cached_graph(self._graph_cache, key, one_window, self.device)
         self.kernel_launches += 1

@@ -17,6 +17,7 @@ __global__ void ensemble_finalize_kernel(GswEnsembleArgs a) {
         if (!st->done) atomicAdd(&s_open, 1);
     }
     __syncthreads();
+    if (a.run != nullptr) build_run_list(a, threadIdx.x, blockDim.x);
     if (threadIdx.x == 0) {
         a.scratch[0] = 0u;
         *a.all_done = (s_open == 0) ? 1 : 0;
@@ -47,6 +48,8 @@ static int check_ens(const GswEnsembleArgs* a) {
     if (!a->brick_ij || !a->brick_nbr || !a->brick_member || !a->flags || !a->q0 || !a->q1 || !a->q2 ||
         !a->bed || !a->members || !a->states || !a->scratch || !a->all_done)
         return set_error(GSW_ERR_INVALID, "ensemble: null pointer");
+    if (a->run != nullptr && a->member_brick_off == nullptr)
+        return set_error(GSW_ERR_INVALID, "ensemble: a running-member list needs member_brick_off");
     return GSW_OK;
 }
 

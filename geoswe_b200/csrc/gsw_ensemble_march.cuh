@@ -7,7 +7,9 @@
 // into its own GswLoopState. The block that finishes last (a ticket counter in scratch
 // memory) then evaluates every member's time-step rule for the next launch, so members
 // keep their own CFL dt with no grid-wide barrier and no host round trip; a member that
-// reaches its end time drops out while the others continue.
+// reaches its end time drops out while the others continue. With a running-member list
+// (GswEnsembleArgs.run) warps walk only the running members' bricks, and the last block
+// rebuilds the list when a member finishes.
 //
 // Included by gsw_ensemble.cu (exact arithmetic) and gsw_fast.cu (fast arithmetic,
 // with namespace gsw renamed).
@@ -27,20 +29,83 @@ __device__ __forceinline__ FlatPhys<float> member_phys(const GswMember& mb) {
     return ph;
 }
 
+// Rebuild the running-member brick list (GswEnsembleArgs.run) from the members' done
+// flags: each thread of the block takes a contiguous chunk of members, counts its
+// running members and their bricks, one thread scans the per-thread totals, and each
+// thread writes its chunk's entries. Every thread of the block calls it.
+__device__ __forceinline__ void build_run_list(const GswEnsembleArgs& a, int tid, int nth) {
+    __shared__ long long s_bricks[256];
+    __shared__ int s_count[256];
+    const int M = a.n_members;
+    const int chunk = (M + nth - 1) / nth;
+    const int k0 = min(M, tid * chunk), k1 = min(M, k0 + chunk);
+    long long nb = 0;
+    int nr = 0;
+    for (int k = k0; k < k1; ++k)
+        if (!a.states[k].done) { nb += a.member_brick_off[k + 1] - a.member_brick_off[k]; ++nr; }
+    s_bricks[tid] = nb;
+    s_count[tid] = nr;
+    __syncthreads();
+    if (tid == 0) {
+        long long pb = 0;
+        int pr = 0;
+        for (int t = 0; t < nth; ++t) {
+            const long long b = s_bricks[t];
+            const int r = s_count[t];
+            s_bricks[t] = pb; s_count[t] = pr;
+            pb += b; pr += r;
+        }
+        a.run[0] = pr;
+        a.run[1 + pr] = pb;
+    }
+    __syncthreads();
+    long long pb = s_bricks[tid];
+    int pr = s_count[tid];
+    for (int k = k0; k < k1; ++k)
+        if (!a.states[k].done) {
+            a.run[1 + pr] = pb;
+            a.run[M + 2 + pr] = k;
+            pb += a.member_brick_off[k + 1] - a.member_brick_off[k];
+            ++pr;
+        }
+}
+
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArgs a, FlatMesh<float> m) {
     if (*a.all_done) return;
     const int lane = threadIdx.x;
     const int W = blockDim.y;
-    for (int64_t b = (int64_t)blockIdx.x * W + threadIdx.y; b < a.n_bricks; b += (int64_t)gridDim.x * W) {
-        const int mi = a.brick_member[b];
+    const bool listed = a.run != nullptr;
+    const int n_run = listed ? (int)a.run[0] : 0;
+    const int64_t bricks = listed ? a.run[1 + n_run] : a.n_bricks;
+    const int S = a.segments > 0 ? a.segments                // row segments per brick, or by the work in flight
+                                 : auto_segments(bricks, (int64_t)gridDim.x * W, m.bh);
+    const int64_t total = bricks * S;
+    for (int64_t item = (int64_t)blockIdx.x * W + threadIdx.y; item < total; item += (int64_t)gridDim.x * W) {
+        const int64_t v = item / S;
+        const int seg = (int)(item - v * S);
+        int64_t b;
+        int mi;
+        if (listed) {                  // the running member whose brick range holds v (warp-uniform)
+            int lo = 0, hi = n_run - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (a.run[1 + mid] <= v) lo = mid; else hi = mid - 1;
+            }
+            mi = (int)a.run[a.n_members + 2 + lo];
+            b = a.member_brick_off[mi] + (v - a.run[1 + lo]);
+        } else {
+            b = v;
+            mi = a.brick_member[b];
+        }
         const GswLoopState* st = a.states + mi;
         if (st->done) continue;                                   // warp-uniform
         const GswMember& mb = a.members[mi];
         const FlatPhys<float> ph = member_phys(mb);
         const float dt = st->dt_f32;
         const float rate = (mb.rain_kind == GSW_RAIN_UNIFORM) ? mb.rain[st->rain_idx] : 0.0f;
-        unsigned long long lam = flat_brick<float, true>(m, ph, b, dt, rate, nullptr);
+        unsigned long long lam = flat_brick<float, true>(m, ph, b, seg * m.bh / S, (seg + 1) * m.bh / S, dt, rate,
+                                                         nullptr);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const unsigned long long w = __shfl_xor_sync(0xffffffffu, lam, o);
@@ -61,16 +126,19 @@ __global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArg
     if (!s_last) return;
     __threadfence();
     const int nth = blockDim.x * blockDim.y;
-    __shared__ int s_open;
-    if (tid == 0) s_open = 0;
+    __shared__ int s_open, s_finished;
+    if (tid == 0) { s_open = 0; s_finished = 0; }
     __syncthreads();
     for (int mi = tid; mi < a.n_members; mi += nth) {
         GswLoopState* st = a.states + mi;
         const unsigned long long lb = atomicAdd((unsigned long long*)&st->lam_bits, 0ull);  // coherent read
+        const int was_done = st->done;
         dt_finalize_one(a.members[mi].dt, st, lb);
         if (!st->done) atomicAdd(&s_open, 1);
+        else if (!was_done) s_finished = 1;
     }
     __syncthreads();
+    if (listed && s_finished && s_open > 0) build_run_list(a, tid, nth);   // block-uniform condition
     if (tid == 0) {
         a.scratch[0] = 0u;
         *a.all_done = (s_open == 0) ? 1 : 0;
@@ -82,6 +150,9 @@ inline int launch_ensemble_step(const GswEnsembleArgs* a, cudaStream_t st) {
     const int W = a->warps > 0 ? a->warps : 4;
     if (W < 1 || W > 8) return set_error(GSW_ERR_INVALID, "ensemble: warps must be in [1, 8]");
     const int grid = a->grid > 0 ? a->grid : 2 * sm_count();
+    const int S = a->segments > 0 ? a->segments : 1;
+    if ((S != 1 && S != 2 && S != 4) || a->brick_h % S != 0 || a->segments < 0)
+        return set_error(GSW_ERR_INVALID, "ensemble: segments must be 0, 1, 2 or 4 and divide brick_h");
     FlatMesh<float> m;
     m.q0 = a->q0; m.q1 = a->q1; m.q2 = a->q2;
     m.o0 = a->qn0; m.o1 = a->qn1; m.o2 = a->qn2;

@@ -28,9 +28,20 @@ struct FlatPhys {
     int ncol;
 };
 
+// Row segments per brick when the caller leaves the choice to the library: one warp
+// per brick once the bricks fill the `warps` that can run at once twice over
+// (throughput), else 2 or 4 warps per brick so that fewer bricks still keep enough
+// warps busy and each warp's march is shorter (latency). A segment recomputes the
+// x-face above its first row and reads two rows past each end.
+__host__ __device__ __forceinline__ int auto_segments(int64_t bricks, int64_t warps, int bh) {
+    int s = bricks >= 2 * warps ? 1 : (2 * bricks >= warps ? 2 : 4);
+    while (s > 1 && bh % s != 0) s >>= 1;
+    return s;
+}
+
 // For the flat kernels' argument struct
 template <typename T>
-struct FlatK { FlatMesh<T> m; FlatPhys<T> ph; const GswLoopState* st; unsigned long long* lam; };
+struct FlatK { FlatMesh<T> m; FlatPhys<T> ph; const GswLoopState* st; unsigned long long* lam; int segs; };
 
 // Slot of brick-relative (row, lane). Lanes 0/31 of the rows above/below the brick are
 // never used by an output cell; they read the zero brick.
@@ -90,12 +101,15 @@ __device__ __forceinline__ Face<T> shfl_up_face(const Face<T>& f) {
     return r;
 }
 
-// One brick, walked by one warp (T = float; double serves the adjoint's fp64 checks).
-// STEP: the fused step (returns this lane's wave speed bits); otherwise the residual.
-// `frame` is the gridded rain frame, or null.
+// Rows [r0, r1) of one brick, walked by one warp (T = float; double serves the adjoint's
+// fp64 checks). A segment reads rows r0-2 .. r1+1 through the brick view (the bricks
+// above and below past the brick's edge) and recomputes the x-face above row r0 from
+// the same inputs as the face below row r0-1, so splitting a brick's rows among warps
+// changes no value. STEP: the fused step (returns this lane's wave speed bits);
+// otherwise the residual. `frame` is the gridded rain frame, or null.
 template <typename T, bool STEP>
 __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, const FlatPhys<T>& ph, int64_t bidx,
-                                                         T dt, T rate, const T* frame) {
+                                                         int r0, int r1, T dt, T rate, const T* frame) {
     const int lane = threadIdx.x;
     unsigned long long lam_local = 0ull;
     BrickView v;
@@ -108,28 +122,28 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
     const int bi = m.bij[2 * bidx], bj = m.bij[2 * bidx + 1];
     const int bh = m.bh;
     Cell<T> cur, nx;
-    const T b_m2 = __ldg(m.b + v.slot(-2, lane));
-    { const int64_t s = v.slot(-1, lane); cur.h = __ldg(m.q0 + s); cur.hu = __ldg(m.q1 + s); cur.hv = __ldg(m.q2 + s); cur.b = __ldg(m.b + s); }
-    { const int64_t s = v.slot(0, lane); nx.h = __ldg(m.q0 + s); nx.hu = __ldg(m.q1 + s); nx.hv = __ldg(m.q2 + s); nx.b = __ldg(m.b + s); }
-    T b_next = __ldg(m.b + v.slot(1, lane));
+    const T b_m2 = __ldg(m.b + v.slot(r0 - 2, lane));
+    { const int64_t s = v.slot(r0 - 1, lane); cur.h = __ldg(m.q0 + s); cur.hu = __ldg(m.q1 + s); cur.hv = __ldg(m.q2 + s); cur.b = __ldg(m.b + s); }
+    { const int64_t s = v.slot(r0, lane); nx.h = __ldg(m.q0 + s); nx.hu = __ldg(m.q1 + s); nx.hv = __ldg(m.q2 + s); nx.b = __ldg(m.b + s); }
+    T b_next = __ldg(m.b + v.slot(r0 + 1, lane));
     // prefetch of the row after next (rows up to bh+1 exist: the brick below or the zero brick)
-    int64_t sp = v.slot(1, lane);
+    int64_t sp = v.slot(r0 + 1, lane);
     T pf_h = __ldg(m.q0 + sp), pf_hu = __ldg(m.q1 + sp), pf_hv = __ldg(m.q2 + sp);
-    T pf_b = __ldg(m.b + v.slot(2, lane));
+    T pf_b = __ldg(m.b + v.slot(r0 + 2, lane));
     make_prims(cur, ph.h_min);
     make_prims(nx, ph.h_min);
     cur.gx = (T)0.5 * (nx.b - b_m2) * ph.inv_dx;
     cur.gy = (T)0;
     nx.gx = (T)0.5 * (b_next - cur.b) * ph.inv_dx;
-    nx.gy = grad_y_flat<T>(m, ph, v, nx.b, 0, lane);
+    nx.gy = grad_y_flat<T>(m, ph, v, nx.b, r0, lane);
     Face<T> Wf;
     srm_face<T, true>(cur, nx, ph.half_dx, ph.inv_dx, ph.g, ph.h_min, Wf);
     cur = nx;
-    for (int r = 0; r < bh; ++r) {
+    for (int r = r0; r < r1; ++r) {
         nx.h = pf_h; nx.hu = pf_hu; nx.hv = pf_hv;
         nx.b = b_next;
         const T b_p2 = pf_b;
-        if (r + 1 < bh) {
+        if (r + 1 < r1) {
             sp = v.slot(r + 2, lane);
             pf_h = __ldg(m.q0 + sp); pf_hu = __ldg(m.q1 + sp); pf_hv = __ldg(m.q2 + sp);
             pf_b = __ldg(m.b + v.slot(r + 3, lane));

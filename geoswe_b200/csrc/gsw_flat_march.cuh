@@ -17,7 +17,9 @@ namespace gsw {
 template <typename T, bool STEP, int MINB>
 __global__ void __launch_bounds__(256, MINB) flat_march_kernel(FlatK<T> p) {
     if (STEP && p.st->done) return;
-    const int64_t bidx = (int64_t)blockIdx.x * blockDim.y + threadIdx.y;
+    const int64_t item = (int64_t)blockIdx.x * blockDim.y + threadIdx.y;   // (brick, row segment)
+    const int64_t bidx = item / p.segs;
+    const int seg = (int)(item - bidx * p.segs);
     unsigned long long lam_local = 0ull;
     T dt = (T)0, rate = (T)0;
     const T* frame = nullptr;
@@ -27,7 +29,9 @@ __global__ void __launch_bounds__(256, MINB) flat_march_kernel(FlatK<T> p) {
         if (p.ph.rain_kind == GSW_RAIN_GRIDDED) frame = p.ph.rain + (int64_t)p.st->rain_idx * p.ph.nx * p.ph.ny;
         if (p.ph.rain_kind == GSW_RAIN_LOOKUP) frame = p.ph.rain + (int64_t)p.st->rain_idx * p.ph.ncol;
     }
-    if (bidx < p.m.nb) lam_local = flat_brick<T, STEP>(p.m, p.ph, bidx, dt, rate, frame);
+    if (bidx < p.m.nb)
+        lam_local = flat_brick<T, STEP>(p.m, p.ph, bidx, seg * p.m.bh / p.segs, (seg + 1) * p.m.bh / p.segs,
+                                        dt, rate, frame);
     if (STEP && p.lam != nullptr) block_max_to(lam_local, p.lam);
 }
 
@@ -50,6 +54,9 @@ inline int fill_flat(const GswFlatArgs* a, FlatK<T>& k, bool step) {
     ph.ntab = (const T*)a->n_tab;
     ph.lookup = a->rain_lookup; ph.ncol = a->rain_ncol;
     k.st = a->state; k.lam = (unsigned long long*)a->lam_target;
+    k.segs = a->segments > 0 ? a->segments : auto_segments(a->n_bricks, (int64_t)sm_count() * 24, a->brick_h);
+    if (k.segs != 1 && k.segs != 2 && k.segs != 4) return set_error(GSW_ERR_INVALID, "flat: segments must be 0, 1, 2 or 4");
+    if (a->brick_h % k.segs != 0) return set_error(GSW_ERR_INVALID, "flat: brick_h must be a multiple of segments");
     if (step) {
         if (!a->state) return set_error(GSW_ERR_INVALID, "flat step: state is required");
         if (!a->n_tab || a->n_tab_len < 1) return set_error(GSW_ERR_INVALID, "flat step: n_tab is required");
@@ -71,7 +78,7 @@ inline int launch_flat(const GswFlatArgs* a, cudaStream_t s) {
     if (k.m.nb == 0) return GSW_OK;
     const int W = a->warps > 0 ? a->warps : 4;
     if (W < 1 || W > 8) return set_error(GSW_ERR_INVALID, "flat: warps must be in [1, 8]");
-    const int64_t blocks = (k.m.nb + W - 1) / W;
+    const int64_t blocks = (k.m.nb * k.segs + W - 1) / W;
     if (blocks > 0x7fffffffLL) return set_error(GSW_ERR_INVALID, "flat: too many bricks");
     const int mb = a->min_blocks;
     if (mb != 0 && (mb < 3 || mb > 5)) return set_error(GSW_ERR_INVALID, "flat: min_blocks must be 0, 3, 4 or 5");

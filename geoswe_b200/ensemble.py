@@ -85,8 +85,11 @@ class Ensemble:
         self._all_done = torch.zeros(1, dtype=torch.int32, device=dev)
         # fixed device buffers: captured graphs hold their addresses across runs
         self._members_dev = torch.zeros(M * C.sizeof(GswMember), dtype=torch.uint8, device=dev)
+        # running-member brick list, rebuilt on the device when a member finishes
+        self._brick_off_dev = torch.from_numpy(self.brick_off.copy()).to(dev)
+        self._run = torch.zeros(2 * M + 2, dtype=torch.int64, device=dev)
         self._parity = np.zeros(M, np.int64)       # buffer of each member's current state
-        self.warps, self.grid, self.min_blocks = int(warps), int(grid), 0
+        self.warps, self.grid, self.min_blocks, self.segments = int(warps), int(grid), 0, 0
         self.kernel_launches = 0
         self._graph_cache = {}
 
@@ -120,7 +123,7 @@ class Ensemble:
         a = GswEnsembleArgs()
         a.abi_version = L.ABI_VERSION
         a.brick_h, a.n_bricks, a.n_members = self.brick_h, self.n_bricks, len(self.members)
-        a.warps, a.grid, a.min_blocks = self.warps, self.grid, self.min_blocks
+        a.warps, a.grid, a.min_blocks, a.segments = self.warps, self.grid, self.min_blocks, self.segments
         a.arith = self.arith
         a.brick_ij, a.brick_nbr, a.brick_member = _ptr(self._bij), _ptr(self._bnbr), _ptr(self._bmem)
         a.flags, a.n_cls = _ptr(self._flags), _ptr(self._ncls)
@@ -129,6 +132,7 @@ class Ensemble:
         a.bed, a.max_h = _ptr(self._b), _ptr(self._max_h)
         a.members, a.states = _ptr(self._members_dev), _ptr(self._states)
         a.scratch, a.all_done = _ptr(self._scratch), _ptr(self._all_done)
+        a.member_brick_off, a.run = _ptr(self._brick_off_dev), _ptr(self._run)
         return a
 
     def _build_members(self, t_end, max_steps, dt_max):
@@ -177,21 +181,23 @@ class Ensemble:
         self.kernel_launches += 2
         return p0
 
-    def time_step(self, t_end, *, warps, grid, min_blocks=0, reps=6, max_steps: int = 10 ** 9, dt_max=None):
+    def time_step(self, t_end, *, warps, grid, min_blocks=0, segments=0, reps=6, max_steps: int = 10 ** 9,
+                  dt_max=None):
         """Mean duration (ms) of one ensemble step launch with the given schedule, from the
         current state; the states are restored before every launch and the members' state
         is left as it was."""
         _protos()
         p0 = self._prepare(t_end, max_steps, dt_max)
-        snap = self._states.clone()
-        saved = (self.warps, self.grid, self.min_blocks)
-        self.warps, self.grid, self.min_blocks = int(warps), int(grid), int(min_blocks)
+        snap, snap_run = self._states.clone(), self._run.clone()
+        saved = (self.warps, self.grid, self.min_blocks, self.segments)
+        self.warps, self.grid, self.min_blocks, self.segments = int(warps), int(grid), int(min_blocks), int(segments)
         args = self._args(self._q[p0], self._q[1 - p0])
-        self.warps, self.grid, self.min_blocks = saved
+        self.warps, self.grid, self.min_blocks, self.segments = saved
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         total = 0.0
         for k in range(reps + 1):
             self._states.copy_(snap)
+            self._run.copy_(snap_run)
             self._scratch.zero_()
             self._all_done.zero_()
             e0.record()
@@ -202,6 +208,7 @@ class Ensemble:
                 total += e0.elapsed_time(e1)
         self.kernel_launches += reps + 1
         self._states.copy_(snap)
+        self._run.copy_(snap_run)
         return total / reps
 
     def run(self, t_end, *, max_steps: int = 10 ** 9, dt_max=None, window: int = 64):
@@ -218,7 +225,7 @@ class Ensemble:
                 L.call("gsw_ensemble_step", C.byref(self._args(src, dst)), st)
             return K
 
-        key = (K, p0, self.warps, self.grid, self.min_blocks)
+        key = (K, p0, self.warps, self.grid, self.min_blocks, self.segments)
         if key not in self._graph_cache:
             self._graph_cache.clear()
             side = torch.cuda.Stream(device=self.device)

@@ -285,7 +285,9 @@ typedef struct GswFlatArgs {
     void*    max_h;            /* slot-indexed, or NULL */
     const int32_t* rain_lookup;/* GSW_RAIN_LOOKUP: per slot, the column of rain[frame * rain_ncol + col] */
     int32_t  rain_ncol;
-    int32_t  reserved2;
+    int32_t  segments;         /* warps per brick: 1 (one warp walks the brick's rows), 2 or 4 (each walks
+                                  brick_h / segments rows: shorter per-warp latency for small meshes),
+                                  0 (chosen from the brick count against the warps the GPU runs at once) */
 } GswFlatArgs;
 
 /* Discharge inlet of the compressed mesh: one ghost (ring) slot per inlet cell, next to
@@ -462,7 +464,8 @@ typedef struct GswEnsembleArgs {
     int32_t  grid;               /* persistent blocks (0: 2 per SM) */
     int32_t  min_blocks;         /* register cap: 0 (compiler's choice), 3 (80 regs), 4 (64 regs) or 5 (48 regs) */
     int32_t  arith;              /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST */
-    int32_t  reserved0;
+    int32_t  segments;           /* warps per brick: 1, 2 or 4 (as GswFlatArgs.segments), or 0: chosen per
+                                    launch from the running members' bricks against the grid's warps */
     const int32_t* brick_ij;     /* (n_bricks, 2) */
     const int32_t* brick_nbr;    /* (n_bricks, 4) global brick ids */
     const int32_t* brick_member; /* (n_bricks) */
@@ -476,6 +479,14 @@ typedef struct GswEnsembleArgs {
     GswLoopState* states;        /* device, n_members */
     uint32_t* scratch;           /* device, >= 4 words, zero before the first step: block tickets */
     int32_t* all_done;           /* device int: 1 once every member is done */
+    /* Running-member brick list (optional; NULL: every launch scans all bricks and skips
+       finished members brick by brick). member_brick_off: device, n_members + 1, member
+       k's bricks are [off[k], off[k+1]). run: device, 2 * n_members + 2 words, written by
+       gsw_ensemble_finalize and rebuilt by the step when a member finishes: run[0] = the
+       running count R, run[1 .. R+1] = their brick-count prefix, run[n_members + 2 + i]
+       = the i-th running member. A launch then visits running members' bricks only. */
+    const int64_t* member_brick_off;
+    int64_t* run;
 } GswEnsembleArgs;
 
 /* Wave speed of every member's current state into states[m].lam_bits (atomicMax). */

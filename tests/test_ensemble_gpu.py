@@ -35,12 +35,16 @@ SPECS = [(1, 40, 50, 0.5, 80.0, 1.0), (2, 64, 64, 0.8, 40.0, 0.8), (3, 90, 70, 0
          (4, 33, 120, 0.6, 60.0, 1.1)]
 
 
-def test_members_equal_standalone_runs():
+@pytest.mark.parametrize("segments", [1, 4])
+def test_members_equal_standalone_runs(segments):
+    """Members end at different times (the running-member list is rebuilt as each one
+    finishes); row segments per brick change no bit."""
     from geoswe_b200.ensemble import Ensemble
     t_ends = [900.0, 600.0, 1200.0, 750.0]
     alone = [_member(*sp) for sp in SPECS]
     steps_alone = [cs.run(t_end=te) for cs, te in zip(alone, t_ends)]
     ens = Ensemble([_member(*sp) for sp in SPECS])
+    ens.segments = segments
     steps = ens.run(t_end=t_ends, window=16)
     assert steps == steps_alone
     for k, cs in enumerate(alone):

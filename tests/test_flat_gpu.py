@@ -92,6 +92,29 @@ def test_flat_run_bitwise_oracle(linf):
         assert same(cs.flat(c).cpu().numpy(), o.q[c]), c
 
 
+def test_row_segments_change_no_bit():
+    """Splitting each brick's rows among 2 or 4 warps (GswFlatArgs.segments) gives the
+    same residual and the same run as one warp per brick."""
+    from geoswe_b200 import RainfallForcing
+    from geoswe_b200.compressed import CompressedSolver
+    q0, bed = flowing(70, 97, seed=12, dtype=np.float32)
+    mask = _blob_mask(70, 97)
+    out = []
+    for segs in (1, 2, 4):
+        s = _dense(q0, bed, mask, friction="manning", manning_n=0.03)
+        cs = CompressedSolver.from_dense(s)
+        cs.set_rain(RainfallForcing(time_s=[0.0, 1e9], rate_mm_h=[30.0, 30.0]))
+        cs.segments = segs
+        r = cs.residual().cpu().numpy()
+        n = cs.run(t_end=60.0)
+        out.append((r, n, cs.t, [cs.flat(c).cpu().numpy() for c in range(3)]))
+    for r, n, t, q in out[1:]:
+        assert same(r, out[0][0])
+        assert n == out[0][1] > 10 and t == out[0][2]
+        for c in range(3):
+            assert same(q[c], out[0][3][c]), c
+
+
 def test_dense_masked_run_equals_flat_run():
     """With the dense solver's velocity norm (cfl_linf) and a mask away from the edges,
     the dense run over the whole grid and the compressed run take the same steps and
