@@ -186,7 +186,7 @@ def measure_dense(args, z, cls, n, world, arith="exact"):
     launches = s.kernel_launches - l0
     assert steps == args.steps, (steps, args.steps)
     kern_ms = time_step_kernel(s, reps=args.kernel_reps)
-    shape = {"tile_rows": s._tile_rows or 32, "warps": s._warps or 4, "min_blocks": s._min_blocks}
+    shape = {"tile_rows": s._tile_rows or "auto", "warps": s._warps or 4, "min_blocks": s._min_blocks}
     del s
     torch.cuda.empty_cache()
     if world > 1:

@@ -21,7 +21,7 @@ import torch
 
 from . import _lib as L
 
-DENSE_SPACE = dict(tile_rows=(16, 32, 64), warps=(2, 4, 8), min_blocks=(0, 3, 4, 5))
+DENSE_SPACE = dict(tile_rows=(0, 4, 8, 16, 32, 64), warps=(2, 4, 8), min_blocks=(0, 3, 4, 5))
 
 
 def _cache_path() -> Path:

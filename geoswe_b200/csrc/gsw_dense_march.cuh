@@ -233,7 +233,15 @@ inline int fill_dense(const GswDenseArgs* a, DenseK<T>& k, bool step) {
     k.ntab = (const T*)a->n_tab; k.nfield = (const T*)a->n_field;
     k.vcap = (T)a->vcap; k.quad = a->quadratic; k.keep_h = a->keep_h;
     k.max_h = (T*)a->max_h; k.cfl_skip = a->cfl_skip; k.h_cfl = (T)a->h_cfl;
-    k.tile_rows = a->tile_rows > 0 ? a->tile_rows : 32;
+    if (a->tile_rows > 0) {
+        k.tile_rows = a->tile_rows;
+    } else {   // rows per warp: the longest march (<= 32 rows) that still gives twice the resident warps
+        const int64_t strips = (a->nyp - 2 * k.lo + 29) / 30, nrows = a->nxp - 2 * k.lo;
+        const int64_t want = 2LL * sm_count() * 24;
+        k.tile_rows = 4;
+        for (int tr = 32; tr > 4; tr >>= 1)
+            if (strips * ((nrows + tr - 1) / tr) >= want) { k.tile_rows = tr; break; }
+    }
     if (step) {
         if (!a->state) return set_error(GSW_ERR_INVALID, "dense step: state (GswLoopState*) is required");
         if (a->rain_kind != GSW_RAIN_NONE && a->rain_kind != GSW_RAIN_UNIFORM && a->rain_kind != GSW_RAIN_GRIDDED)

@@ -165,7 +165,8 @@ typedef struct GswDenseArgs {
     void*    max_h;            /* running max depth, pitch = pitch, or NULL */
     const uint8_t* cfl_skip;   /* interior (nx, ny) C-order: 1 = excluded from the wave speed */
     double   h_cfl;            /* wave-speed wet threshold (and divisor) */
-    int32_t  tile_rows;        /* rows per warp strip (0: default 32) */
+    int32_t  tile_rows;        /* rows per warp strip; 0: the largest of 32, 16, 8, 4 that gives at least
+                                  twice the warps the GPU runs at once */
     int32_t  warps;            /* warps per block (0: default 4) */
     int32_t  min_blocks;       /* register cap: 0 (compiler's choice), 3 (80 regs), 4 (64 regs) or 5 (48 regs) */
     int32_t  arith;            /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST (GSW_F32 step only) */
