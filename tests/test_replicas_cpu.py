@@ -32,3 +32,13 @@ def test_max_over_ranks_gloo_world_2():
         out = m.dict()
         mp.start_processes(_rank, args=(2, _free_port(), out), nprocs=2, start_method="spawn", join=True)
         assert dict(out) == {0: 15.0, 1: 15.0}
+
+
+def test_reference_arm_uses_every_core():
+    """The CPU reference arm runs one spawned process per core, each its own sample,
+    and reports their aggregate over the common timed interval."""
+    from oracle import numpy_ref
+    r = numpy_ref.time_rain_on_terrain_parallel(n=48, steps=2, warm=1, procs=2)
+    assert r["cores"] == 2 and r["value"] > 0 and r["seconds"] > 0
+    one = numpy_ref.time_rain_on_terrain(n=48, steps=2, warm=1)
+    assert one["cores"] == 1 and one["value"] > 0
