@@ -128,6 +128,11 @@ class GswMember(C.Structure):
                 ("keep_h", i32), ("rain_kind", i32), ("reserved0", i32), ("rain", vp), ("n_tab", vp)]
 
 
+class GswTuneResult(C.Structure):
+    _fields_ = [("abi_version", u32), ("tile_rows", i32), ("warps", i32), ("min_blocks", i32),
+                ("segments", i32), ("n_tried", i32), ("ms", C.c_float), ("reserved", i32)]
+
+
 class GswEnsembleArgs(C.Structure):
     _fields_ = [("abi_version", u32), ("brick_h", i32), ("n_bricks", i64), ("n_members", i32),
                 ("warps", i32), ("grid", i32), ("min_blocks", i32), ("arith", i32), ("segments", i32),
@@ -148,6 +153,8 @@ _PROTOS = {
     "gsw_inflow_apply": [C.POINTER(GswInflowArgs), vp],
     "gsw_dt_finalize": [C.POINTER(GswDtParams), vp, vp],
     "gsw_dt_params_upload": [C.POINTER(GswDtParams), vp, vp],
+    "gsw_dense_autotune": [C.POINTER(GswDenseArgs), C.c_int32, C.c_int32, C.POINTER(GswTuneResult), vp],
+    "gsw_flat_autotune": [C.POINTER(GswFlatArgs), C.c_int32, C.c_int32, C.POINTER(GswTuneResult), vp],
     "gsw_dt_finalize_dev": [vp, vp, vp],
     "gsw_loop_commit": [vp, vp],
     "gsw_flat_inflow_apply": [C.POINTER(GswFlatInflowArgs), vp],

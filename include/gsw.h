@@ -534,6 +534,34 @@ GSW_API int gsw_dt_finalize_dev(const GswDtParams* dev, GswLoopState* state, voi
 GSW_API int gsw_loop_commit(GswLoopState* state, void* stream);
 
 /* ------------------------------------------------------------------------- */
+/* Launch-shape search (no counterpart in the reference: its launch shapes are */
+/* fixed). Times the fused step at every shape of the search space with CUDA   */
+/* events on `stream` and the caller's buffers, and returns the fastest:       */
+/*   dense: tile_rows {0 (automatic), 4, 8, 16, 32, 64} x warps {2, 4, 8} x     */
+/*          register cap min_blocks {0, 3, 4, 5}                               */
+/*   flat:  warps {2, 4, 8} x min_blocks {0, 3, 4, 5} x segments {0, 1, 2, 4}   */
+/* The step's outputs (qn*) are overwritten; lam_target and max_h are not      */
+/* touched; the loop state is read (it must not be done). Results are cached   */
+/* per device, kernel family, arithmetic, dtype and size class (< 2^20,        */
+/* < 2^24, larger) behind a mutex; use_cache = 1 returns a cached result       */
+/* without launching.                                                          */
+/* ------------------------------------------------------------------------- */
+typedef struct GswTuneResult {
+    uint32_t abi_version;      /* GSW_ABI_VERSION, set by the caller (the rest is written by the library) */
+    int32_t  tile_rows;        /* dense */
+    int32_t  warps;
+    int32_t  min_blocks;
+    int32_t  segments;         /* flat */
+    int32_t  n_tried;          /* shapes timed */
+    float    ms;               /* mean launch time of the winner */
+    int32_t  reserved;
+} GswTuneResult;
+GSW_API int gsw_dense_autotune(const GswDenseArgs* a, int32_t reps, int32_t use_cache, GswTuneResult* out,
+                               void* stream);
+GSW_API int gsw_flat_autotune(const GswFlatArgs* a, int32_t reps, int32_t use_cache, GswTuneResult* out,
+                              void* stream);
+
+/* ------------------------------------------------------------------------- */
 /* Library                                                                    */
 /* ------------------------------------------------------------------------- */
 GSW_API const char* gsw_last_error(void);
