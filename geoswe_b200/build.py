@@ -24,7 +24,7 @@ LIB = PKG / "libgsw.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC",
-              "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
+              "-Xcompiler", "-fvisibility=hidden", "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"]
 # The fast-arithmetic compilation of the binary32 step kernels (gsw_fast.cu): FMA
 # contraction and flush-to-zero; its square root and division are the approximate
 # instructions named in gsw_core.cuh.

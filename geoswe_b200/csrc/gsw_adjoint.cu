@@ -367,6 +367,7 @@ static int fill_adj(const GswFlatAdjArgs* a, AdjK<T>& k) {
     ph.rain_kind = f.rain_kind; ph.rain = (const T*)f.rain; ph.ngh = f.ngh; ph.nx = f.nx; ph.ny = f.ny;
     ph.ntab = (const T*)f.n_tab;
     ph.lookup = f.rain_lookup; ph.ncol = f.rain_ncol;
+    ph.g_recip = (T)0;          // the recomputed faces divide (the same bits as the forward's)
     k.st = f.state;
     k.li0 = (const T*)a->lam_in0; k.li1 = (const T*)a->lam_in1; k.li2 = (const T*)a->lam_in2;
     k.lo0 = (T*)a->lam_out0; k.lo1 = (T*)a->lam_out1; k.lo2 = (T*)a->lam_out2;

@@ -16,6 +16,7 @@ int set_error(int code, const char* fmt, ...);
 int check_launch(const char* what);
 int sm_count();
 void count_launch(int n = 1);
+float div_const_recip(float g);
 }  // namespace gsw_rt
 
 namespace gsw {
@@ -24,6 +25,7 @@ using gsw_rt::set_error;
 using gsw_rt::check_launch;
 using gsw_rt::sm_count;
 using gsw_rt::count_launch;
+using gsw_rt::div_const_recip;
 
 // Max of a non-negative IEEE-bits value over the block, then one atomicMax.
 // Every thread of the block must call it (it holds a block barrier).

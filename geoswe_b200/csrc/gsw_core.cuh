@@ -77,6 +77,28 @@ __device__ __forceinline__ double sqrt_z(double x) { return x == 0.0 ? x : sqrt(
 __device__ __forceinline__ double div_z(double a, double b) { return a / b; }
 #endif
 
+// q = h / g for the HLLC star depth, by the constant's reciprocal when the library has
+// shown that this is the IEEE quotient: y = RN(1/g), q0 = RN(h y), r = h - g q0 (exact,
+// one FMA), q = RN(q0 + r y) -- P. Markstein's correction step ("IA-64 and Elementary
+// Functions", 2000), as used for division by a constant by Brisebarre, Muller and
+// Raina (IEEE Trans. Computers 53(8), 2004). gsw_rt::div_const_recip checks the
+// sequence against the IEEE quotient for every binary32 significand of h with this g
+// (rounding commutes with scaling by powers of two, so [1, 2) covers every h whose
+// products stay normal, which the range test below ensures) and passes y, else 0.
+template <typename T>
+__device__ __forceinline__ T div_g(T h, T g, T y) { return gdiv(h, g); }
+#ifndef GSW_FAST_ARITH
+template <>
+__device__ __forceinline__ float div_g<float>(float h, float g, float y) {
+    if (y != 0.0f && h >= 0x1p-100f && h <= 0x1p100f) {
+        const float q0 = h * y;
+        const float r = fmaf(-g, q0, h);
+        return fmaf(r, y, q0);
+    }
+    return h / g;
+}
+#endif
+
 // Primitive state of one cell (PRIMS macro, rhs_cuda.py:931-938) plus what the
 // faces need: free surface and the central bed gradients.
 template <typename T>
@@ -142,14 +164,14 @@ __device__ __forceinline__ double pow_m43(double x) {
 // build, rhs_cuda.py:1717-1722): uN normal, uT transverse velocity.
 template <typename T>
 __device__ __forceinline__ void hllc(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
-                                     T g, T h_min, T& Fh, T& FN, T& FT) {
+                                     T g, T h_min, T& Fh, T& FN, T& FT, T g_recip = (T)0) {
     const T z = Real<T>::zero();
     const T half = (T)0.5, quarter = (T)0.25, two = (T)2.0;
     const T aL = sqrt_z(g * (hL > z ? hL : z));
     const T aR = sqrt_z(g * (hR > z ? hR : z));
     const T u_st = half * (uNL + uNR) + aL - aR;
     const T h_rt = half * (aL + aR) + quarter * (uNL - uNR);
-    const T h_st = (h_rt > z) ? gdiv(h_rt * h_rt, g) : z;
+    const T h_st = (h_rt > z) ? div_g(h_rt * h_rt, g, g_recip) : z;
     const T a_st = sqrt_z(g * (h_st > z ? h_st : z));
     const T SL_w = gmin(uNL - aL, u_st - a_st);
     const T SR_w = gmax(uNR + aR, u_st + a_st);
@@ -206,7 +228,7 @@ struct Face { T Fh, Fn, Ft, srcL, srcR; bool wet; };
 
 template <typename T, bool XAXIS>
 __device__ __forceinline__ void srm_face(const Cell<T>& L, const Cell<T>& R,
-                                         T half_d, T inv_d, T g, T h_min, Face<T>& F) {
+                                         T half_d, T inv_d, T g, T h_min, Face<T>& F, T g_recip = (T)0) {
     const T z = Real<T>::zero();
     F.wet = !(L.h < h_min && R.h < h_min);
     if (!F.wet) { F.Fh = z; F.Fn = z; F.Ft = z; F.srcL = z; F.srcR = z; return; }
@@ -225,8 +247,8 @@ __device__ __forceinline__ void srm_face(const Cell<T>& L, const Cell<T>& R,
     const T h_Lf = gmax(z, eta_Lf - zf0);
     const T h_Rf = gmax(z, eta_Rf - zf0);
     T Fh, FN, FT;
-    if (XAXIS) hllc<T>(h_Lf, L.u, L.v, h_Rf, R.u, R.v, g, h_min, Fh, FN, FT);
-    else       hllc<T>(h_Lf, L.v, L.u, h_Rf, R.v, R.u, g, h_min, Fh, FN, FT);
+    if (XAXIS) hllc<T>(h_Lf, L.u, L.v, h_Rf, R.u, R.v, g, h_min, Fh, FN, FT, g_recip);
+    else       hllc<T>(h_Lf, L.v, L.u, h_Rf, R.v, R.u, g, h_min, Fh, FN, FT, g_recip);
     F.Fh = Fh * inv_d;
     F.Fn = FN * inv_d;
     F.Ft = FT * inv_d;
@@ -308,11 +330,13 @@ __device__ __forceinline__ void wetdry_friction(T& h, T& hu, T& hv, bool frictio
 __device__ __forceinline__ unsigned long long lam_dense_bits(float h, float hu, float hv,
                                                              float g, float h_cfl) {
     if (h < h_cfl) return 0ull;
-    const float u = div_z(hu, h);
-    const float v = div_z(hv, h);
-    const float au = fabsf(u), av = fabsf(v);
-    const float lam = ((au > av) ? au : av) + gsqrt(g * h);
-    const bool fin = (lam <= 3.0e38f) && (au <= 3.0e38f) && (av <= 3.0e38f);
+    // max(|hu/h|, |hv/h|) with one division: a correctly rounded division by h > 0 is
+    // monotonic and symmetric, so it equals max(|hu|, |hv|) / h to the bit (NaN momentum
+    // is tested on its own; a NaN or infinite h leaves the quotient non-finite)
+    const float ahu = fabsf(hu), ahv = fabsf(hv);
+    const float aw = div_z(ahu > ahv ? ahu : ahv, h);
+    const float lam = aw + gsqrt(g * h);
+    const bool fin = (hu == hu) && (hv == hv) && (lam <= 3.0e38f) && (aw <= 3.0e38f);
     return fin ? (unsigned long long)__double_as_longlong((double)lam) : 0x7ff0000000000000ull;
 }
 // Dense loop, fp64 (the generic path, solver.py:2668-2693 with swe.max_wave_speed_2d):
@@ -341,9 +365,16 @@ __device__ __forceinline__ unsigned long long lam_flat_bits(float h, float hu, f
     if (h != h) return 0x7ff8000000000000ull;
     if (h < h_min) return 0ull;
     const float hs = h > h_min_cfl ? h : h_min_cfl;
-    const float u = div_z(hu, hs), v = div_z(hv, hs);
     const float c = gsqrt(g * (h > 0.0f ? h : 0.0f));
-    const float speed = linf ? fmaxf(fabsf(u), fabsf(v)) : sqrt_z(u * u + v * v);
+    float speed;
+    if (linf) {   // one division, as in lam_dense_bits (fmaxf ignores a NaN operand, as before)
+        const float ahu = (hu == hu) ? fabsf(hu) : 0.0f, ahv = (hv == hv) ? fabsf(hv) : 0.0f;
+        speed = div_z(ahu > ahv ? ahu : ahv, hs);
+        if (hu != hu && hv != hv) speed = __int_as_float(0x7fffffff);
+    } else {
+        const float u = div_z(hu, hs), v = div_z(hv, hs);
+        speed = sqrt_z(u * u + v * v);
+    }
     const float l = speed + c;
     return (unsigned long long)__double_as_longlong((double)l);
 }

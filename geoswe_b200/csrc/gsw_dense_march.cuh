@@ -37,6 +37,7 @@ struct DenseK {
     const uint8_t* cfl_skip;
     T h_cfl;
     int tile_rows;
+    T g_recip;                   // RN(1/g) for the star depth's h / g, or 0 (gsw_core.cuh div_g)
 };
 
 template <typename T>
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
         nx.gx = (T)0.5 * (b_next - cur.b) * p.inv_dx;
         nx.gy = grad_y(p, nx.b, i0, c, lane);
         Face<T> Wf;
-        srm_face<T, true>(cur, nx, p.half_dx, p.inv_dx, p.g, p.h_min, Wf);
+        srm_face<T, true>(cur, nx, p.half_dx, p.inv_dx, p.g, p.h_min, Wf, p.g_recip);
         cur = nx;
 
         for (int r = i0; r < i1; ++r) {
@@ -156,10 +157,10 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
             nx.gy = grad_y(p, nx.b, r + 1, c, lane);
 
             Face<T> Ef;
-            srm_face<T, true>(cur, nx, p.half_dx, p.inv_dx, p.g, p.h_min, Ef);
+            srm_face<T, true>(cur, nx, p.half_dx, p.inv_dx, p.g, p.h_min, Ef, p.g_recip);
             const Cell<T> rn = shfl_cell_down(cur);
             Face<T> Nf;
-            srm_face<T, false>(cur, rn, p.half_dy, p.inv_dy, p.g, p.h_min, Nf);
+            srm_face<T, false>(cur, rn, p.half_dy, p.inv_dy, p.g, p.h_min, Nf, p.g_recip);
             const Face<T> Sf = shfl_face_up(Nf);
 
             if (out_lane) {
@@ -227,6 +228,7 @@ inline int fill_dense(const GswDenseArgs* a, DenseK<T>& k, bool step) {
         k.half_dx = (T)0.5 * dx; k.half_dy = (T)0.5 * dy;
     }
     k.g = (T)a->g; k.h_min = (T)a->h_min;
+    k.g_recip = sizeof(T) == 4 ? (T)div_const_recip((float)a->g) : (T)0;
     k.st = a->state; k.lam = (unsigned long long*)a->lam_target;
     k.rain_kind = a->rain_kind; k.rain = (const T*)a->rain;
     k.friction_kind = a->friction_kind; k.ncls = a->n_cls; k.cpitch = a->n_cls_pitch;

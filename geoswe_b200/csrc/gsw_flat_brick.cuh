@@ -26,6 +26,7 @@ struct FlatPhys {
     const T* rain; const T* ntab;
     const int32_t* lookup;   // GSW_RAIN_LOOKUP: per-slot column of the rain row
     int ncol;
+    T g_recip;               // RN(1/g) for the star depth's h / g, or 0 (gsw_core.cuh div_g)
 };
 
 // Row segments per brick when the caller leaves the choice to the library: one warp
@@ -137,7 +138,7 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
     nx.gx = (T)0.5 * (b_next - cur.b) * ph.inv_dx;
     nx.gy = grad_y_flat<T>(m, ph, v, nx.b, r0, lane);
     Face<T> Wf;
-    srm_face<T, true>(cur, nx, ph.half_dx, ph.inv_dx, ph.g, ph.h_min, Wf);
+    srm_face<T, true>(cur, nx, ph.half_dx, ph.inv_dx, ph.g, ph.h_min, Wf, ph.g_recip);
     cur = nx;
     for (int r = r0; r < r1; ++r) {
         nx.h = pf_h; nx.hu = pf_hu; nx.hv = pf_hv;
@@ -152,10 +153,10 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
         nx.gx = (T)0.5 * (b_p2 - cur.b) * ph.inv_dx;
         nx.gy = grad_y_flat<T>(m, ph, v, nx.b, r + 1, lane);
         Face<T> Ef;
-        srm_face<T, true>(cur, nx, ph.half_dx, ph.inv_dx, ph.g, ph.h_min, Ef);
+        srm_face<T, true>(cur, nx, ph.half_dx, ph.inv_dx, ph.g, ph.h_min, Ef, ph.g_recip);
         const Cell<T> rn = shfl_down_cell<T>(cur);
         Face<T> Nf;
-        srm_face<T, false>(cur, rn, ph.half_dy, ph.inv_dy, ph.g, ph.h_min, Nf);
+        srm_face<T, false>(cur, rn, ph.half_dy, ph.inv_dy, ph.g, ph.h_min, Nf, ph.g_recip);
         const Face<T> Sf = shfl_up_face<T>(Nf);
         if (lane >= 1 && lane <= 30) {
             const int64_t o = bidx * v.BS + (int64_t)r * GSW_BRICK_PITCH + (lane - 1);

@@ -7,7 +7,10 @@
 // host round trip; the host polls `done` once per window.
 #include "gsw_common.cuh"
 #include <atomic>
+#include <cmath>
+#include <mutex>
 #include <string.h>
+#include <unordered_map>
 
 namespace gsw_rt {
 
@@ -42,6 +45,41 @@ int sm_count() {
             cached = 148;
     }
     return cached;
+}
+
+// RN(1/g) when the correction sequence of gsw::div_g reproduces the IEEE quotient h / g
+// for every binary32 significand of h (checked exhaustively, once per g per process;
+// the IEEE quotient by the double quotient rounded once more, exact since 53 >= 2*24+2
+// bits), else 0 (the kernels then divide).
+float div_const_recip(float g) {
+    static std::mutex mu;
+    static std::unordered_map<uint32_t, float> cache;
+    uint32_t key;
+    memcpy(&key, &g, sizeof(key));
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    float y = 0.0f;
+    if (std::isnormal(g) && g > 0.0f) {
+        const float yy = (float)(1.0 / (double)g);
+        bool ok = std::isnormal(yy);
+        for (uint32_t m = 0; ok && m < (1u << 23); ++m) {
+            const uint32_t bits = 0x3f800000u | m;
+            float h;
+            memcpy(&h, &bits, sizeof(h));
+            const float ref = (float)((double)h / (double)g);
+            const float q0 = h * yy;
+            const float r = std::fmaf(-g, q0, h);
+            const float q = std::fmaf(r, yy, q0);
+            ok = memcmp(&q, &ref, sizeof(q)) == 0;
+        }
+        if (ok) y = yy;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = y;
+    return y;
 }
 
 }  // namespace gsw_rt
