@@ -49,6 +49,14 @@ class _Tables:
     """Device copies of the forcing tables, in the solver's dtype."""
 
 
+def _to_device(x, device, dtype):
+    """A host array or tensor on `device` in `dtype`: one copy of the data as given,
+    the dtype conversion on the device."""
+    if not torch.is_tensor(x):
+        x = torch.from_numpy(np.ascontiguousarray(x))
+    return x.to(device).to(dtype)
+
+
 def _cached_graph(cache, key, capture, device, keep=4):
     """The CUDA graph of `capture()` for `key`, captured on first use on a side stream
     (the captured kernels read the loop's `done` flag first, so a replay after the loop
@@ -93,17 +101,16 @@ class Solver2D:
         if ngh < 2:
             raise ValueError(f"ngh={ngh} is too small: the fused SRM-HLLC step reads two cells "
                              f"beyond every interior cell. Construct Mesh2D with ngh >= 2.")
-        q0 = np.asarray(q0.detach().cpu() if torch.is_tensor(q0) else q0)
-        b = np.asarray(b.detach().cpu() if torch.is_tensor(b) else b)
+        if not torch.is_tensor(q0):
+            q0 = np.asarray(q0)
+        if not torch.is_tensor(b):
+            b = np.asarray(b)
         if tuple(q0.shape) != (3, mesh.nx, mesh.ny):
             raise ValueError(f"q0 must have shape (3, nx, ny) = (3, {mesh.nx}, {mesh.ny}); "
                              f"got {tuple(q0.shape)}")
         if tuple(b.shape) != (mesh.nx, mesh.ny):
             raise ValueError(f"the bed must have shape (nx, ny) = ({mesh.nx}, {mesh.ny}); "
                              f"got {tuple(b.shape)}")
-        for what, arr in (("the bed", b), ("the initial state q0", q0)):
-            if not np.isfinite(arr).all():
-                raise ValueError(f"Solver2D: {what} holds non-finite values (NaN or inf)")
         rate = getattr(getattr(cfg, "rainfall_forcing", None), "rate_mm_h", None)
         if rate is not None and int(getattr(rate, "ndim", 1)) == 3 and tuple(rate.shape[1:]) != (mesh.nx, mesh.ny):
             raise ValueError(f"Config.rainfall_forcing.rate_mm_h has shape {tuple(rate.shape)}; gridded "
@@ -132,15 +139,19 @@ class Solver2D:
         dev, td = self.device, self.t_dtype
         self._buf = [torch.zeros((3, self.nxp, self.pitch), dtype=td, device=dev) for _ in range(2)]
         self._cur = 0
-        qpad = np.zeros((3, self.nxp, self.nyp), dtype=self.np_dtype)
-        qpad[:, ngh:ngh + mesh.nx, ngh:ngh + mesh.ny] = q0.astype(self.np_dtype, copy=False)
-        self._buf[0][:, :, :self.nyp].copy_(torch.from_numpy(qpad))
-        bpad = np.zeros((self.nxp, self.nyp), dtype=self.np_dtype)
-        bpad[ngh:ngh + mesh.nx, ngh:ngh + mesh.ny] = b.astype(self.np_dtype, copy=False)
-        self._pad_bed(bpad)
+        # inputs go to the device as they are (one copy each, converted there); padding and
+        # the finiteness check run on the device
+        q_dev = _to_device(q0, dev, td)
+        b_dev = _to_device(b, dev, td)
+        bad = [what for what, arr in (("the bed", b_dev), ("the initial state q0", q_dev))
+               if not bool(torch.isfinite(arr).all())]
+        if bad:
+            raise ValueError(f"Solver2D: {bad[0]} holds non-finite values (NaN or inf)")
+        self._buf[0][:, ngh:ngh + mesh.nx, ngh:ngh + mesh.ny] = q_dev
         self._b = torch.zeros((self.nxp, self.pitch), dtype=td, device=dev)
-        self._b[:, :self.nyp].copy_(torch.from_numpy(bpad))
-        self._b_host = bpad
+        self._b[ngh:ngh + mesh.nx, ngh:ngh + mesh.ny] = b_dev
+        self._pad_bed(self._b[:, :self.nyp])
+        del q_dev, b_dev
         self._mask = None
         self.inside_mask_interior = None
         self._ncls = None
@@ -165,7 +176,8 @@ class Solver2D:
 
     # ------------------------------------------------------------------ layout
     def _pad_bed(self, bpad):
-        """Ghost bed as the ghost state is filled (solver.py:1466-1484)."""
+        """Ghost bed as the ghost state is filled (solver.py:1466-1484); `bpad` is the
+        padded (nxp, nyp) bed, a NumPy array or a device tensor view, filled in place."""
         ngh = self.mesh.ngh
         if self.cfg.bc_x == "periodic":
             bpad[:ngh, :] = bpad[-2 * ngh:-ngh, :]
@@ -174,8 +186,8 @@ class Solver2D:
             bpad[:ngh, :] = bpad[ngh:ngh + 1, :]
             bpad[-ngh:, :] = bpad[-ngh - 1:-ngh, :]
         if self.cfg.bc_y == "periodic":
-            bpad[:, :ngh] = bpad[:, -2 * ngh:-ngh]
-            bpad[:, -ngh:] = bpad[:, ngh:2 * ngh]
+            bpad[:, :ngh] = bpad[:, -2 * ngh:-ngh].clone() if torch.is_tensor(bpad) else bpad[:, -2 * ngh:-ngh]
+            bpad[:, -ngh:] = bpad[:, ngh:2 * ngh].clone() if torch.is_tensor(bpad) else bpad[:, ngh:2 * ngh]
         else:
             bpad[:, :ngh] = bpad[:, ngh:ngh + 1]
             bpad[:, -ngh:] = bpad[:, -ngh - 1:-ngh]
