@@ -345,6 +345,8 @@ class CompressedSolver:
         self.warps, self.min_blocks, self.segments = 0, 0, 0
         from . import autotune
         best = autotune.load(autotune.kind("flat", self.arith), self.nslots)
+        if not best and self.nslots >= 1 << 20:
+            self.min_blocks = 4          # untuned: a register cap (64) rather than the compiler's ~100
         if best:
             self.warps, self.min_blocks = int(best["warps"]), int(best["min_blocks"])
             g = int(best.get("segments", 0))

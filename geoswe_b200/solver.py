@@ -129,12 +129,14 @@ class Solver2D:
         self.pitch = _pitch(self.nyp, self.np_dtype.itemsize)
         self.arith = L.ARITH_FAST if cfg.arith == "fast" else L.ARITH_EXACT
         self._tile_rows, self._warps, self._min_blocks = int(tile_rows), int(warps), int(min_blocks)
-        if autotuned and not (tile_rows or warps or min_blocks):
+        if autotuned and not (tile_rows or warps or min_blocks) and self.np_dtype == np.float32:
             from . import autotune
             best = autotune.load(autotune.kind("dense", self.arith), mesh.nx * mesh.ny)
-            if best and self.np_dtype == np.float32:
+            if best:
                 self._tile_rows, self._warps = int(best["tile_rows"]), int(best["warps"])
                 self._min_blocks = int(best["min_blocks"])
+            elif mesh.nx * mesh.ny >= 1 << 20:
+                self._min_blocks = 4     # untuned: the 64-register cap every large-grid tuning has chosen
         self._use_graphs = bool(use_graphs)
         dev, td = self.device, self.t_dtype
         self._buf = [torch.zeros((3, self.nxp, self.pitch), dtype=td, device=dev) for _ in range(2)]
