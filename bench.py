@@ -127,7 +127,7 @@ def make_solver(z, cls, n, dtype="float32", arith="exact"):
 # (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on the 4096 x 4096 case of
 # the same workload and scaled to a launch here by the cells it processes (the traffic
 # is proportional to the cells: no re-reads beyond the bricks' halo rows).
-DRAM_BYTES_PER_CELL = {"dense": 39.04, "flat": 32.24}
+DRAM_BYTES_PER_CELL = {"dense": 36.66, "flat": 32.24}
 
 
 def max_over_ranks(x, device):
