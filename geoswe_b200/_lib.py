@@ -34,7 +34,7 @@ i32, i64, u32, u64, f64 = C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_doub
 class GswLoopState(C.Structure):
     _fields_ = [("t", f64), ("dt", f64), ("t_new", f64), ("steps", i64), ("lam_bits", u64),
                 ("lam_used", f64), ("dt_f32", C.c_float), ("rain_idx", i32), ("done", i32),
-                ("error", i32), ("pending", i32), ("ticket", u32), ("reserved", i32 * 2)]
+                ("error", i32), ("pending", i32), ("reserved", i32 * 3)]
 
 
 class GswDtParams(C.Structure):
@@ -54,8 +54,7 @@ class GswDenseArgs(C.Structure):
                 ("friction_kind", i32), ("n_cls", vp), ("n_cls_pitch", i64), ("n_tab", vp),
                 ("n_tab_len", i32), ("n_field", vp), ("vcap", f64), ("quadratic", i32),
                 ("keep_h", i32), ("max_h", vp), ("cfl_skip", vp), ("h_cfl", f64),
-                ("tile_rows", i32), ("warps", i32), ("min_blocks", i32), ("arith", i32),
-                ("dt_params", vp)]
+                ("tile_rows", i32), ("warps", i32), ("min_blocks", i32), ("arith", i32)]
 
 
 class GswBcArgs(C.Structure):
@@ -87,7 +86,7 @@ class GswFlatArgs(C.Structure):
                 ("linf", i32), ("rain_kind", i32), ("state", vp), ("lam_target", vp), ("rain", vp),
                 ("ngh", i32), ("nx", i32), ("ny", i32), ("n_tab_len", i32), ("n_cls", vp), ("n_tab", vp),
                 ("vcap", f64), ("quadratic", i32), ("keep_h", i32), ("max_h", vp), ("rain_lookup", vp),
-                ("rain_ncol", i32), ("segments", i32), ("dt_params", vp)]
+                ("rain_ncol", i32), ("segments", i32)]
 
 
 class GswFlatInflowArgs(C.Structure):

@@ -788,21 +788,15 @@ class CompressedSolver:
         _host_lib()
 
         forced = bool(self._forcing)
-        # with nothing after the step that reads the loop time (ring stage, forcings), the
-        # step kernel's last block evaluates the next dt: one launch fewer per step
-        fused = not forced and self._ring is None
-        per_step = 2 + len(self._inflows) + (self._ring is not None) + 3 * forced - int(fused)
+        per_step = 2 + len(self._inflows) + (self._ring is not None) + 3 * forced
 
         def one_step(k_parity):
             s = _stream()
-            if not fused:
-                L.call("gsw_dt_finalize_dev", _ptr(self._dtp_dev), _ptr(self._state), s)
+            L.call("gsw_dt_finalize_dev", _ptr(self._dtp_dev), _ptr(self._state), s)
             src, dst = self._q[k_parity], self._q[1 - k_parity]
             for f in self._inflows:             # inlet ghosts at t_n, before the step
                 L.call("gsw_flat_inflow_apply", C.byref(self._inflow_args(f, src)), s)
             a = self._args(src, dst)
-            if fused:
-                a.dt_params = _ptr(self._dtp_dev)
             if forced:                          # the wave speed is taken after the forcings
                 a.lam_target = None
             L.call("gsw_flat_step", C.byref(a), s)
@@ -820,15 +814,11 @@ class CompressedSolver:
                 one_step(k % 2)
             return per_step * K
 
-        if fused:                                # the first step's dt
-            L.call("gsw_dt_finalize_dev", _ptr(self._dtp_dev), _ptr(self._state), _stream())
-            self.kernel_launches += 1
         if start == 1:
             # one step outside the window, so every captured window starts on buffer 0
             one_step(1)
             self.kernel_launches += per_step
-        key = (K, fused, self._rain_kind, len(self._inflows), self._ring is not None, self.warps, self.min_blocks,
-               self.segments,
+        key = (K, self._rain_kind, len(self._inflows), self._ring is not None, self.warps, self.min_blocks, self.segments,
                tuple(sorted(self._forcing)))
         g, per = _cached_graph(self._graph_cache, key, one_window, self.device)
         self.kernel_launches += 1
@@ -839,10 +829,8 @@ class CompressedSolver:
             if st.done:
                 break
             if every > 0.0:
-                # unfused: a pending step has run (its dt came first); fused: the step
-                # kernel committed its step and `pending` is the next, not yet run
-                executed = int(st.steps) + (0 if fused else int(st.pending))
-                t_now = float(st.t_new) if (st.pending and not fused) else float(st.t)
+                executed = int(st.steps) + int(st.pending)
+                t_now = float(st.t_new) if st.pending else float(st.t)
                 if t_now >= next_ckpt:
                     self._write_checkpoint(ckpt_dir, self._q[(start + executed) % 2], t_now, steps0 + executed)
                     while next_ckpt <= t_now:

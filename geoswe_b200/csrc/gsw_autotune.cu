@@ -3,8 +3,8 @@
 // No counterpart in the reference, whose kernels have fixed launch shapes. Each call
 // times the step at every shape of a fixed search space with CUDA events on the
 // caller's stream and buffers, and returns the fastest. The step's outputs serve as
-// scratch; the wave-speed target, the running maximum and a fused dt rule are left
-// out of the timed launches (NULL) and the loop state is only read. Results are kept
+// scratch; the wave-speed target and the running maximum are left untouched (the
+// timed launches get NULL for both) and the loop state is only read. Results are kept
 // per (device, kernel family, arithmetic, binary size, size class) in a table guarded
 // by a mutex, so a second call for the same class returns without launching.
 #include "gsw_common.cuh"
@@ -82,7 +82,6 @@ extern "C" int gsw_dense_autotune(const GswDenseArgs* a, int32_t reps, int32_t u
                 GswDenseArgs b = *a;
                 b.lam_target = nullptr;
                 b.max_h = nullptr;
-                b.dt_params = nullptr;
                 b.tile_rows = tr; b.warps = w; b.min_blocks = mb;
                 const float ms = time_shape([&] { return gsw_dense_step(&b, stream); }, reps, s, e0, e1);
                 if (ms < 0.0f) continue;
@@ -128,7 +127,6 @@ extern "C" int gsw_flat_autotune(const GswFlatArgs* a, int32_t reps, int32_t use
                 GswFlatArgs b = *a;
                 b.lam_target = nullptr;
                 b.max_h = nullptr;
-                b.dt_params = nullptr;
                 b.warps = w; b.min_blocks = mb; b.segments = g;
                 const float ms = time_shape([&] { return gsw_flat_step(&b, stream); }, reps, s, e0, e1);
                 if (ms < 0.0f) continue;

@@ -131,29 +131,6 @@ __device__ __forceinline__ void dt_finalize_one(const GswDtParams& p, GswLoopSta
     if (p.dt_log != nullptr) p.dt_log[s->steps] = dt;
 }
 
-// The end of a fused step that also evaluates the next dt (gsw_dt_finalize_dev folded
-// into the step): every block calls this after its wave-speed atomicMax into
-// st->lam_bits; the block that arrives last (st->ticket) commits the step and evaluates
-// the next dt from the reduced wave speed, then clears the ticket for the next launch.
-// Every thread of the block must call it.
-__device__ __forceinline__ void step_tail_finalize(const GswDtParams* dtp, GswLoopState* st) {
-    __shared__ int s_last;
-    __syncthreads();
-    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-    if (tid == 0) {
-        __threadfence();
-        const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
-        s_last = (atomicAdd(&st->ticket, 1u) == nblocks - 1u);
-    }
-    __syncthreads();
-    if (s_last && tid == 0) {
-        __threadfence();
-        const unsigned long long lb = atomicAdd((unsigned long long*)&st->lam_bits, 0ull);  // coherent read
-        st->ticket = 0u;
-        dt_finalize_one(*dtp, st, lb);
-    }
-}
-
 }  // namespace gsw
 
 #define GSW_CHECK_ABI(a)                                                                     \

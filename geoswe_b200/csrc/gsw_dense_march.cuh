@@ -38,7 +38,6 @@ struct DenseK {
     T h_cfl;
     int tile_rows;
     T g_recip;                   // RN(1/g) for the star depth's h / g, or 0 (gsw_core.cuh div_g)
-    const GswDtParams* dtp;      // fused dt rule (step only), or null
 };
 
 template <typename T>
@@ -206,7 +205,6 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
         }
     }
     if (STEP && p.lam != nullptr) block_max_to(lam_local, p.lam);
-    if (STEP && p.dtp != nullptr) step_tail_finalize(p.dtp, const_cast<GswLoopState*>(p.st));
 }
 
 template <typename T>
@@ -231,9 +229,6 @@ inline int fill_dense(const GswDenseArgs* a, DenseK<T>& k, bool step) {
     }
     k.g = (T)a->g; k.h_min = (T)a->h_min;
     k.g_recip = sizeof(T) == 4 ? (T)div_const_recip((float)a->g) : (T)0;
-    k.dtp = step ? a->dt_params : nullptr;
-    if (k.dtp && (!a->state || a->lam_target != &a->state->lam_bits))
-        return set_error(GSW_ERR_INVALID, "dense step: a fused dt rule needs lam_target = &state->lam_bits");
     k.st = a->state; k.lam = (unsigned long long*)a->lam_target;
     k.rain_kind = a->rain_kind; k.rain = (const T*)a->rain;
     k.friction_kind = a->friction_kind; k.ncls = a->n_cls; k.cpitch = a->n_cls_pitch;

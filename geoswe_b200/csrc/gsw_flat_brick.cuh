@@ -42,10 +42,7 @@ __host__ __device__ __forceinline__ int auto_segments(int64_t bricks, int64_t wa
 
 // For the flat kernels' argument struct
 template <typename T>
-struct FlatK {
-    FlatMesh<T> m; FlatPhys<T> ph; const GswLoopState* st; unsigned long long* lam; int segs;
-    const GswDtParams* dtp;      // fused dt rule (step only), or null
-};
+struct FlatK { FlatMesh<T> m; FlatPhys<T> ph; const GswLoopState* st; unsigned long long* lam; int segs; };
 
 // Slot of brick-relative (row, lane). Lanes 0/31 of the rows above/below the brick are
 // never used by an output cell; they read the zero brick.

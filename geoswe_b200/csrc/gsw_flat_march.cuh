@@ -33,7 +33,6 @@ __global__ void __launch_bounds__(256, MINB) flat_march_kernel(FlatK<T> p) {
         lam_local = flat_brick<T, STEP>(p.m, p.ph, bidx, seg * p.m.bh / p.segs, (seg + 1) * p.m.bh / p.segs,
                                         dt, rate, frame);
     if (STEP && p.lam != nullptr) block_max_to(lam_local, p.lam);
-    if (STEP && p.dtp != nullptr) step_tail_finalize(p.dtp, const_cast<GswLoopState*>(p.st));
 }
 
 template <typename T>
@@ -56,9 +55,6 @@ inline int fill_flat(const GswFlatArgs* a, FlatK<T>& k, bool step) {
     ph.lookup = a->rain_lookup; ph.ncol = a->rain_ncol;
     ph.g_recip = sizeof(T) == 4 ? (T)div_const_recip((float)a->g) : (T)0;
     k.st = a->state; k.lam = (unsigned long long*)a->lam_target;
-    k.dtp = step ? a->dt_params : nullptr;
-    if (k.dtp && (!a->state || a->lam_target != &a->state->lam_bits))
-        return set_error(GSW_ERR_INVALID, "flat step: a fused dt rule needs lam_target = &state->lam_bits");
     k.segs = a->segments > 0 ? a->segments : auto_segments(a->n_bricks, (int64_t)sm_count() * 24, a->brick_h);
     if (k.segs != 1 && k.segs != 2 && k.segs != 4) return set_error(GSW_ERR_INVALID, "flat: segments must be 0, 1, 2 or 4");
     if (a->brick_h % k.segs != 0) return set_error(GSW_ERR_INVALID, "flat: brick_h must be a multiple of segments");

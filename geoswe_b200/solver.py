@@ -510,9 +510,8 @@ class Solver2D:
         a.state = _ptr(self._state)
         L.call("gsw_inflow_apply", C.byref(a), s)
 
-    def _launch_step(self, k_parity: int, T, fused_dt=False):
-        """Ghost fill, inflow, fused step and stage for the buffer pair (k, 1-k). With
-        `fused_dt` the step kernel also evaluates the next dt (no stage boundaries)."""
+    def _launch_step(self, k_parity: int, T):
+        """Ghost fill, inflow, fused step and stage for the buffer pair (k, 1-k)."""
         src, dst = self._buf[k_parity], self._buf[1 - k_parity]
         s = _stream()
         L.call("gsw_bc_fill", C.byref(self._bc_args(src)), s)
@@ -520,10 +519,7 @@ class Solver2D:
             self._launch_inflow(inl, src, s)
         n = 2 + len(T.inflows) + 2 * len(T.stages) + (1 if len(T.stages) > 1 else 0)
         self._counting += n
-        a = self._dense_args(src, dst, T)
-        if fused_dt:
-            a.dt_params = _ptr(self._dtp_dev)
-        L.call("gsw_dense_step", C.byref(a), s)
+        L.call("gsw_dense_step", C.byref(self._dense_args(src, dst, T)), s)
         multi = len(T.stages) > 1
         for st in T.stages:
             a = L.GswStageArgs()
@@ -715,15 +711,11 @@ class Solver2D:
             self._dtp_dev = torch.zeros(C.sizeof(L.GswDtParams), dtype=torch.uint8, device=self.device)
         L.call("gsw_dt_params_upload", C.byref(p), _ptr(self._dtp_dev), _stream())
         start_cur = self._cur
-        # with no stage boundary (whose kernels read the step's end time after the step),
-        # the step kernel's last block evaluates the next dt: one launch fewer per step
-        fused = not T.stages
 
         def one_step(k_parity):
-            if not fused:
-                L.call("gsw_dt_finalize_dev", _ptr(self._dtp_dev), _ptr(self._state), _stream())
-                self._counting += 1
-            self._launch_step(k_parity, T, fused_dt=fused)
+            L.call("gsw_dt_finalize_dev", _ptr(self._dtp_dev), _ptr(self._state), _stream())
+            self._counting += 1
+            self._launch_step(k_parity, T)
 
         def one_window():
             self._counting = 0
@@ -732,16 +724,13 @@ class Solver2D:
             return self._counting
 
         lead = 0
-        if fused:                            # the first step's dt
-            L.call("gsw_dt_finalize_dev", _ptr(self._dtp_dev), _ptr(self._state), _stream())
-            lead += 1
         if start_cur == 1:
             # one step outside the window, so every captured window starts on buffer 0
             self._counting = 0
             one_step(1)
-            lead += self._counting
+            lead = self._counting
         if self._use_graphs:
-            g, per = _cached_graph(self._graph_cache, (K, fused, self._tile_rows, self._warps, self._min_blocks),
+            g, per = _cached_graph(self._graph_cache, (K, self._tile_rows, self._warps, self._min_blocks),
                                    one_window, self.device)
 
             def run_window():

@@ -105,8 +105,7 @@ typedef struct GswLoopState {
     int32_t  done;       /* 1: loop condition false, step cap reached, or error */
     int32_t  error;      /* 0 or a GSW_ERR_* code raised on the device */
     int32_t  pending;    /* 1: t_new/steps not committed yet */
-    uint32_t ticket;     /* block-arrival counter of a step that evaluates the next dt (zero between launches) */
-    int32_t  reserved[2];
+    int32_t  reserved[3];
 } GswLoopState;
 
 /* Time-step rule (replaces the host arithmetic of Solver2D.run / cfl_dt /
@@ -171,12 +170,6 @@ typedef struct GswDenseArgs {
     int32_t  warps;            /* warps per block (0: default 4) */
     int32_t  min_blocks;       /* register cap: 0 (compiler's choice), 3 (80 regs), 4 (64 regs) or 5 (48 regs) */
     int32_t  arith;            /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST (GSW_F32 step only) */
-    /* Fused dt rule (step only; NULL: none): device GswDtParams. The step's last block
-       then does what gsw_dt_finalize_dev would do before the next step (commit this
-       step, test the loop condition, evaluate the next dt from lam_target, which must
-       be &state->lam_bits), using state->ticket. Only for loops with nothing between
-       steps that reads the loop time after the step (a stage boundary does). */
-    const GswDtParams* dt_params;
 } GswDenseArgs;
 
 /* One fused step over the interior: SRM-HLLC residual, rain, forward Euler,
@@ -296,8 +289,6 @@ typedef struct GswFlatArgs {
     int32_t  segments;         /* warps per brick: 1 (one warp walks the brick's rows), 2 or 4 (each walks
                                   brick_h / segments rows: shorter per-warp latency for small meshes),
                                   0 (chosen from the brick count against the warps the GPU runs at once) */
-    const GswDtParams* dt_params; /* fused dt rule, as GswDenseArgs.dt_params (no ring stage or forcings
-                                     after the step) */
 } GswFlatArgs;
 
 /* Discharge inlet of the compressed mesh: one ghost (ring) slot per inlet cell, next to
