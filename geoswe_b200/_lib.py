@@ -96,7 +96,7 @@ class GswFlatInflowArgs(C.Structure):
 
 
 class GswFlatAdjArgs(C.Structure):
-    _fields_ = [("abi_version", u32), ("reserved0", i32), ("f", GswFlatArgs),
+    _fields_ = [("abi_version", u32), ("min_blocks", i32), ("f", GswFlatArgs),
                 ("lam_in0", vp), ("lam_in1", vp), ("lam_in2", vp), ("lam_out0", vp), ("lam_out1", vp),
                 ("lam_out2", vp), ("rbar0", vp), ("rbar1", vp), ("rbar2", vp), ("n_bar", vp), ("rate_bar", vp)]
 

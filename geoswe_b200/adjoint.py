@@ -170,6 +170,7 @@ class FlatAdjoint:
                              "with arith='exact'")
         self.cs = cs
         self.dev = cs.device
+        self.adj_min_blocks = 8          # register cap of the binary32 reverse kernels: 0, 6 (80) or 8 (64 regs)
         self.code = L.F32 if dtype == "float32" else L.F64
         self.td = torch.float32 if dtype == "float32" else torch.float64
         self.N, self.K, self.S = int(n_steps), int(window), int(snapshots)
@@ -487,6 +488,7 @@ class FlatAdjoint:
             L.call("gsw_flat_inflow_apply", C.byref(self._inflow_args(q)), s)
         a = L.GswFlatAdjArgs()
         a.abi_version = L.ABI_VERSION
+        a.min_blocks = self.adj_min_blocks if self.code == L.F32 else 0
         a.f = self._flat_args(q)
         lin, lout = self._lam[1], self._lam[0]
         a.lam_in0, a.lam_in1, a.lam_in2 = _ptr(lin[0]), _ptr(lin[1]), _ptr(lin[2])

@@ -76,8 +76,8 @@ __device__ __forceinline__ void load_state(const FlatMesh<T>& m, int64_t s, Cell
 }
 
 // ---------------------------------------------------------------------------- A
-template <typename T>
-__global__ void __launch_bounds__(128) adj_tail_kernel(AdjK<T> p) {
+template <typename T, int MINB>
+__global__ void __launch_bounds__(128, MINB) adj_tail_kernel(AdjK<T> p) {
     __shared__ double s_nbar[256];
     __shared__ double s_rate[8];
     const int tid = threadIdx.x + 32 * threadIdx.y;
@@ -178,8 +178,8 @@ __global__ void __launch_bounds__(128) adj_tail_kernel(AdjK<T> p) {
 }
 
 // ---------------------------------------------------------------------------- B
-template <typename T>
-__global__ void __launch_bounds__(128) adj_face_kernel(AdjK<T> p) {
+template <typename T, int MINB>
+__global__ void __launch_bounds__(128, MINB) adj_face_kernel(AdjK<T> p) {
     const FlatMesh<T>& m = p.m;
     const FlatPhys<T>& ph = p.ph;
     const int lane = threadIdx.x;
@@ -384,9 +384,17 @@ static int launch_adj(const GswFlatAdjArgs* a, cudaStream_t s) {
     const int W = 4;
     const int64_t blocks = (k.m.nb + W - 1) / W;
     if (blocks > 0x7fffffffLL) return set_error(GSW_ERR_INVALID, "adjoint: too many bricks");
-    adj_tail_kernel<T><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
+    // register cap of the binary32 reverse kernels: 0 (compiler's choice), 6 (80) or 8 (64 registers)
+    const int mb = sizeof(T) == 4 ? a->min_blocks : 0;
+    if (mb != 0 && mb != 6 && mb != 8) return set_error(GSW_ERR_INVALID, "adjoint: min_blocks must be 0, 6 or 8");
+    const dim3 grid((unsigned)blocks), block(32, W);
+    if (mb == 6) adj_tail_kernel<T, sizeof(T) == 4 ? 6 : 1><<<grid, block, 0, s>>>(k);
+    else if (mb == 8) adj_tail_kernel<T, sizeof(T) == 4 ? 8 : 1><<<grid, block, 0, s>>>(k);
+    else adj_tail_kernel<T, 1><<<grid, block, 0, s>>>(k);
     if (int rc = check_launch("adj_tail")) return rc;
-    adj_face_kernel<T><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
+    if (mb == 6) adj_face_kernel<T, sizeof(T) == 4 ? 6 : 1><<<grid, block, 0, s>>>(k);
+    else if (mb == 8) adj_face_kernel<T, sizeof(T) == 4 ? 8 : 1><<<grid, block, 0, s>>>(k);
+    else adj_face_kernel<T, 1><<<grid, block, 0, s>>>(k);
     return check_launch("adj_face");
 }
 

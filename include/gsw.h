@@ -402,7 +402,7 @@ GSW_API int gsw_bricks_build(const uint8_t* stored, int nxp, int nyp, int brick_
 /* ------------------------------------------------------------------------- */
 typedef struct GswFlatAdjArgs {
     uint32_t abi_version;
-    int32_t  reserved0;
+    int32_t  min_blocks;  /* register cap of the binary32 reverse kernels: 0 (compiler's), 6 (80), 8 (64 regs) */
     GswFlatArgs f;     /* the step being reversed: q* = the state it read (inlet ghosts written),
                           state = its dt, rain frame and step index (steps); qn*, max_h unused */
     const void* lam_in0; const void* lam_in1; const void* lam_in2;   /* adjoint of the new state */
