@@ -127,7 +127,27 @@ def make_solver(z, cls, n, dtype="float32", arith="exact"):
 # (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on the 4096 x 4096 case of
 # the same workload and scaled to a launch here by the cells it processes (the traffic
 # is proportional to the cells: no re-reads beyond the bricks' halo rows).
-DRAM_BYTES_PER_CELL = {"dense": 36.66, "flat": 32.24}
+DRAM_BYTES_PER_CELL = {"dense": 36.66, "flat": 32.13, "flat_compressed": 48.89}
+
+# Warp instructions per updated cell of the step kernels: ncu smsp__inst_executed.sum of
+# one launch at 4096 x 4096 (tuned shape) divided by the cells it updates. With the SM
+# clock they give the instruction-issue roofline the step kernels are bound by: one warp
+# instruction per scheduler per cycle, four schedulers per SM.
+INST_PER_CELL = {"dense": 38.73, "dense_fast": 23.71, "flat_tidal": 34.23, "flat_compressed": 46.88}
+
+
+def issue_roofline(kind, cells, kern_ms, clocks):
+    """Issue-rate roofline of a step kernel: achieved warp instructions per second (the
+    ncu count per cell x cells / the CUDA-event launch time) against 4 x SMs x the
+    sampled SM clock (max clock when no sample)."""
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz") or 1965.0
+    peak = 4.0 * sms * mhz * 1e6
+    achieved = INST_PER_CELL[kind] * cells / (kern_ms / 1e3)
+    return {"bound": "instruction issue", "warp_inst_per_cell": INST_PER_CELL[kind],
+            "achieved": achieved, "peak": peak, "unit": "warp instructions/s", "frac": achieved / peak,
+            "sm_mhz": mhz, "source": "ncu smsp__inst_executed.sum per cell (4096 x 4096, profiles/)"}
 
 
 def max_over_ranks(x, device):
@@ -185,7 +205,9 @@ def measure_dense(args, z, cls, n, world, arith="exact"):
     ms = e0.elapsed_time(e1)
     launches = s.kernel_launches - l0
     assert steps == args.steps, (steps, args.steps)
+    torch.cuda.nvtx.range_push("kernel_timing")        # the launches an ncu capture targets
     kern_ms = time_step_kernel(s, reps=args.kernel_reps)
+    torch.cuda.nvtx.range_pop()
     shape = {"tile_rows": s._tile_rows or "auto", "warps": s._warps or 4, "min_blocks": s._min_blocks}
     del s
     torch.cuda.empty_cache()
@@ -222,6 +244,7 @@ def run_gsw(args, rank, world):
                      "traffic_unit": "GB per launch (ncu, 4096x4096 capture scaled by cells)",
                      "kernel": "dense_march_kernel<float,true>", "kernel_ms": kern_ms,
                      "bytes_per_cell": bpc, "peak_source": peak_kind},
+        "issue": issue_roofline("dense", cells, kern_ms, m["clocks"]),
         "clocks": m["clocks"],
         "arith": "exact (IEEE, bit-identical to the reference kernel without FMA contraction)",
         "launch_shape": m["shape"],
@@ -240,6 +263,7 @@ def run_gsw(args, rank, world):
             "roofline": {"bound": "hbm", "achieved": f_ach, "peak": peak, "unit": "GB/s", "frac": f_ach / peak,
                          "kernel": "gsw_fast::dense_march_kernel<float,true>", "kernel_ms": f["kern_ms"],
                          "peak_source": peak_kind},
+            "issue": issue_roofline("dense_fast", cells, f["kern_ms"], f["clocks"]),
             "clocks": f["clocks"], "launch_shape": f["shape"]}
     if rank == 0 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args)
@@ -552,7 +576,9 @@ def run_compressed(args):
     wet = float((r_dense[0] != 0).float().mean())
     del r_dense, r_flat
     tune = None
-    if not args.no_tune:
+    if args.flat_shape:
+        cs.warps, cs.min_blocks, cs.segments = (int(v) for v in args.flat_shape.split(","))
+    elif not args.no_tune:
         best, table = autotune.tune_flat(cs, reps=4)
         tune = {"best": best}
     cs.run(t_end=1e12, max_steps=args.warmup, window=cs._window_size())
@@ -564,7 +590,9 @@ def run_compressed(args):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    torch.cuda.nvtx.range_push("kernel_timing")        # the launches an ncu capture targets
     kern_ms = autotune.time_flat_step(cs, reps=args.kernel_reps)
+    torch.cuda.nvtx.range_pop()
     cells = int(cs.N_active)
     peak, peak_kind = _peaks()
     achieved = 38.0 * cells / (kern_ms / 1e3) / 1e9
@@ -577,7 +605,10 @@ def run_compressed(args):
             "residual_bit_identical_to_dense": identical, "residual_nonzero_fraction": wet,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "kernel_ms": kern_ms, "bytes_per_cell": 38,
+                         "traffic": DRAM_BYTES_PER_CELL["flat_compressed"] * cells / 1e9,
+                         "traffic_unit": "GB per launch (ncu, 4096x4096 capture scaled by active cells)",
                          "peak_source": peak_kind},
+            "issue": issue_roofline("flat_compressed", cells, kern_ms, None),
             "gpu_launches": int(cs.kernel_launches - l0),
             "launch_shape": {"warps": cs.warps or 4, "min_blocks": cs.min_blocks, "segments": cs.segments or "auto"},
             "autotune": tune}
@@ -629,9 +660,11 @@ def run_tidal(args):
     cs.set_ring(dict(i=ri, j=rj, bed=rbed, wg=np.ones((ri.size, 1), np.float32), NG=1, n=int(ri.size),
                      t_common=t_c, stage_all=stage))
     build_s = time.perf_counter() - t0
+    if args.flat_shape:
+        cs.warps, cs.min_blocks, cs.segments = (int(v) for v in args.flat_shape.split(","))
     cs.run(t_end=1e12, max_steps=args.warmup)
     tune = None
-    if not args.no_tune:
+    if not args.no_tune and not args.flat_shape:
         best, table = autotune.tune_flat(cs, reps=4)
         tune = {"best": best, "table": table}
     cs.run(t_end=1e12, max_steps=args.warmup, window=cs._window_size())   # captures the timed window's graph
@@ -647,7 +680,9 @@ def run_tidal(args):
     clocks = clk.stop()
     ms = e0.elapsed_time(e1)
     launches = cs.kernel_launches - l0
+    torch.cuda.nvtx.range_push("kernel_timing")        # the launches an ncu capture targets
     kern_ms = autotune.time_flat_step(cs, reps=args.kernel_reps)
+    torch.cuda.nvtx.range_pop()
     cells = int(cs.N_active)
     peak, peak_kind = _peaks()
     achieved = 38.0 * cells / (kern_ms / 1e3) / 1e9
@@ -665,6 +700,7 @@ def run_tidal(args):
                          "kernel": "flat_march_kernel<float,1>",
                          "kernel_ms": kern_ms, "bytes_per_cell": 38, "peak_source": peak_kind,
                          "brick_bytes_GBs": stored_bytes / (kern_ms / 1e3) / 1e9},
+            "issue": issue_roofline("flat_tidal", cells, kern_ms, clocks) if args.arith == "exact" else None,
             "gpu_launches": int(launches), "clocks": clocks, "build_s": build_s, "simulated_s": cs.t,
             "launch_shape": {"warps": cs.warps or 4, "min_blocks": cs.min_blocks, "segments": cs.segments or 1},
             "autotune": tune}
@@ -741,6 +777,8 @@ def main():
                     help="step arithmetic of the tidal and ensemble cases")
     ap.add_argument("--exact-shape", default="", help="dense launch shape 'tile_rows,warps,min_blocks' (no tuning)")
     ap.add_argument("--fast-shape", default="", help="the same for the fast arithmetic")
+    ap.add_argument("--flat-shape", default="", help="compressed-mesh launch shape 'warps,min_blocks,segments' "
+                                                     "(no tuning)")
     ap.add_argument("--err-n", type=int, default=96, help="fp64 depth-error sample size (0: skip)")
     ap.add_argument("--err-t-end", type=float, default=600.0)
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
