@@ -351,8 +351,8 @@ def run_ensemble(args):
     if not args.no_tune:                     # the plain solver gets its own tuned launch shape
         big = max(loop_members, key=lambda m: m.nslots)
         best, _ = autotune.tune_flat(big, store=False)
-        for m in loop_members:
-            m.warps, m.min_blocks, m.segments = best["warps"], best["min_blocks"], best["segments"]
+        for m in loop_members:       # warps per brick stay automatic: they follow each member's size
+            m.warps, m.min_blocks = best["warps"], best["min_blocks"]
         loop_shape = best
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()

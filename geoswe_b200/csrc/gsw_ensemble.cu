@@ -20,6 +20,7 @@ __global__ void ensemble_finalize_kernel(GswEnsembleArgs a) {
     if (a.run != nullptr) build_run_list(a, threadIdx.x, blockDim.x);
     if (threadIdx.x == 0) {
         a.scratch[0] = 0u;
+        a.scratch[1] = 0u;
         *a.all_done = (s_open == 0) ? 1 : 0;
     }
 }

@@ -9,7 +9,8 @@
 // keep their own CFL dt with no grid-wide barrier and no host round trip; a member that
 // reaches its end time drops out while the others continue. With a running-member list
 // (GswEnsembleArgs.run) warps walk only the running members' bricks, and the last block
-// rebuilds the list when a member finishes.
+// rebuilds the list when a member finishes. Warps take their next brick from a counter
+// in scratch memory, so the uneven bricks of uneven members balance over the grid.
 //
 // Included by gsw_ensemble.cu (exact arithmetic) and gsw_fast.cu (fast arithmetic,
 // with namespace gsw renamed).
@@ -82,7 +83,14 @@ __global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArg
     const int S = a.segments > 0 ? a.segments                // row segments per brick, or by the work in flight
                                  : auto_segments(bricks, (int64_t)gridDim.x * W, m.bh);
     const int64_t total = bricks * S;
-    for (int64_t item = (int64_t)blockIdx.x * W + threadIdx.y; item < total; item += (int64_t)gridDim.x * W) {
+    // work items (brick, row segment) are taken from a counter (scratch[1]) as warps free
+    // up, so bricks of uneven cost balance across the fixed persistent grid
+    unsigned int* next_item = a.scratch + 1;
+    for (;;) {
+        long long got = 0;
+        if (lane == 0) got = (long long)atomicAdd(next_item, 1u);
+        const int64_t item = __shfl_sync(0xffffffffu, got, 0);
+        if (item >= total) break;
         const int64_t v = item / S;
         const int seg = (int)(item - v * S);
         int64_t b;
@@ -141,7 +149,8 @@ __global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArg
     __syncthreads();
     if (listed && s_finished && s_open > 0) build_run_list(a, tid, nth);   // block-uniform condition
     if (tid == 0) {
-        a.scratch[0] = 0u;
+        a.scratch[0] = 0u;           // every block has passed its loop: both counters back to zero
+        a.scratch[1] = 0u;
         *a.all_done = (s_open == 0) ? 1 : 0;
     }
 }
@@ -154,6 +163,7 @@ inline int launch_ensemble_step(const GswEnsembleArgs* a, cudaStream_t st) {
     const int S = a->segments > 0 ? a->segments : 1;
     if ((S != 1 && S != 2 && S != 4) || a->brick_h % S != 0 || a->segments < 0)
         return set_error(GSW_ERR_INVALID, "ensemble: segments must be 0, 1, 2 or 4 and divide brick_h");
+    if (a->n_bricks * 4 >= (int64_t)UINT32_MAX) return set_error(GSW_ERR_INVALID, "ensemble: too many bricks");
     FlatMesh<float> m;
     m.q0 = a->q0; m.q1 = a->q1; m.q2 = a->q2;
     m.o0 = a->qn0; m.o1 = a->qn1; m.o2 = a->qn2;

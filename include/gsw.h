@@ -478,7 +478,7 @@ typedef struct GswEnsembleArgs {
     float*   max_h;              /* per slot, or NULL */
     const GswMember* members;    /* device, n_members */
     GswLoopState* states;        /* device, n_members */
-    uint32_t* scratch;           /* device, >= 4 words, zero before the first step: block tickets */
+    uint32_t* scratch;           /* device, >= 4 words, zero before the first step: block and work counters */
     int32_t* all_done;           /* device int: 1 once every member is done */
     /* Running-member brick list (optional; NULL: every launch scans all bricks and skips
        finished members brick by brick). member_brick_off: device, n_members + 1, member
@@ -504,8 +504,8 @@ GSW_API int gsw_ensemble_step(const GswEnsembleArgs* a, void* stream);
 
 /* gsw_ensemble_step without caller scratch. No counterpart in the reference (its
  * scenarios run one after another, with no device scratch).
- * The step's scratch is its block ticket counter: GSW_ENS_SCRATCH_WORDS uint32 words,
- * zero before a launch and left at zero by it. This entry point keeps those words in a
+ * The step's scratch is its block ticket counter and its work-item counter:
+ * GSW_ENS_SCRATCH_WORDS uint32 words, zero before a launch and left at zero by it. This entry point keeps those words in a
  * static, 256-byte aligned device array of the library (GSW_ENS_STATIC_SCRATCH_WORDS
  * words per device) and ignores a->scratch; a requirement above that size is refused
  * with GSW_ERR_RANGE. It allocates nothing: on the first call on a device it looks the
@@ -513,7 +513,7 @@ GSW_API int gsw_ensemble_step(const GswEnsembleArgs* a, void* stream);
  * outside any stream capture. The array is shared by all callers on a device: calls
  * whose launches overlap in time (other streams, other threads) race on the ticket
  * counter and must be serialised by the caller. */
-#define GSW_ENS_SCRATCH_WORDS        1
+#define GSW_ENS_SCRATCH_WORDS        2
 #define GSW_ENS_STATIC_SCRATCH_WORDS 64
 GSW_API int gsw_ensemble_step_static(const GswEnsembleArgs* a, void* stream);
 
