@@ -6,7 +6,6 @@ importing a solver raises. There is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
-import os
 from pathlib import Path
 
 _PKG = Path(__file__).resolve().parent

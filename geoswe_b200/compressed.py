@@ -12,7 +12,6 @@ reached from the canonical order through ``slot_of`` (a permutation).
 from __future__ import annotations
 
 import ctypes as C
-import math
 import time
 import warnings
 from typing import Optional

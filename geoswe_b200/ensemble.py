@@ -10,7 +10,6 @@ captured in a CUDA graph. A member's trajectory is bit-identical to running it a
 from __future__ import annotations
 
 import ctypes as C
-import time
 from typing import Sequence
 
 import numpy as np

@@ -21,7 +21,6 @@ import torch
 
 from . import _lib as L
 from .config import Config
-from .forcing import RainfallForcing, StageBoundary
 from .mesh import Mesh2D
 
 

@@ -1,7 +1,7 @@
 """Small seeded cases shared by the tests (sizes the oracle finishes in seconds)."""
 import numpy as np
 
-from geoswe_b200.synthetic import fractal_bed, voronoi_classes, dam_break
+from geoswe_b200.synthetic import fractal_bed
 
 
 def rough_partly_dry(nx, ny, seed=7, dtype=np.float64):

@@ -4,7 +4,6 @@ Tests marked ``gpu`` need a CUDA device and the built libgsw.so; everything else
 on the CPU (the oracle against the reference's golden fixtures, host logic, the C ABI
 loading). The oracle under oracle/ is the checker only.
 """
-import os
 import sys
 from pathlib import Path
 

@@ -4,7 +4,6 @@ The oracle (oracle/gsw_oracle.c) evaluates the reference kernel text per cell wi
 four faces; the kernel shares each face between its two cells. Both use separately
 rounded IEEE operations, so every comparison here is exact equality (-0 == +0).
 """
-import math
 
 import numpy as np
 import pytest

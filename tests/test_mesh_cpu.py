@@ -6,7 +6,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from geoswe_b200.compressed import BRICK_PITCH, BRICK_W, build_bricks, build_tables
+from geoswe_b200.compressed import BRICK_W, build_bricks, build_tables
 from geoswe_b200.synthetic import dilate_cross
 
 M = np.load(Path(__file__).resolve().parent / "golden" / "reference_mesh.npz")
