@@ -142,6 +142,10 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
         srm_face<T, true>(cur, nx, p.half_dx, p.inv_dx, p.g, p.h_min, Wf, p.g_recip);
         cur = nx;
 
+#ifdef GSW_FAST_ARITH
+#pragma unroll 2      // two rows in flight: 1.76 -> 1.62 ms at 8192^2 fast (the exact step, and the
+                      // flat march with either arithmetic, slow down)
+#endif
         for (int r = i0; r < i1; ++r) {
             nx.h = pf_h; nx.hu = pf_hu; nx.hv = pf_hv;
             nx.b = b_next;
