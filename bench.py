@@ -133,7 +133,7 @@ DRAM_BYTES_PER_CELL = {"dense": 36.66, "flat": 32.13, "flat_compressed": 48.89}
 # one launch at 4096 x 4096 (tuned shape) divided by the cells it updates. With the SM
 # clock they give the instruction-issue roofline the step kernels are bound by: one warp
 # instruction per scheduler per cycle, four schedulers per SM.
-INST_PER_CELL = {"dense": 38.73, "dense_fast": 23.71, "flat_tidal": 34.23, "flat_compressed": 46.88}
+INST_PER_CELL = {"dense": 38.73, "dense_fast": 22.68, "flat_tidal": 34.23, "flat_compressed": 46.88}
 
 
 def issue_roofline(kind, cells, kern_ms, clocks):
