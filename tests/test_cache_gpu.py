@@ -80,7 +80,7 @@ def test_checkpoint_resume_equals_uninterrupted(tmp_path):
     n_full = full.run(t_end=t_end, window=8, checkpoint_every_s=150.0, ckpt_dir=tmp_path / "a")
     meta = json.load(open(tmp_path / "a" / "ckpt_meta.json"))
     assert meta["t"] == full.t and meta["steps"] == n_full
-    # an interrupted run: stopped by a step budget (no clipped step), checkpointed on the way
+    # an interrupted run: stopped by a step cap (no clipped step), checkpointed on the way
     part = CompressedSolver.from_cache(CACHE)
     m = n_full // 3
     part.run(t_end=t_end, window=8, max_steps=m, checkpoint_every_s=150.0, ckpt_dir=tmp_path / "b")
