@@ -38,11 +38,18 @@ def _check(rc):
         raise L.GswError("mesh", rc, L.lib().gsw_last_error().decode(errors="replace"))
 
 
+# The reference's refusal of a mesh with no neighbour links at all (compressed_rhs.py:
+# 222-224, nbr_to_int16_delta): no inside cell, or nothing stored around them.
+_DEGENERATE = ("no interior neighbors (empty/degenerate active set) -- the inside mask selects no cell "
+               "with a stored neighbour; check the mask and the ring width")
+
+
 def build_tables(inside_pad: np.ndarray, ring: int = 2):
     """The reference's CompressedSWE tables for a padded inside mask (nxp, nyp):
     dict(N, N_active, ij (N,2) int32, nbr (N,4) int16, is_active (N) uint8,
     active_id (nxp, nyp) int32, fully_covered). Raises ValueError when a stored row is
-    too wide for int16 deltas, as the reference does."""
+    too wide for int16 deltas or when no cell has a stored neighbour, as the reference
+    does."""
     Lb = _host_lib()
     inside = np.ascontiguousarray(inside_pad, dtype=np.uint8)
     nxp, nyp = inside.shape
@@ -59,6 +66,8 @@ def build_tables(inside_pad: np.ndarray, ring: int = 2):
     if rc == L.ERR_RANGE:
         raise ValueError(Lb.gsw_last_error().decode())
     _check(rc)
+    if N == 0 or not (nbr != -32768).any():
+        raise ValueError(_DEGENERATE)
     if not cov.value:
         warnings.warn("CompressedSWE: active set not fully covered by the stored ring -- affected "
                       "active cells fall back to a ghost stencil", stacklevel=2)
@@ -296,6 +305,8 @@ class CompressedSolver:
         self._stored = st
         self.N_stored = int(st.sum())
         self.N_active = int(inside.sum())
+        if self.N_stored == 0:
+            raise ValueError(_DEGENERATE)
         bij, bnbr = build_bricks(st.to(torch.uint8).cpu().numpy(), self.brick_h)
         self.n_bricks = int(len(bij))
         BS = self.brick_h * BRICK_PITCH

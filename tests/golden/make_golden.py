@@ -179,13 +179,23 @@ def mesh_cases(G, out):
     cases["band"][10:38, 5:47] = True
     cases["band"][20:30, 15:25] = False
     cases["rect"][4:26, 3:37] = True
+    cases["single"] = np.zeros((7, 9), bool)          # one inside cell
+    cases["single"][3, 4] = True
+    cases["empty"] = np.zeros((6, 5), bool)           # no inside cell
+    cases["edge"] = np.zeros((12, 10), bool)          # inside cells on the array edge: ring not covered
     for name, inside_int in cases.items():
         nxp, nyp = inside_int.shape[0] + 4, inside_int.shape[1] + 4
         inside = np.zeros((nxp, nyp), bool)
         inside[2:-2, 2:-2] = inside_int
+        if name == "edge":
+            inside[0:5, 3:8] = True
         mesh_pad = Mesh2D(nx=nxp, ny=nyp, dx=1.0, dy=1.0, ngh=0)
-        cs = CompressedSWE(mesh_pad, inside, ring=2)
         out[f"mesh_{name}_inside"] = inside
+        try:
+            cs = CompressedSWE(mesh_pad, inside, ring=2)
+        except ValueError as e:                       # the reference refuses this active set
+            out[f"mesh_{name}_raises"] = np.str_(str(e))
+            continue
         out[f"mesh_{name}_ij"] = np.asarray(cs.cm.ij_active)
         out[f"mesh_{name}_aid"] = np.asarray(cs.cm.active_id_padded)
         out[f"mesh_{name}_nbr32"] = np.asarray(cs.cm.neighbors)
@@ -261,5 +271,17 @@ def main():
         print(f, (HERE / f).stat().st_size, "bytes")
 
 
+def main_mesh(ref="/root/reference/src"):
+    """Only the mesh tables (reference_mesh.npz)."""
+    G = _import_reference(ref)
+    mesh_out = {}
+    mesh_cases(G, mesh_out)
+    np.savez_compressed(HERE / "reference_mesh.npz", **mesh_out)
+
+
 if __name__ == "__main__":
-    main()
+    if "--mesh-only" in sys.argv:
+        sys.argv.remove("--mesh-only")
+        main_mesh()
+    else:
+        main()

@@ -217,3 +217,13 @@ def test_flat_ring_stage_tidal_bitwise_oracle():
     for c in range(3):
         assert same(cs.flat(c).cpu().numpy(), o.q[c]), c
     assert abs(float(cs.flat(1).cpu().numpy()[cs.is_active != 0].max())) > 0   # the tide drives a flow
+
+
+def test_empty_mask_refused_like_the_reference():
+    """An inside mask with no cell: the reference's CompressedSWE raises ValueError
+    (no interior neighbors); so does from_dense."""
+    from geoswe_b200.compressed import CompressedSolver
+    q0, bed = flowing(30, 31, seed=2, dtype=np.float32)
+    s = _dense(q0, bed, np.zeros((30, 31), bool))
+    with pytest.raises(ValueError, match="no interior neighbors"):
+        CompressedSolver.from_dense(s)

@@ -15,6 +15,14 @@ CASES = sorted({k.split("_")[1] for k in M.files})
 
 @pytest.mark.parametrize("case", CASES)
 def test_tables_bit_exact(case):
+    """Every case the reference builds (including one inside cell, and inside cells on
+    the array edge whose ring is not covered) is matched bit for bit; a case the
+    reference refuses (no inside cell) is refused here with the same ValueError."""
+    if f"mesh_{case}_raises" in M.files:
+        assert "no interior neighbors" in str(M[f"mesh_{case}_raises"])
+        with pytest.raises(ValueError, match="no interior neighbors"):
+            build_tables(M[f"mesh_{case}_inside"], ring=2)
+        return
     tb = build_tables(M[f"mesh_{case}_inside"], ring=2)
     assert np.array_equal(tb["ij"], M[f"mesh_{case}_ij"])
     assert np.array_equal(tb["active_id"], M[f"mesh_{case}_aid"])
