@@ -59,18 +59,24 @@ def load(kind, cells):
 
 
 def _store(kind, cells, entry):
+    """Add an entry to the JSON cache. Best effort: processes tuning at the same time
+    (one per GPU) each write their own temporary file and rename it into place; a
+    process whose write fails keeps its result in memory only."""
     p = _cache_path()
-    p.parent.mkdir(parents=True, exist_ok=True)
-    data = {}
-    if p.exists():
-        try:
-            data = json.loads(p.read_text())
-        except Exception:
-            data = {}
-    data[_key(kind, cells)] = entry
-    tmp = p.with_suffix(".tmp")
-    tmp.write_text(json.dumps(data, indent=1))
-    tmp.replace(p)
+    try:
+        p.parent.mkdir(parents=True, exist_ok=True)
+        data = {}
+        if p.exists():
+            try:
+                data = json.loads(p.read_text())
+            except Exception:
+                data = {}
+        data[_key(kind, cells)] = entry
+        tmp = p.with_name(f"{p.name}.{os.getpid()}.tmp")
+        tmp.write_text(json.dumps(data, indent=1))
+        os.replace(tmp, p)
+    except OSError:
+        pass
 
 
 def time_dense_step(s, reps=10, tile_rows=0, warps=0, min_blocks=0, dt=None):

@@ -42,3 +42,27 @@ def test_reference_arm_uses_every_core():
     assert r["cores"] == 2 and r["value"] > 0 and r["seconds"] > 0
     one = numpy_ref.time_rain_on_terrain(n=48, steps=2, warm=1)
     assert one["cores"] == 1 and one["value"] > 0
+
+
+def test_tuner_cache_writes_from_many_processes(tmp_path, monkeypatch):
+    """Ranks that tune at the same time write the cache without failing."""
+    import multiprocessing as mp
+    monkeypatch.setenv("GSW_TUNE_CACHE", str(tmp_path / "autotune.json"))
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_store_many, args=(str(tmp_path / "autotune.json"), r)) for r in range(4)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in procs)
+    import json
+    json.loads((tmp_path / "autotune.json").read_text())
+
+
+def _store_many(path, rank):
+    import os
+    os.environ["GSW_TUNE_CACHE"] = path
+    from geoswe_b200 import autotune
+    autotune._key = lambda kind, cells: f"{kind}|{cells}"      # no device query on the CPU
+    for k in range(50):
+        autotune._store("dense", rank * 1000 + k, {"tile_rows": 32, "warps": 4, "min_blocks": 4, "ms": 1.0})
