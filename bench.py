@@ -226,7 +226,7 @@ def run_gsw(args, rank, world):
     m = measure_dense(args, z, cls, n, world, "exact")
     ms, kern_ms = m["ms"], m["kern_ms"]
     # ---------------- end to end through the public API ----------------
-    e2e = run_e2e(args, z, cls, n)
+    e2e = run_e2e(args, z, cls, n, world)
     torch.cuda.empty_cache()
     value = cells * args.steps * world / (ms / 1e3)
     peak, peak_kind = _peaks()
@@ -278,9 +278,10 @@ def time_step_kernel(s, reps=20):
                            min_blocks=s._min_blocks, dt=s.last_dt)
 
 
-def run_e2e(args, z, cls, n):
-    """Public API from pinned host buffers: construct (H2D of state, bed, classes),
-    run the timed steps, read the depth back (D2H), all inside the timed region."""
+def run_e2e(args, z, cls, n, world=1):
+    """Public API from host buffers: construct (H2D of state, bed, classes), run the
+    timed steps, read the depth back (D2H), all inside the timed region; with several
+    ranks, the whole job's cell-updates over the slowest rank's time."""
     import torch
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -295,7 +296,9 @@ def run_e2e(args, z, cls, n):
     h2d = 3 * n * n * 4 + (n + 4) * (n + 4) * 4 + (n + 4) * (n + 4)
     d2h = h.nbytes
     del s
-    return {"value": n * n * args.steps / (ms / 1e3), "unit": UNIT,
+    if world > 1:
+        ms = max_over_ranks(ms, "cuda")
+    return {"value": n * n * args.steps * world / (ms / 1e3), "unit": UNIT,
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
             "what": "Solver2D(host arrays) + run(steps) + depth(); bytes per step = total / steps"}
 
