@@ -169,6 +169,7 @@ _PROTOS = {
     "gsw_mesh_count": [vp, C.c_int, C.c_int, C.c_int, vp, vp],
     "gsw_mesh_build": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp],
     "gsw_bricks_build": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp],
+    "gsw_bricks_slot_of": [vp, C.c_int64, vp, C.c_int64, C.c_int, C.c_int, C.c_int, vp],
     "gsw_ensemble_lammax": [C.POINTER(GswEnsembleArgs), vp],
     "gsw_ensemble_finalize": [C.POINTER(GswEnsembleArgs), vp],
     "gsw_ensemble_step": [C.POINTER(GswEnsembleArgs), vp],

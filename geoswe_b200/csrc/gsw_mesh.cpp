@@ -183,3 +183,31 @@ extern "C" GSW_API int gsw_bricks_build(const uint8_t* stored, int nxp, int nyp,
         }
     return GSW_OK;
 }
+
+// The brick slot of every canonical cell: slot = brick * brick_h * GSW_BRICK_PITCH +
+// (i mod brick_h) * GSW_BRICK_PITCH + (j mod GSW_BRICK_W) for the brick at
+// (i / brick_h, j / GSW_BRICK_W). A host other than this package's Python side needs
+// this map to place the reference's canonical flat arrays into brick storage and back.
+extern "C" GSW_API int gsw_bricks_slot_of(const int32_t* ij, int64_t n_cells, const int32_t* brick_ij,
+                                          int64_t n_bricks, int brick_h, int nxp, int nyp, int64_t* slot_of) {
+    if (!ij || !brick_ij || !slot_of || n_cells < 0 || n_bricks < 0 || brick_h < 2 || nxp <= 0 || nyp <= 0)
+        return set_error(GSW_ERR_INVALID, "bricks_slot_of: bad arguments");
+    const int BI = (nxp + brick_h - 1) / brick_h, BJ = (nyp + GSW_BRICK_W - 1) / GSW_BRICK_W;
+    std::vector<int64_t> bid((size_t)BI * BJ, -1);
+    for (int64_t b = 0; b < n_bricks; ++b) {
+        const int a = brick_ij[2 * b], c = brick_ij[2 * b + 1];
+        if (a < 0 || a >= BI || c < 0 || c >= BJ) return set_error(GSW_ERR_INVALID, "bricks_slot_of: brick %lld "
+                                                                     "outside the grid", (long long)b);
+        bid[(size_t)a * BJ + c] = b;
+    }
+    const int64_t BS = (int64_t)brick_h * GSW_BRICK_PITCH;
+    for (int64_t k = 0; k < n_cells; ++k) {
+        const int i = ij[2 * k], j = ij[2 * k + 1];
+        if (i < 0 || i >= nxp || j < 0 || j >= nyp) return set_error(GSW_ERR_INVALID, "bricks_slot_of: cell %lld "
+                                                                     "outside the grid", (long long)k);
+        const int64_t b = bid[(size_t)(i / brick_h) * BJ + j / GSW_BRICK_W];
+        if (b < 0) return set_error(GSW_ERR_INVALID, "bricks_slot_of: cell %lld has no brick", (long long)k);
+        slot_of[k] = b * BS + (int64_t)(i % brick_h) * GSW_BRICK_PITCH + (j % GSW_BRICK_W);
+    }
+    return GSW_OK;
+}

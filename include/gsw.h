@@ -394,6 +394,13 @@ GSW_API int gsw_mesh_build(const uint8_t* inside, int nxp, int nyp, int ring, in
                            int16_t* nbr16, uint8_t* is_active, int32_t* active_id, int32_t* covered);
 GSW_API int gsw_bricks_build(const uint8_t* stored, int nxp, int nyp, int brick_h,
                              int64_t* n_bricks, int32_t* brick_ij, int32_t* brick_nbr);
+/* Canonical cell k (padded row, column ij[2k], ij[2k+1], as gsw_mesh_build returns
+ * them) -> its slot in brick storage, for bricks from gsw_bricks_build. A host that
+ * keeps the reference's canonical flat arrays uses it to scatter them into brick
+ * storage and gather results back. No counterpart in the reference (its kernels read
+ * the canonical arrays directly). */
+GSW_API int gsw_bricks_slot_of(const int32_t* ij, int64_t n_cells, const int32_t* brick_ij, int64_t n_bricks,
+                               int brick_h, int nxp, int nyp, int64_t* slot_of);
 
 /* ------------------------------------------------------------------------- */
 /* Adjoint of the compressed-mesh step. No counterpart in the reference, which */

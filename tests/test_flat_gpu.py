@@ -227,3 +227,19 @@ def test_empty_mask_refused_like_the_reference():
     s = _dense(q0, bed, np.zeros((30, 31), bool))
     with pytest.raises(ValueError, match="no interior neighbors"):
         CompressedSolver.from_dense(s)
+
+
+def test_library_slot_map_equals_the_solvers():
+    """The host entry point gsw_bricks_slot_of gives the canonical-to-slot map the
+    solver builds on the device."""
+    from geoswe_b200 import _lib as L
+    from geoswe_b200.compressed import CompressedSolver
+    q0, bed = flowing(70, 97, seed=12, dtype=np.float32)
+    cs = CompressedSolver.from_dense(_dense(q0, bed, _blob_mask(70, 97)))
+    ij = np.ascontiguousarray(cs.ij_active, np.int32)
+    bij = np.ascontiguousarray(cs._bij.cpu().numpy(), np.int32)
+    slot = np.empty(len(ij), np.int64)
+    lib = L.lib()
+    assert lib.gsw_bricks_slot_of(ij.ctypes.data, len(ij), bij.ctypes.data, len(bij), cs.brick_h, cs.nxp, cs.nyp,
+                                  slot.ctypes.data) == 0
+    assert np.array_equal(slot, cs._slot.cpu().numpy())

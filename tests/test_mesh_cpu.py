@@ -82,3 +82,31 @@ def test_reference_cache_tables_match_builder():
     assert t["N"] == meta["N"]
     assert np.array_equal(t["ij"], ij) and np.array_equal(t["nbr"], np.load(d / "nbr.npy"))
     assert np.array_equal(t["is_active"], act)
+
+
+@pytest.mark.parametrize("bh", [4, 16])
+def test_bricks_slot_of(bh):
+    """gsw_bricks_slot_of places every canonical cell in its brick, at its row and
+    column, each in its own slot."""
+    import ctypes as C
+    from geoswe_b200 import _lib as L
+    inside = M["mesh_band_inside"]
+    tb = build_tables(inside)
+    stored = tb["active_id"] >= 0
+    bij, _ = build_bricks(stored, bh)
+    nxp, nyp = inside.shape
+    ij = np.ascontiguousarray(tb["ij"], np.int32)
+    slot = np.empty(len(ij), np.int64)
+    lib = L.lib()
+    rc = lib.gsw_bricks_slot_of(ij.ctypes.data, len(ij), np.ascontiguousarray(bij, np.int32).ctypes.data, len(bij),
+                                bh, nxp, nyp, slot.ctypes.data)
+    assert rc == 0, lib.gsw_last_error()
+    BS = bh * 32
+    assert len(np.unique(slot)) == len(slot) and slot.min() >= 0 and slot.max() < len(bij) * BS
+    b, rem = slot // BS, slot % BS
+    assert np.array_equal(bij[b, 0] * bh + rem // 32, ij[:, 0])
+    assert np.array_equal(bij[b, 1] * BRICK_W + rem % 32, ij[:, 1])
+    bad = ij.copy()
+    bad[0] = (nxp + 5, 0)
+    assert lib.gsw_bricks_slot_of(bad.ctypes.data, len(bad), np.ascontiguousarray(bij, np.int32).ctypes.data,
+                                  len(bij), bh, nxp, nyp, slot.ctypes.data) == L.ERR_INVALID
