@@ -30,6 +30,7 @@ struct AdjK {
     T* rb0; T* rb1; T* rb2;                      // residual adjoints (scratch, zero off the stored slots)
     double* n_bar; int n_tab_len;
     double* rate_bar;
+    int segs;                 // warps per brick: each marches brick_h / segs rows
 };
 
 template <typename T>
@@ -87,7 +88,9 @@ __global__ void __launch_bounds__(128, MINB) adj_tail_kernel(AdjK<T> p) {
     const FlatMesh<T>& m = p.m;
     const FlatPhys<T>& ph = p.ph;
     const int lane = threadIdx.x;
-    const int64_t bidx = (int64_t)blockIdx.x * blockDim.y + threadIdx.y;
+    const int64_t item = (int64_t)blockIdx.x * blockDim.y + threadIdx.y;   // (brick, row segment)
+    const int64_t bidx = item / p.segs;
+    const int seg = (int)(item - bidx * p.segs);
     double rate_acc = 0.0;
     const T dt = sizeof(T) == 4 ? (T)p.st->dt_f32 : (T)p.st->dt;
     T rate = (T)0;
@@ -98,21 +101,22 @@ __global__ void __launch_bounds__(128, MINB) adj_tail_kernel(AdjK<T> p) {
         const BrickView v = brick_view(m, bidx);
         const int bi = m.bij[2 * bidx], bj = m.bij[2 * bidx + 1];
         const int bh = m.bh;
+        const int r0 = seg * bh / p.segs, r1 = (seg + 1) * bh / p.segs;
         Cell<T> cur, nx;
-        const T b_m2 = __ldg(m.b + v.slot(-2, lane));
-        load_state(m, v.slot(-1, lane), cur);
-        load_state(m, v.slot(0, lane), nx);
-        T b_next = __ldg(m.b + v.slot(1, lane));
+        const T b_m2 = __ldg(m.b + v.slot(r0 - 2, lane));
+        load_state(m, v.slot(r0 - 1, lane), cur);
+        load_state(m, v.slot(r0, lane), nx);
+        T b_next = __ldg(m.b + v.slot(r0 + 1, lane));
         make_prims(cur, ph.h_min);
         make_prims(nx, ph.h_min);
         cur.gx = (T)0.5 * (nx.b - b_m2) * ph.inv_dx;
         cur.gy = (T)0;
         nx.gx = (T)0.5 * (b_next - cur.b) * ph.inv_dx;
-        nx.gy = grad_y_flat<T>(m, ph, v, nx.b, 0, lane);
+        nx.gy = grad_y_flat<T>(m, ph, v, nx.b, r0, lane);
         Face<T> Wf;
         srm_face<T, true>(cur, nx, ph.half_dx, ph.inv_dx, ph.g, ph.h_min, Wf);
         cur = nx;
-        for (int r = 0; r < bh; ++r) {
+        for (int r = r0; r < r1; ++r) {
             {
                 const int64_t s = v.slot(r + 1, lane);
                 nx.h = __ldg(m.q0 + s); nx.hu = __ldg(m.q1 + s); nx.hv = __ldg(m.q2 + s);
@@ -183,25 +187,28 @@ __global__ void __launch_bounds__(128, MINB) adj_face_kernel(AdjK<T> p) {
     const FlatMesh<T>& m = p.m;
     const FlatPhys<T>& ph = p.ph;
     const int lane = threadIdx.x;
-    const int64_t bidx = (int64_t)blockIdx.x * blockDim.y + threadIdx.y;
+    const int64_t item = (int64_t)blockIdx.x * blockDim.y + threadIdx.y;   // (brick, row segment)
+    const int64_t bidx = item / p.segs;
+    const int seg = (int)(item - bidx * p.segs);
     if (bidx >= m.nb) return;                                  // warp-uniform
     const BrickView v = brick_view(m, bidx);
     const int bh = m.bh;
+    const int r0 = seg * bh / p.segs, r1 = (seg + 1) * bh / p.segs;
     Cell<T> cur, nx;
-    const T b_m2 = __ldg(m.b + v.slot(-2, lane));
-    int64_t s = v.slot(-1, lane);
+    const T b_m2 = __ldg(m.b + v.slot(r0 - 2, lane));
+    int64_t s = v.slot(r0 - 1, lane);
     load_state(m, s, cur);
     Bar3<T> rb_cur = load_bar<T>(p.rb0, p.rb1, p.rb2, s);
-    s = v.slot(0, lane);
+    s = v.slot(r0, lane);
     load_state(m, s, nx);
     Bar3<T> rb_nx = load_bar<T>(p.rb0, p.rb1, p.rb2, s);
-    T b_next = __ldg(m.b + v.slot(1, lane));
+    T b_next = __ldg(m.b + v.slot(r0 + 1, lane));
     make_prims(cur, ph.h_min);
     make_prims(nx, ph.h_min);
     cur.gx = (T)0.5 * (nx.b - b_m2) * ph.inv_dx;
     cur.gy = (T)0;
     nx.gx = (T)0.5 * (b_next - cur.b) * ph.inv_dx;
-    nx.gy = grad_y_flat<T>(m, ph, v, nx.b, 0, lane);
+    nx.gy = grad_y_flat<T>(m, ph, v, nx.b, r0, lane);
     const Bar3<T> zero3 = {(T)0, (T)0, (T)0};
     Bar3<T> carry = zero3;                   // the x-face above the current row, cell below
     if (nonzero(rb_cur) || nonzero(rb_nx)) {
@@ -211,7 +218,7 @@ __global__ void __launch_bounds__(128, MINB) adj_face_kernel(AdjK<T> p) {
     }
     cur = nx;
     rb_cur = rb_nx;
-    for (int r = 0; r < bh; ++r) {
+    for (int r = r0; r < r1; ++r) {
         s = v.slot(r + 1, lane);
         nx.h = __ldg(m.q0 + s); nx.hu = __ldg(m.q1 + s); nx.hv = __ldg(m.q2 + s);
         rb_nx = load_bar<T>(p.rb0, p.rb1, p.rb2, s);
@@ -382,7 +389,8 @@ static int launch_adj(const GswFlatAdjArgs* a, cudaStream_t s) {
     if (int rc = fill_adj<T>(a, k)) return rc;
     if (k.m.nb == 0) return GSW_OK;
     const int W = 4;
-    const int64_t blocks = (k.m.nb + W - 1) / W;
+    k.segs = auto_segments(k.m.nb, (int64_t)sm_count() * 32, k.m.bh);
+    const int64_t blocks = (k.m.nb * k.segs + W - 1) / W;
     if (blocks > 0x7fffffffLL) return set_error(GSW_ERR_INVALID, "adjoint: too many bricks");
     // register cap of the binary32 reverse kernels: 0 (compiler's choice), 6 (80) or 8 (64 registers)
     const int mb = sizeof(T) == 4 ? a->min_blocks : 0;
