@@ -124,7 +124,7 @@ class GswFlatForcingArgs(C.Structure):
 class GswMember(C.Structure):
     _fields_ = [("dt", GswDtParams), ("inv_dx", C.c_float), ("g", C.c_float), ("h_min", C.c_float),
                 ("h_min_cfl", C.c_float), ("vcap", C.c_float), ("linf", i32), ("quadratic", i32),
-                ("keep_h", i32), ("rain_kind", i32), ("reserved0", i32), ("rain", vp), ("n_tab", vp)]
+                ("keep_h", i32), ("rain_kind", i32), ("g_recip", C.c_float), ("rain", vp), ("n_tab", vp)]
 
 
 class GswTuneResult(C.Structure):
@@ -170,6 +170,7 @@ _PROTOS = {
     "gsw_mesh_build": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp],
     "gsw_bricks_build": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp],
     "gsw_bricks_slot_of": [vp, C.c_int64, vp, C.c_int64, C.c_int, C.c_int, C.c_int, vp],
+    "gsw_div_const_recip": [C.c_float],
     "gsw_ensemble_lammax": [C.POINTER(GswEnsembleArgs), vp],
     "gsw_ensemble_finalize": [C.POINTER(GswEnsembleArgs), vp],
     "gsw_ensemble_step": [C.POINTER(GswEnsembleArgs), vp],
@@ -202,6 +203,7 @@ def lib():
         fn = getattr(L, name)
         fn.argtypes = argt
         fn.restype = C.c_int
+    L.gsw_div_const_recip.restype = C.c_float
     L.gsw_last_error.restype = C.c_char_p
     L.gsw_last_error.argtypes = []
     L.gsw_abi_version.restype = C.c_uint32

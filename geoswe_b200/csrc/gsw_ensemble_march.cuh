@@ -27,7 +27,7 @@ __device__ __forceinline__ FlatPhys<float> member_phys(const GswMember& mb) {
     ph.linf = mb.linf; ph.quad = mb.quadratic; ph.keep_h = mb.keep_h;
     ph.rain_kind = mb.rain_kind; ph.rain = mb.rain; ph.ntab = mb.n_tab;
     ph.ngh = 0; ph.nx = 0; ph.ny = 0; ph.lookup = nullptr; ph.ncol = 0;
-    ph.g_recip = 0.0f;       // members divide (each has its own g)
+    ph.g_recip = mb.g_recip; // 0: the member divides
     return ph;
 }
 

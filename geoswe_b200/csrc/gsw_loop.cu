@@ -139,6 +139,7 @@ extern "C" int gsw_loop_commit(GswLoopState* state, void* stream) {
     return check_launch("loop_commit");
 }
 
+extern "C" float gsw_div_const_recip(float g) { return gsw_rt::div_const_recip(g); }
 extern "C" const char* gsw_last_error(void) { return gsw_rt::g_err; }
 extern "C" uint32_t gsw_abi_version(void) { return GSW_ABI_VERSION; }
 extern "C" uint64_t gsw_launch_count(void) { return (uint64_t)gsw_rt::g_launches.load(); }

@@ -144,6 +144,7 @@ class Ensemble:
             mb.inv_dx = float(np.float32(1.0 / m.dx))
             mb.g, mb.h_min, mb.h_min_cfl, mb.vcap = m.g, m.h_min, m.h_min_cfl, m.vcap
             mb.linf, mb.quadratic, mb.keep_h = int(m.cfl_linf), int(m.quad), int(m.keep_h)
+            mb.g_recip = L.lib().gsw_div_const_recip(float(np.float32(m.g)))   # the flat step's h / g
             if m._rain_kind not in (L.RAIN_NONE, L.RAIN_UNIFORM):
                 raise NotImplementedError("Ensemble members take uniform rain (one rate per frame)")
             mb.rain_kind = m._rain_kind

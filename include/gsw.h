@@ -458,7 +458,7 @@ typedef struct GswMember {
     float    inv_dx, g, h_min, h_min_cfl, vcap;
     int32_t  linf, quadratic, keep_h;
     int32_t  rain_kind;      /* GSW_RAIN_NONE or GSW_RAIN_UNIFORM */
-    int32_t  reserved0;
+    float    g_recip;        /* gsw_div_const_recip(g), or 0 (the star depth's h / g divides) */
     const float* rain;       /* uniform rate (m/s) per rain frame */
     const float* n_tab;      /* the member's Manning class table */
 } GswMember;
@@ -571,6 +571,11 @@ GSW_API int gsw_flat_autotune(const GswFlatArgs* a, int32_t reps, int32_t use_ca
 /* ------------------------------------------------------------------------- */
 /* Library                                                                    */
 /* ------------------------------------------------------------------------- */
+/* RN(1/g) when the reciprocal-and-remainder sequence the step uses for the HLLC star
+ * depth's h / g reproduces the IEEE quotient for every binary32 significand of h (an
+ * exhaustive check, once per g per process), else 0. The dense and flat steps apply it
+ * themselves; an ensemble caller passes it in GswMember.g_recip. */
+GSW_API float gsw_div_const_recip(float g);
 GSW_API const char* gsw_last_error(void);
 GSW_API uint32_t    gsw_abi_version(void);
 /* Number of this library's kernels launched since load (all entry points). */

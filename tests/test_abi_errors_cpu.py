@@ -81,3 +81,16 @@ def test_adjoint_refuses_fast_arguments():
     a.min_blocks = 3
     rc, msg = _call("gsw_adj_flat_step", C.byref(a), None)
     assert rc == L.ERR_INVALID
+
+
+def test_constant_reciprocal_check():
+    """gsw_div_const_recip: RN(1/g) for the gravity values in use (their sequence is
+    exhaustively checked to give the IEEE quotient), 0 for values it cannot take."""
+    import numpy as np
+    lib = L.lib()
+    for g in (9.81, 9.80665, 9.8):
+        y = lib.gsw_div_const_recip(g)
+        assert y == float(np.float32(1.0 / np.float64(np.float32(g))))
+    assert lib.gsw_div_const_recip(0.0) == 0.0
+    assert lib.gsw_div_const_recip(-9.81) == 0.0
+    assert lib.gsw_div_const_recip(float("inf")) == 0.0
