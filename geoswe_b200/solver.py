@@ -73,21 +73,48 @@ def _cached_graph(cache, key, capture, device, keep=4):
     return cache[key]
 
 
+def pad_bed(bpad, ngh, bc_x, bc_y):
+    """Ghost bed as the ghost state is filled (solver.py:1466-1484): x first over the
+    full x extent, then y; a periodic axis wraps, every other kind repeats the edge
+    cell. `bpad` is the padded (nxp, nyp) bed, a NumPy array or a tensor view, filled
+    in place."""
+    if bc_x == "periodic":
+        bpad[:ngh, :] = bpad[-2 * ngh:-ngh, :]
+        bpad[-ngh:, :] = bpad[ngh:2 * ngh, :]
+    else:
+        bpad[:ngh, :] = bpad[ngh:ngh + 1, :]
+        bpad[-ngh:, :] = bpad[-ngh - 1:-ngh, :]
+    if bc_y == "periodic":
+        bpad[:, :ngh] = bpad[:, -2 * ngh:-ngh].clone() if torch.is_tensor(bpad) else bpad[:, -2 * ngh:-ngh]
+        bpad[:, -ngh:] = bpad[:, ngh:2 * ngh].clone() if torch.is_tensor(bpad) else bpad[:, ngh:2 * ngh]
+    else:
+        bpad[:, :ngh] = bpad[:, ngh:ngh + 1]
+        bpad[:, -ngh:] = bpad[:, -ngh - 1:-ngh]
+
+
 class Solver2D:
     """Two-dimensional shallow-water solver on the dense padded grid.
 
     ``q0`` has shape (3, nx, ny) and ``b`` (nx, ny), host or device arrays. The padded
     state is exposed as ``q`` (a (3, nx+2ngh, ny+2ngh) CUDA tensor view) and the depth
     as ``depth()`` (NumPy). ``run``/``step``/``cfl_dt`` follow the reference.
+
+    With ``comm`` (a torch.distributed process group of more than one rank) the run is
+    split over the ranks of a ``dims`` Cartesian layout (solver.py:1286-1454): ``mesh``,
+    ``q0`` and ``b`` are this rank's block (``partition.block_of``), faces that border
+    another rank take their ghosts from it (``halo.Halo2D``; the bed once, the state
+    every step) and the wave speed is the maximum over the ranks, so every rank takes
+    the same dt and the blocks together equal the single-domain run bit for bit.
     """
 
     def __init__(self, mesh: Mesh2D, cfg: Config, q0, b, comm=None, dims=None, *,
                  device=None, track_max_depth: bool = True, use_graphs: bool = True,
                  tile_rows: int = 0, warps: int = 0, min_blocks: int = 0, autotuned: bool = True):
         _require_cuda()
-        if comm is not None and getattr(comm, "size", 1) > 1:
-            raise NotImplementedError("Solver2D: multi-rank runs are not part of this package "
-                                      "(one GPU per solver)")
+        from .halo import comm_size
+        self.comm = comm
+        self.halo = None
+        multi = comm_size(comm) > 1
         cfg.require_production_scheme("Solver2D")
         if "dirichlet" in (cfg.bc_x, cfg.bc_y):
             raise ValueError("bc 'dirichlet' exists for Solver1D only; in 2D impose a water "
@@ -153,6 +180,16 @@ class Solver2D:
         self._b[ngh:ngh + mesh.nx, ngh:ngh + mesh.ny] = b_dev
         self._pad_bed(self._b[:, :self.nyp])
         del q_dev, b_dev
+        if multi:
+            from .halo import Halo2D
+            self.halo = Halo2D(comm, self.nxp, self.nyp, ngh, dtype=str(self.np_dtype),
+                               periods=(cfg.bc_x == "periodic", cfg.bc_y == "periodic"),
+                               dims=dims, device=self.device)
+            # the bed's ghosts at a rank seam are the neighbour's cells, not the local
+            # extrapolation (solver.py:1449-1454)
+            self.halo.exchange(self._b)
+            # the step sequence holds collectives; it is launched eagerly
+            self._use_graphs = False
         self._mask = None
         self.inside_mask_interior = None
         self._ncls = None
@@ -164,6 +201,8 @@ class Solver2D:
         self._stepped = False
         self._inflows = []
         self._state = torch.zeros(128, dtype=torch.uint8, device=dev)
+        lam = L.GswLoopState.lam_bits.offset // 8
+        self._lam_view = self._state.view(torch.int64)[lam:lam + 1]   # the wave-speed bits
         self._state_host = torch.zeros(128, dtype=torch.uint8).pin_memory()
         self._lam_scratch = torch.zeros(1, dtype=torch.int64, device=dev)
         self._graph_cache = {}
@@ -177,21 +216,7 @@ class Solver2D:
 
     # ------------------------------------------------------------------ layout
     def _pad_bed(self, bpad):
-        """Ghost bed as the ghost state is filled (solver.py:1466-1484); `bpad` is the
-        padded (nxp, nyp) bed, a NumPy array or a device tensor view, filled in place."""
-        ngh = self.mesh.ngh
-        if self.cfg.bc_x == "periodic":
-            bpad[:ngh, :] = bpad[-2 * ngh:-ngh, :]
-            bpad[-ngh:, :] = bpad[ngh:2 * ngh, :]
-        else:
-            bpad[:ngh, :] = bpad[ngh:ngh + 1, :]
-            bpad[-ngh:, :] = bpad[-ngh - 1:-ngh, :]
-        if self.cfg.bc_y == "periodic":
-            bpad[:, :ngh] = bpad[:, -2 * ngh:-ngh].clone() if torch.is_tensor(bpad) else bpad[:, -2 * ngh:-ngh]
-            bpad[:, -ngh:] = bpad[:, ngh:2 * ngh].clone() if torch.is_tensor(bpad) else bpad[:, ngh:2 * ngh]
-        else:
-            bpad[:, :ngh] = bpad[:, ngh:ngh + 1]
-            bpad[:, -ngh:] = bpad[:, -ngh - 1:-ngh]
+        pad_bed(bpad, self.mesh.ngh, self.cfg.bc_x, self.cfg.bc_y)
 
     @property
     def q(self):
@@ -312,6 +337,10 @@ class Solver2D:
     def add_inflow(self, idx_i, idx_j, normal, ds, t_series, q_series, dry_frac=0.10):
         """One discharge inlet on padded cells (idx_i, idx_j) along a physical edge;
         ``normal`` is the inward unit normal (axis-aligned)."""
+        if self.halo is not None:
+            raise NotImplementedError("add_inflow: discharge inlets are not supported on a run split "
+                                      "over several ranks (the inlet's depth sum would need a sum over "
+                                      "the ranks every step); run the inlet's domain on one rank")
         ii = np.asarray(idx_i, dtype=np.int64).ravel()
         jj = np.asarray(idx_j, dtype=np.int64).ravel()
         if ii.shape != jj.shape:
@@ -488,8 +517,9 @@ class Solver2D:
         a.nxp, a.nyp, a.ngh, a.pitch = self.nxp, self.nyp, self.mesh.ngh, self.pitch
         a.q0, a.q1, a.q2 = _ptr(buf[0]), _ptr(buf[1]), _ptr(buf[2])
         kinds = [L.BC_CODES[k] for k in self.cfg.face_kinds()]
-        for f in range(4):
-            a.kinds[f] = kinds[f]
+        for f, side in enumerate(("x-", "x+", "y-", "y+")):
+            # a face bordering another rank takes its ghosts from the halo exchange
+            a.kinds[f] = L.BC_NONE if self.halo is not None and self.halo.has_neighbor(side) else kinds[f]
         a.state = _ptr(self._state)
         return a
 
@@ -514,6 +544,8 @@ class Solver2D:
         src, dst = self._buf[k_parity], self._buf[1 - k_parity]
         s = _stream()
         L.call("gsw_bc_fill", C.byref(self._bc_args(src)), s)
+        if self.halo is not None:
+            self.halo.exchange(src)
         for inl in T.inflows:
             self._launch_inflow(inl, src, s)
         n = 2 + len(T.inflows) + 2 * len(T.stages) + (1 if len(T.stages) > 1 else 0)
@@ -597,6 +629,8 @@ class Solver2D:
         src = self._buf[self._cur]
         s = _stream()
         L.call("gsw_bc_fill", C.byref(self._bc_args(src)), s)
+        if self.halo is not None:
+            self.halo.exchange(src)
         for inl in T.inflows:
             self._launch_inflow(inl, src, s)
 
@@ -615,6 +649,8 @@ class Solver2D:
         T = self._tables()
         self._write_state()
         self._lammax_into_state(T.ghost_skip)
+        if self.halo is not None:
+            self.halo.allreduce_max_(self._lam_view)
         lam_max = self._read_state().lam_bits
         lam_max = float(np.array([lam_max], dtype=np.uint64).view(np.float64)[0])
         if not math.isfinite(lam_max):
@@ -698,6 +734,8 @@ class Solver2D:
     def _run_device(self, t_end, max_steps, dt_max, window=0):
         T = self._tables()
         K = int(window) if window else self._window_size()
+        if self.halo is not None and not window:
+            K = min(K, 32)     # launched eagerly: poll often, so few no-op steps follow the end
         if max_steps and max_steps < K and not window:
             K = int(max_steps)
         K += K % 2
@@ -712,6 +750,8 @@ class Solver2D:
         start_cur = self._cur
 
         def one_step(k_parity):
+            if self.halo is not None:     # every rank takes the dt of the largest wave speed
+                self.halo.allreduce_max_(self._lam_view)
             L.call("gsw_dt_finalize_dev", _ptr(self._dtp_dev), _ptr(self._state), _stream())
             self._counting += 1
             self._launch_step(k_parity, T)

@@ -1,0 +1,284 @@
+"""The Cartesian split of the dense grid on the CPU: the strip bounds (pinned to the
+reference's own partition tests, tests/test_partition.py), the face exchange of
+``halo.Halo2D`` between gloo ranks, and a split oracle run -- each rank the oracle's
+NumPy step on its block, ghosts at the seams from ``Halo2D``, dt the minimum over the
+ranks -- equal bit for bit to the single-domain oracle run. The oracle is the
+checker; the exchange under test is the package's."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+import torch.distributed as dist  # noqa: E402
+import torch.multiprocessing as mp  # noqa: E402
+
+from geoswe_b200.halo import SIDES, Halo2D, check_face_extent, compute_dims  # noqa: E402
+from geoswe_b200.partition import block_of, strip_bounds  # noqa: E402
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _spawn(fn, world, *args):
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        mp.start_processes(fn, args=(world, _free_port(), out, *args), nprocs=world,
+                           start_method="spawn", join=True)
+        return dict(out)
+
+
+def _init(rank, world, port):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+
+
+# ------------------------------------------------------------------ layout
+def test_compute_dims_is_the_most_square_split():
+    want = {1: [1, 1], 2: [2, 1], 3: [3, 1], 4: [2, 2], 6: [3, 2], 7: [7, 1], 8: [4, 2],
+            12: [4, 3], 16: [4, 4]}
+    assert {n: compute_dims(n) for n in want} == want
+
+
+def test_strip_bounds_pins():
+    """Known answers of the reference's tests/test_partition.py."""
+    assert strip_bounds(32000 * 16, 16) == [32000 * r for r in range(17)]
+    assert strip_bounds(10, 3) == [0, 3, 7, 10]
+    assert strip_bounds(7, 1) == [0, 7]
+    for n, k in ((4096, 4), (1000, 7), (33, 5)):
+        w = np.linspace(0.97, 1.03, k)
+        assert strip_bounds(n, k, w) == strip_bounds(np.ones(n), k, w)
+    rng = np.random.default_rng(0)
+    w = 1.0 + 0.0056 * rng.standard_normal(1024)
+    n = 32000 * w.size
+    jb = strip_bounds(n, w.size, w)
+    strips = np.diff(jb)
+    assert jb[0] == 0 and jb[-1] == n and (strips > 0).all()
+    assert np.abs(strips - n * w / w.sum()).max() <= 1.0
+    col = np.r_[np.zeros(100), np.full(300, 5.0), np.full(600, 1.0)]
+    jb = strip_bounds(col, 3, [1.0, 1.0, 1.0])
+    assert max(abs(col[jb[r]:jb[r + 1]].sum() - 700.0) for r in range(3)) <= 5.0
+    jb = strip_bounds(col, 2, [3.0, 1.0])
+    assert abs(col[:jb[1]].sum() - 0.75 * col.sum()) <= 5.0
+    assert strip_bounds(4, 4, [1e-9, 1.0, 1.0, 1e-9]) == [0, 1, 2, 3, 4]
+    jb = strip_bounds(np.r_[np.zeros(50), 1.0, np.zeros(49)], 3)
+    assert jb[0] == 0 and jb[-1] == 100 and all(b > a for a, b in zip(jb, jb[1:]))
+
+
+@pytest.mark.parametrize("bad", [[1.0, 1.0], [1.0, 0.0, 1.0], [1.0, -1.0, 1.0], [1.0, np.nan, 1.0],
+                                 [1.0, np.inf, 1.0]])
+def test_strip_bounds_refuses_bad_weights(bad):
+    with pytest.raises(ValueError, match="weights"):
+        strip_bounds(300, 3, bad)
+
+
+def test_strip_bounds_refuses_too_many_ranks():
+    with pytest.raises(ValueError, match="cannot be split"):
+        strip_bounds(3, 4)
+    with pytest.raises(ValueError, match="n_ranks"):
+        strip_bounds(3, 0)
+
+
+def test_blocks_tile_the_grid():
+    nx, ny, dims = 23, 18, (3, 2)
+    cover = np.zeros((nx, ny), int)
+    for r in range(6):
+        x0, x1, y0, y1 = block_of(nx, ny, dims, (r // 2, r % 2))
+        cover[x0:x1, y0:y1] += 1
+    assert (cover == 1).all()
+
+
+def test_face_extent_message():
+    """Mirrors the reference's check (mpi_halo.py:256-275): only the extent along the
+    face must agree, and the message names the face, the rank and both extents."""
+    mine = (40, 24, 4)
+    for side, nbr, theirs, want in (("x-", 3, (40, 20, 4), ("face x-", "rank 3", "nyp=24", "nyp=20")),
+                                    ("y+", 1, (36, 24, 4), ("face y+", "nxp=40", "nxp=36")),
+                                    ("x+", 1, (40, 24, 2), ("ngh=4", "ngh=2"))):
+        with pytest.raises(RuntimeError) as e:
+            check_face_extent(side, nbr, mine, theirs)
+        assert all(w in str(e.value) for w in want), str(e.value)
+    for side, theirs in (("x-", (33, 24, 4)), ("x+", (33, 24, 4)), ("y-", (40, 19, 4)), ("y+", (40, 19, 4))):
+        check_face_extent(side, 1, mine, theirs)
+
+
+# ------------------------------------------------------------------ exchange
+NX, NY, G = 23, 18, 2
+
+
+def _exchange_rank(rank, world, port, out, dims, periods):
+    _init(rank, world, port)
+    try:
+        cx, cy = rank // dims[1], rank % dims[1]
+        x0, x1, y0, y1 = block_of(NX, NY, dims, (cx, cy))
+        nx, ny = x1 - x0, y1 - y0
+        halo = Halo2D(None, nx + 2 * G, ny + 2 * G, G, dtype="float64", periods=periods, dims=dims)
+        W = ny + 2 * G + 3                            # a row pitch past nyp stays untouched
+        a = torch.full((3, nx + 2 * G, W), -1.0, dtype=torch.float64)
+        gi = torch.arange(x0, x1, dtype=torch.float64)[:, None]
+        gj = torch.arange(y0, y1, dtype=torch.float64)[None, :]
+        for c in range(3):
+            a[c, G:G + nx, G:G + ny] = c * 1e6 + gi * 1000 + gj
+        halo.exchange(a)
+        bad = []
+        for i in range(nx + 2 * G):
+            for j in range(W):
+                inner_i, inner_j = G <= i < G + nx, G <= j < G + ny
+                if inner_i and inner_j:
+                    continue
+                got = a[:, i, j]
+                if j >= ny + 2 * G or not (inner_i or inner_j):   # pitch columns, corners
+                    if j >= ny + 2 * G and (got != -1.0).any():
+                        bad.append(("pitch", i, j))
+                    continue
+                side = ("x-" if i < G else "x+") if not inner_i else ("y-" if j < G else "y+")
+                if not halo.has_neighbor(side):
+                    if (got != -1.0).any():
+                        bad.append(("physical face written", side, i, j))
+                    continue
+                ii, jj = x0 + i - G, y0 + j - G
+                ii, jj = ii % NX, jj % NY
+                want = torch.tensor([c * 1e6 + ii * 1000 + jj for c in range(3)], dtype=torch.float64)
+                if not torch.equal(got, want):
+                    bad.append((side, i, j, got.tolist(), want.tolist()))
+        out[rank] = dict(bad=bad[:5], nbad=len(bad), nbr=(halo.nbr_x, halo.nbr_y),
+                         sides=[s for s in SIDES if halo.has_neighbor(s)])
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,dims,periods", [
+    (2, [2, 1], (False, False)),
+    (2, [1, 2], (False, False)),
+    (2, [2, 1], (True, False)),          # both x faces border the same rank
+    (2, [2, 1], (False, True)),          # periodic y not split: the ghost fill's wrap
+    (4, [2, 2], (True, True)),
+    (4, [4, 1], (False, False)),
+])
+def test_exchange_fills_seams_only(world, dims, periods):
+    out = _spawn(_exchange_rank, world, dims, periods)
+    for r in range(world):
+        assert out[r]["nbad"] == 0, (r, out[r])
+    if dims == [2, 1] and periods == (True, False):
+        assert out[0]["nbr"][0] == (1, 1) and set(out[0]["sides"]) == {"x-", "x+"}
+    if periods == (False, True):
+        assert all("y-" not in out[r]["sides"] for r in range(world))
+
+
+def _mismatch_rank(rank, world, port, out):
+    _init(rank, world, port)
+    try:
+        Halo2D(None, 20, 10 + 2 * rank, G, dtype="float32", dims=[2, 1])
+        out[rank] = "accepted"
+    except RuntimeError as e:
+        out[rank] = str(e)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_face_extent_mismatch_raises_on_both_ranks():
+    out = _spawn(_mismatch_rank, 2)
+    assert "nyp=10" in out[0] and "nyp=12" in out[0] and "rank 1" in out[0]
+    assert "nyp=12" in out[1] and "nyp=10" in out[1] and "rank 0" in out[1]
+
+
+# ------------------------------------------------------------------ split oracle run
+NSTEPS = 25
+
+
+def _oracle_inputs(dtype):
+    from tests._cases import flowing
+    return flowing(NX, NY, seed=5, dtype=dtype)
+
+
+def _oracle_solver(qp, bp, kinds, dtype):
+    from oracle.numpy_ref import NumpySolver2D
+    return NumpySolver2D(qp, bp, G, 2.0, 2.5, kinds=kinds, friction="manning", manning_n=0.03,
+                         rain_times=[0.0, 1e9], rain_mm_h=[80.0, 80.0])
+
+
+def _kinds_axes(kinds):
+    return ("periodic" if kinds[0] == "periodic" else "x", "periodic" if kinds[2] == "periodic" else "y")
+
+
+def _split_rank(rank, world, port, out, dims, kinds, dtype):
+    _init(rank, world, port)
+    try:
+        from geoswe_b200.solver import pad_bed
+        dtype = np.dtype(dtype)
+        q0, bed = _oracle_inputs(dtype)
+        periods = (kinds[0] == "periodic", kinds[2] == "periodic")
+        coords = (rank // dims[1], rank % dims[1])
+        x0, x1, y0, y1 = block_of(NX, NY, dims, coords)
+        nx, ny = x1 - x0, y1 - y0
+        halo = Halo2D(None, nx + 2 * G, ny + 2 * G, G, dtype=str(dtype), periods=periods, dims=dims)
+        qp = np.zeros((3, nx + 2 * G, ny + 2 * G), dtype)
+        qp[:, G:G + nx, G:G + ny] = q0[:, x0:x1, y0:y1]
+        bp = np.zeros((nx + 2 * G, ny + 2 * G), dtype)
+        bp[G:G + nx, G:G + ny] = bed[x0:x1, y0:y1]
+        bx, by = _kinds_axes(kinds)
+        pad_bed(bp, G, bx, by)
+        halo.exchange(torch.from_numpy(bp))
+        local = [("none" if halo.has_neighbor(s) else k) for s, k in zip(SIDES, kinds)]
+        s = _oracle_solver(qp, bp, local, dtype)
+        dts = []
+        for _ in range(NSTEPS):
+            dt = s.rain_step_limit(s.cfl_dt())
+            dt = float(halo.allreduce_min_(torch.tensor([dt], dtype=torch.float64))[0])
+            halo.exchange(torch.from_numpy(s.q))
+            s.step(dt)
+            dts.append(dt)
+        out[rank] = dict(block=(x0, x1, y0, y1), q=s.q[:, G:G + nx, G:G + ny].copy(),
+                         bed=bp.copy(), dts=dts)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,dims,kinds,dtype", [
+    (2, [2, 1], ("wall", "fall", "wall", "wall"), "float32"),
+    (2, [1, 2], ("wall", "fall", "extrapolate", "wall"), "float32"),
+    (2, [2, 1], ("periodic", "periodic", "wall", "wall"), "float64"),
+    (4, [2, 2], ("periodic",) * 4, "float32"),
+    (3, [1, 3], ("fall", "wall", "wall", "fall"), "float64"),
+])
+def test_split_oracle_run_equals_single_domain(world, dims, kinds, dtype):
+    from geoswe_b200.solver import pad_bed
+    out = _spawn(_split_rank, world, dims, kinds, dtype)
+    dt_ = np.dtype(dtype)
+    q0, bed = _oracle_inputs(dt_)
+    qp = np.zeros((3, NX + 2 * G, NY + 2 * G), dt_)
+    qp[:, G:-G, G:-G] = q0
+    bp = np.zeros((NX + 2 * G, NY + 2 * G), dt_)
+    bp[G:-G, G:-G] = bed
+    bx, by = _kinds_axes(kinds)
+    pad_bed(bp, G, bx, by)
+    s = _oracle_solver(qp, bp, list(kinds), dt_)
+    dts = []
+    for _ in range(NSTEPS):
+        dt = s.rain_step_limit(s.cfl_dt())
+        s.step(dt)
+        dts.append(dt)
+    for r in range(world):
+        x0, x1, y0, y1 = out[r]["block"]
+        assert out[r]["dts"] == dts, r
+        np.testing.assert_array_equal(out[r]["q"], s.q[:, G + x0:G + x1, G + y0:G + y1])
+        # the exchanged bed equals the single-domain padded bed away from the corners
+        lb = out[r]["bed"]
+        gb = bp[x0:x1 + 2 * G, y0:y1 + 2 * G]
+        if x0 == 0 and bx == "periodic":
+            gb = None                     # the wrap's image lies at the far end; checked by q
+        if gb is not None and y0 == 0 and by == "periodic":
+            gb = None
+        if gb is not None and x1 == NX and bx == "periodic":
+            gb = None
+        if gb is not None and y1 == NY and by == "periodic":
+            gb = None
+        if gb is not None:
+            np.testing.assert_array_equal(lb[G:-G, :], gb[G:-G, :])
+            np.testing.assert_array_equal(lb[:, G:-G], gb[:, G:-G])
+    assert s.q[0, G:-G, G:-G].max() > 0.5           # a flowing case, not a trivial one

@@ -1,0 +1,90 @@
+"""A dense run split over ranks equals the single-domain run bit for bit.
+
+Two processes share the one GPU, each a rank of a gloo group running ``Solver2D`` on
+its block (faces staged through host memory, as the exchange does for any backend but
+NCCL); the kernels of the two processes never wait on each other -- every wait is on
+the host, in the gloo calls. The single-domain run is this process's own.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from tests._cases import flowing
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+import torch.distributed as dist  # noqa: E402
+import torch.multiprocessing as mp  # noqa: E402
+
+NX, NY, T_END = 46, 37, 6.0
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _make(mesh_shape, bc, dtype, q0, bed, **kw):
+    from geoswe_b200 import Config, Mesh2D, Solver2D
+    mesh = Mesh2D(nx=mesh_shape[0], ny=mesh_shape[1], dx=2.0, dy=2.5, ngh=2)
+    cfg = Config(bc_x=bc[0], bc_y=bc[1], dtype=dtype, friction="manning", manning_n=0.03,
+                 rainfall=80.0 / 3.6e6)
+    return Solver2D(mesh, cfg, q0, bed, **kw)
+
+
+def _rank(rank, world, port, out, dims, bc, dtype, host_loop):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        torch.cuda.set_device(0)
+        from geoswe_b200.partition import block_of
+        q0, bed = flowing(NX, NY, seed=5, dtype=np.dtype(dtype))
+        x0, x1, y0, y1 = block_of(NX, NY, dims, (rank // dims[1], rank % dims[1]))
+        s = _make((x1 - x0, y1 - y0), bc, dtype, q0[:, x0:x1, y0:y1].copy(), bed[x0:x1, y0:y1].copy(),
+                  comm=dist.group.WORLD, dims=dims)
+        refused = False
+        try:
+            s.add_inflow([2], [3], (1.0, 0.0), 2.0, [0.0, 1.0], [1.0, 1.0])
+        except NotImplementedError:
+            refused = True
+        if host_loop:
+            steps = s.run(T_END, callback=lambda solver, k: None)
+        else:
+            steps = s.run(T_END)
+        q = s.q_interior.detach().cpu().numpy().copy()
+        out[rank] = dict(block=(x0, x1, y0, y1), steps=steps, t=s.t, q=q, refused=refused,
+                         exchanges=s.halo.exchanges, launches=s.kernel_launches)
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("dims,bc,dtype,host_loop", [
+    ([2, 1], ("wall", "extrapolate"), "float32", False),
+    ([1, 2], ("wall", "wall"), "float32", False),
+    ([2, 1], ("periodic", "wall"), "float64", True),
+])
+def test_split_run_equals_single_domain(dims, bc, dtype, host_loop):
+    q0, bed = flowing(NX, NY, seed=5, dtype=np.dtype(dtype))
+    ref = _make((NX, NY), bc, dtype, q0, bed)
+    ref_steps = ref.run(T_END, callback=(lambda solver, k: None) if host_loop else None)
+    want = ref.q_interior.detach().cpu().numpy()
+    torch.cuda.synchronize()
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_rank, args=(2, _free_port(), out, dims, bc, dtype, host_loop), nprocs=2,
+                           start_method="spawn", join=True)
+        out = dict(out)
+    assert ref_steps > 20
+    for r in range(2):
+        o = out[r]
+        x0, x1, y0, y1 = o["block"]
+        assert o["refused"], "add_inflow on a split run must raise"
+        assert o["steps"] == ref_steps and o["t"] == ref.t, (r, o["steps"], ref_steps, o["t"], ref.t)
+        assert o["exchanges"] >= ref_steps and o["launches"] > 0
+        np.testing.assert_array_equal(o["q"], want[:, x0:x1, y0:y1])
