@@ -12,7 +12,7 @@ from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["strip_bounds", "block_of"]
+__all__ = ["strip_bounds", "block_of", "members_of"]
 
 
 def _shares(n_ranks, weights):
@@ -63,6 +63,18 @@ def strip_bounds(col_work, n_ranks, weights=None):
         if bnd[r] > bnd[r + 1] - 1:
             bnd[r] = bnd[r + 1] - 1
     return bnd
+
+
+def members_of(member_work, n_ranks, rank, weights=None):
+    """The ensemble members (a contiguous ``range`` of member indices) that ``rank``
+    advances when an ensemble is spread over ``n_ranks`` GPUs: members are independent,
+    so each rank runs its share as its own ``Ensemble`` and nothing is exchanged.
+    ``member_work`` is each member's work (its active cells, say) or a member count."""
+    bnd = strip_bounds(member_work, n_ranks, weights)
+    rank = int(rank)
+    if not 0 <= rank < int(n_ranks):
+        raise ValueError(f"members_of: rank {rank} outside 0..{int(n_ranks) - 1}")
+    return range(bnd[rank], bnd[rank + 1])
 
 
 def block_of(nx, ny, dims, coords, x_work=None, y_work=None):

@@ -93,6 +93,17 @@ def test_blocks_tile_the_grid():
     assert (cover == 1).all()
 
 
+def test_members_split_by_work():
+    from geoswe_b200.partition import members_of
+    work = [100] * 48 + [400] * 16                  # 64 members, the last 16 four times larger
+    parts = [members_of(work, 4, r) for r in range(4)]
+    assert [p.start for p in parts] == [0, 28, 50, 57] and parts[-1].stop == 64
+    assert [sum(work[i] for i in p) for p in parts] == [2800] * 4
+    assert list(members_of(64, 8, 3)) == list(range(24, 32))
+    with pytest.raises(ValueError, match="rank"):
+        members_of(64, 8, 8)
+
+
 def test_face_extent_message():
     """Mirrors the reference's check (mpi_halo.py:256-275): only the extent along the
     face must agree, and the message names the face, the rank and both extents."""
