@@ -161,6 +161,8 @@ class FlatAdjoint:
     def __init__(self, cs: CompressedSolver, *, gauges: Sequence[int], n_steps: int, window: int,
                  snapshots: int = 55, dtype: str = "float32", rain_times=None, rain_base=None,
                  inlet: Optional[Inlet] = None):
+        if getattr(cs, "flat_halo", None) is not None:
+            raise NotImplementedError("FlatAdjoint: the adjoint of a run split over ranks is not supported")
         if window < 1 or window > n_steps:
             raise ValueError("window must be in [1, n_steps]")
         if dtype not in ("float32", "float64"):

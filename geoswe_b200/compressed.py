@@ -90,9 +90,18 @@ def build_bricks(stored_pad: np.ndarray, brick_h: int):
 
 
 class CompressedSolver:
-    """Shallow-water solver on the compressed active-cell mesh (GPU, float32)."""
+    """Shallow-water solver on the compressed active-cell mesh (GPU, float32).
+
+    Built by ``from_dense`` from a ``Solver2D`` split over ranks (``comm=``), it runs this
+    rank's block: the neighbours' inside cells in the seam ghost rows are stored but not
+    updated here, and before every step ``halo.FlatHalo`` refreshes them from the ranks
+    that own them; the wave speed is the maximum over the ranks. The blocks equal the
+    single-domain compressed run bit for bit (compressed_solver.py:1069-1310, 3079-3087).
+    """
 
     brick_h = 16
+    halo = None
+    flat_halo = None
 
     @classmethod
     def from_dense(cls, s: Solver2D, *, cfl_linf: bool = False, dt_max=None, brick_h: Optional[int] = None,
@@ -143,7 +152,18 @@ class CompressedSolver:
             inside[g_:-g_, g_:-g_] = 1
         else:
             inside = s._mask[:, :s.nyp].contiguous()
-        sl, lin, ii, jj = self._build_layout(inside)
+        halo = getattr(s, "halo", None)
+        if halo is None:
+            sl, lin, ii, jj = self._build_layout(inside)
+        else:
+            if any(halo.periods):
+                raise ValueError("CompressedSolver.from_dense: a split run with a periodic axis cannot be "
+                                 "compressed (the compressed mesh has no periodic closure)")
+            # the neighbours' inside cells in the seam ghost rows join the stored set's
+            # seed, so every cell an active stencil here reads is stored on both ranks
+            ext = inside.to(torch.float32)
+            halo.exchange(ext)
+            sl, lin, ii, jj = self._build_layout((ext > 0.5).to(torch.uint8), active=inside)
         pidx_of_slot = ii * s.pitch + jj
 
         def pack_dense(field2d_pitched, dtype=torch.float32):
@@ -173,6 +193,12 @@ class CompressedSolver:
             self._ncls = None
             self._ntab = torch.tensor([n], dtype=torch.float32, device=dev)
         self._init_runtime(track_max_depth)
+        if halo is not None:
+            from .halo import FlatHalo
+            slot_pad = torch.full((s.nxp * s.nyp,), -1, dtype=torch.int64, device=dev)
+            slot_pad[lin] = sl
+            self.halo = halo
+            self.flat_halo = FlatHalo(halo, slot_pad.reshape(s.nxp, s.nyp))
         self.build_seconds = time.perf_counter() - t0
         if say:
             say(f"[compressed] N_active={self.N_active} N_stored={self.N_stored} bricks={self.n_bricks} "
@@ -287,13 +313,17 @@ class CompressedSolver:
         self.dt_max_user = dt_max
         self._dense_had_rain = False
 
-    def _build_layout(self, inside):
+    def _build_layout(self, inside, active=None):
         """Stored set (the inside mask dilated twice with the 4-neighbour cross,
         compressed_rhs.py:256), Hilbert bricks, the canonical id -> slot map and the slot
-        flags. `inside` is a device uint8 (nxp, nyp) mask. Returns (slots, padded linear
-        index, i, j) of every stored cell."""
+        flags. `inside` is a device uint8 (nxp, nyp) mask; `active` (default `inside`)
+        marks the cells this solver updates -- on a split run `inside` also holds the
+        neighbours' inside cells in the seam ghost rows, stored but not updated here.
+        Returns (slots, padded linear index, i, j) of every stored cell."""
         dev = self.device
         self._inside = inside
+        if active is None:
+            active = inside
         st = inside.bool()
         for _ in range(2):
             d = st.clone()
@@ -304,7 +334,7 @@ class CompressedSolver:
             st = d
         self._stored = st
         self.N_stored = int(st.sum())
-        self.N_active = int(inside.sum())
+        self.N_active = int(active.sum())
         if self.N_stored == 0:
             raise ValueError(_DEGENERATE)
         bij, bnbr = build_bricks(st.to(torch.uint8).cpu().numpy(), self.brick_h)
@@ -331,7 +361,7 @@ class CompressedSolver:
         slot_of[k] = sl
         self._slot = slot_of
         flags = torch.zeros(self.nslots, dtype=torch.uint8, device=dev)
-        flags[sl] = (1 + 2 * inside.reshape(-1)[lin].to(torch.uint8))
+        flags[sl] = (1 + 2 * active.reshape(-1)[lin].to(torch.uint8))
         self._flags = flags
         self._tables_cache = None
         self._slot_cells = sl
@@ -366,6 +396,10 @@ class CompressedSolver:
         self.t = 0.0
         self.nsteps = 0
         self.kernel_launches = 0
+        self.halo = None
+        self.flat_halo = None
+        lam = L.GswLoopState.lam_bits.offset // 8
+        self._lam_view = self._state.view(torch.int64)[lam:lam + 1]   # the wave-speed bits
 
     # ------------------------------------------------------------- forcings
     def set_rain(self, rain):
@@ -782,7 +816,13 @@ class CompressedSolver:
                           "here. from_dense does not carry rainfall over; pass the same RainfallForcing "
                           "to set_rain().", stacklevel=2)
         dm = dt_max if dt_max is not None else self.dt_max_user
+        split = self.flat_halo is not None
+        if split and (self._inflows or self._ring is not None or self._forcing or every > 0.0):
+            raise NotImplementedError("CompressedSolver.run: a run split over ranks takes rain and friction "
+                                      "only (no inlets, ring stage, flat-loop forcings or checkpoints)")
         K = int(window) if window else self._window_size()
+        if split and not window:
+            K = min(K, 32)     # launched eagerly: poll often, so few no-op steps follow the end
         if max_steps and max_steps < K and not window:
             K = int(max_steps)
         K += K % 2
@@ -802,8 +842,12 @@ class CompressedSolver:
 
         def one_step(k_parity):
             s = _stream()
+            if split:                           # every rank takes the dt of the largest wave speed
+                self.halo.allreduce_max_(self._lam_view)
             L.call("gsw_dt_finalize_dev", _ptr(self._dtp_dev), _ptr(self._state), s)
             src, dst = self._q[k_parity], self._q[1 - k_parity]
+            if split:                           # seam ghosts from the neighbours, before the step
+                self.flat_halo.exchange(src)
             for f in self._inflows:             # inlet ghosts at t_n, before the step
                 L.call("gsw_flat_inflow_apply", C.byref(self._inflow_args(f, src)), s)
             a = self._args(src, dst)
@@ -830,10 +874,16 @@ class CompressedSolver:
             self.kernel_launches += per_step
         key = (K, self._rain_kind, len(self._inflows), self._ring is not None, self.warps, self.min_blocks, self.segments,
                tuple(sorted(self._forcing)))
-        g, per = _cached_graph(self._graph_cache, key, one_window, self.device)
+        if split:                               # the step sequence holds collectives: eager
+            g, per = None, 0
+        else:
+            g, per = _cached_graph(self._graph_cache, key, one_window, self.device)
         self.kernel_launches += 1
         while True:
-            g.replay()
+            if g is None:
+                per = one_window()
+            else:
+                g.replay()
             self.kernel_launches += per
             st = self._read_state()
             if st.done:
@@ -891,6 +941,8 @@ class CompressedSolver:
         `missing_ok`."""
         import json
         import os
+        if self.flat_halo is not None:
+            raise NotImplementedError("load_checkpoint: checkpoints of a run split over ranks are not supported")
         mp = os.path.join(ckpt_dir, "ckpt_meta.json")
         if not os.path.exists(mp):
             if missing_ok:
@@ -928,6 +980,8 @@ class CompressedSolver:
         reference's cache format (save_cache, compressed_solver.py:2504-2560), which its
         run_cached and from_cache here both read. Inlets are not part of the format (the
         reference passes them to run_cached)."""
+        if self.flat_halo is not None:
+            raise NotImplementedError("save_cache: caches of a run split over ranks are not supported")
         import json
         import os
         os.makedirs(cache_dir, exist_ok=True)

@@ -34,6 +34,9 @@ class Ensemble:
     def __init__(self, members: Sequence[CompressedSolver], *, warps: int = 0, grid: int = 0):
         if not members:
             raise ValueError("Ensemble: no members")
+        if any(getattr(m, "flat_halo", None) is not None for m in members):
+            raise ValueError("Ensemble: a member split over ranks cannot join an ensemble; spread whole "
+                             "members over the ranks instead (partition.members_of)")
         bh = {m.brick_h for m in members}
         if len(bh) != 1:
             raise ValueError(f"Ensemble: members must share brick_h (got {sorted(bh)})")

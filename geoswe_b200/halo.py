@@ -31,7 +31,7 @@ from typing import Optional
 import torch
 import torch.distributed as dist
 
-__all__ = ["Halo2D", "compute_dims", "check_face_extent", "comm_size", "SIDES"]
+__all__ = ["Halo2D", "FlatHalo", "compute_dims", "check_face_extent", "comm_size", "SIDES"]
 
 SIDES = ("x-", "x+", "y-", "y+")
 _OPPOSITE = {"x-": "x+", "x+": "x-", "y-": "y+", "y+": "y-"}
@@ -208,22 +208,28 @@ class Halo2D:
         sides = [s for s in SIDES if self.has_neighbor(s)]
         for s in sides:
             bufs[s][0].copy_(faces[s][0])
+        works = self.post({s: bufs[s][0] for s in sides}, {s: bufs[s][1] for s in sides})
+        self.exchanges += 1
+        return {"works": works, "faces": faces, "bufs": bufs, "sides": sides}
+
+    def post(self, sends, recvs):
+        """Post one contiguous buffer to the neighbour across each side in ``sends`` and
+        a receive from it into ``recvs[side]``; returns the works to wait on. The
+        buffers are on the device for NCCL, in host memory otherwise."""
         ops = []
         # per axis: sends towards - then +, receives from + then -; so where both faces
         # of an axis border the same rank (two ranks on a periodic axis) the i-th message
         # between a pair lands in the i-th receive, with or without tags
         for lo, hi in (("x-", "x+"), ("y-", "y+")):
             for s in (lo, hi):
-                if s in bufs:
-                    ops.append(dist.P2POp(dist.isend, bufs[s][0], self._peer(self._neighbor(s)),
+                if s in sends:
+                    ops.append(dist.P2POp(dist.isend, sends[s], self._peer(self._neighbor(s)),
                                           self.group, _TAG[_OPPOSITE[s]]))
             for s in (hi, lo):
-                if s in bufs:
-                    ops.append(dist.P2POp(dist.irecv, bufs[s][1], self._peer(self._neighbor(s)),
+                if s in recvs:
+                    ops.append(dist.P2POp(dist.irecv, recvs[s], self._peer(self._neighbor(s)),
                                           self.group, _TAG[s]))
-        works = dist.batch_isend_irecv(ops) if ops else []
-        self.exchanges += 1
-        return {"works": works, "faces": faces, "bufs": bufs, "sides": sides}
+        return dist.batch_isend_irecv(ops) if ops else []
 
     def wait_exchange(self, handle):
         """Complete the exchange: wait for the transfers, then unpack the received
@@ -258,3 +264,74 @@ class Halo2D:
         dist.all_reduce(h, op=dist.ReduceOp.MIN, group=self.group)
         t.copy_(h)
         return t
+
+
+class FlatHalo:
+    """Seam exchange of the compressed mesh, the reference's ``CompressedHalo``
+    (compressed_solver.py:1069-1132) on this package's brick slots.
+
+    For each face that borders another rank, the stored cells of the ``ngh`` rows
+    (columns) next to the face are gathered into a dense ``(3, ngh, P)`` buffer at
+    ``(offset from the face's first row, position along the face)`` -- ``P = nyp`` for
+    an x face, ``nxp`` for a y face -- and the neighbour scatters the positions of its
+    own stored ghost cells out of it. Dense positions make the two ranks agree on the
+    cell order whatever their stored sets are; a position the sender does not store
+    arrives as 0, and only at a ghost cell that no active cell of the receiver reads.
+
+    ``slot_pad`` is the ``(nxp, nyp)`` map of padded cell -> brick slot (-1 where not
+    stored). The state planes exchanged are flat slot arrays."""
+
+    def __init__(self, halo: Halo2D, slot_pad):
+        self.halo = halo
+        g, nxp, nyp = halo.ngh, halo.nxp, halo.nyp
+        if tuple(slot_pad.shape) != (nxp, nyp):
+            raise ValueError(f"FlatHalo: slot map {tuple(slot_pad.shape)} is not ({nxp}, {nyp})")
+        dev = slot_pad.device
+        self.staged = not halo.device_direct and dev.type != "cpu"
+        self.faces = {}
+        for side in SIDES:
+            if not halo.has_neighbor(side):
+                continue
+            if side[0] == "x":
+                send = (slice(g, 2 * g) if side == "x-" else slice(nxp - 2 * g, nxp - g), slice(None))
+                recv = (slice(0, g) if side == "x-" else slice(nxp - g, nxp), slice(None))
+                sblk, rblk, P = slot_pad[send], slot_pad[recv], nyp
+            else:
+                send = (slice(None), slice(g, 2 * g) if side == "y-" else slice(nyp - 2 * g, nyp - g))
+                recv = (slice(None), slice(0, g) if side == "y-" else slice(nyp - g, nyp))
+                sblk, rblk, P = slot_pad[send].t(), slot_pad[recv].t(), nxp
+            sflat, rflat = sblk.reshape(-1), rblk.reshape(-1)
+            spos = torch.nonzero(sflat >= 0).reshape(-1)
+            rpos = torch.nonzero(rflat >= 0).reshape(-1)
+            f = dict(P=P, spos=spos, sslot=sflat[spos], rpos=rpos, rslot=rflat[rpos],
+                     sdense=torch.zeros((3, g * P), dtype=torch.float32, device=dev),
+                     rdense=torch.zeros((3, g * P), dtype=torch.float32, device=dev))
+            if self.staged:
+                pin = torch.cuda.is_available()
+                f["shost"] = torch.zeros((3, g * P), dtype=torch.float32, pin_memory=pin)
+                f["rhost"] = torch.zeros((3, g * P), dtype=torch.float32, pin_memory=pin)
+            self.faces[side] = f
+        self.exchanges = 0
+
+    def send_cells(self, side):
+        return int(self.faces[side]["spos"].numel()) if side in self.faces else 0
+
+    def exchange(self, planes):
+        """Refresh the stored seam ghost cells of the three flat planes in place."""
+        sends, recvs = {}, {}
+        for side, f in self.faces.items():
+            for c in range(3):
+                f["sdense"][c].index_copy_(0, f["spos"], planes[c].index_select(0, f["sslot"]))
+            if self.staged:
+                f["shost"].copy_(f["sdense"])
+                sends[side], recvs[side] = f["shost"], f["rhost"]
+            else:
+                sends[side], recvs[side] = f["sdense"], f["rdense"]
+        for w in self.halo.post(sends, recvs):
+            w.wait()
+        for side, f in self.faces.items():
+            if self.staged:
+                f["rdense"].copy_(f["rhost"])
+            for c in range(3):
+                planes[c].index_copy_(0, f["rslot"], f["rdense"][c].index_select(0, f["rpos"]))
+        self.exchanges += 1

@@ -293,3 +293,64 @@ def test_split_oracle_run_equals_single_domain(world, dims, kinds, dtype):
             np.testing.assert_array_equal(lb[G:-G, :], gb[G:-G, :])
             np.testing.assert_array_equal(lb[:, G:-G], gb[:, G:-G])
     assert s.q[0, G:-G, G:-G].max() > 0.5           # a flowing case, not a trivial one
+
+
+# ------------------------------------------------------------------ compressed-mesh seams
+def _flat_rank(rank, world, port, out, dims):
+    _init(rank, world, port)
+    try:
+        from geoswe_b200.halo import FlatHalo
+        rng = np.random.default_rng(11)
+        glob = rng.random((NX + 2 * G, NY + 2 * G)) < 0.7          # stored cells, global padded frame
+        cx, cy = rank // dims[1], rank % dims[1]
+        x0, x1, y0, y1 = block_of(NX, NY, dims, (cx, cy))
+        nxp, nyp = x1 - x0 + 2 * G, y1 - y0 + 2 * G
+        halo = Halo2D(None, nxp, nyp, G, dtype="float32", dims=dims)
+        stored = glob[x0:x0 + nxp, y0:y0 + nyp].copy()
+        ghost = np.ones((nxp, nyp), bool)
+        ghost[G:-G, G:-G] = False
+        extra = ghost & ~stored & (np.random.default_rng(100 + rank).random((nxp, nyp)) < 0.3)
+        stored |= extra                                              # ghosts the owner does not store
+        n = int(stored.sum())
+        slots = np.random.default_rng(200 + rank).permutation(n + 5)[:n]
+        slot_pad = np.full((nxp, nyp), -1, np.int64)
+        slot_pad[stored] = slots
+        planes = [torch.full((n + 5,), -1.0) for _ in range(3)]
+        ii, jj = np.nonzero(stored & ~ghost)
+        for c in range(3):
+            planes[c][torch.from_numpy(slot_pad[ii, jj])] = torch.from_numpy(
+                (c * 1e6 + (x0 + ii - G) * 1000 + (y0 + jj - G)).astype(np.float32))
+        fh = FlatHalo(halo, torch.from_numpy(slot_pad))
+        fh.exchange(planes)
+        bad = []
+        for i, j in zip(*np.nonzero(stored)):
+            got = [float(planes[c][slot_pad[i, j]]) for c in range(3)]
+            inner_i, inner_j = G <= i < nxp - G, G <= j < nyp - G
+            if inner_i and inner_j:
+                want = [c * 1e6 + (x0 + i - G) * 1000 + (y0 + j - G) for c in range(3)]
+            elif not (inner_i or inner_j):
+                continue     # corners: a y face spans the full x extent, as the reference's does
+            else:
+                side = ("x-" if i < G else "x+") if not inner_i else ("y-" if j < G else "y+")
+                if not halo.has_neighbor(side):
+                    want = [-1.0] * 3
+                elif extra[i, j]:
+                    want = [0.0] * 3                                 # the sender stores no such cell
+                else:
+                    want = [c * 1e6 + (x0 + i - G) * 1000 + (y0 + j - G) for c in range(3)]
+            if got != want:
+                bad.append((int(i), int(j), got, want))
+        untouched = all(float(planes[c][s]) == -1.0 for c in range(3)
+                        for s in sorted(set(range(n + 5)) - set(slots.tolist())))
+        out[rank] = dict(nbad=len(bad), bad=bad[:4], untouched=untouched,
+                         sent=sum(fh.send_cells(s) for s in SIDES))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,dims", [(2, [2, 1]), (2, [1, 2]), (4, [2, 2])])
+def test_flat_seam_exchange(world, dims):
+    out = _spawn(_flat_rank, world, dims)
+    for r in range(world):
+        assert out[r]["nbad"] == 0, (r, out[r]["bad"])
+        assert out[r]["untouched"] and out[r]["sent"] > 0
