@@ -207,6 +207,27 @@ def test_graph_replay_equals_eager():
     assert same(out[0][2][:, 2:-2, 2:-2], out[1][2][:, 2:-2, 2:-2])
 
 
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_host_loop_equals_device_loop(dtype):
+    """run(callback=...) -- cfl_dt read back and step(dt) from the host each step, the
+    reference's own loop (solver.py:2975-3027) -- equals the device loop bit for bit,
+    with rain (its dt limit) and friction on."""
+    from geoswe_b200 import Config, Mesh2D, Solver2D
+    q0, bed = flowing(52, 47, seed=4, dtype=np.dtype(dtype))
+    out = []
+    for host in (True, False):
+        mesh = Mesh2D(nx=52, ny=47, dx=2.0, dy=2.5, ngh=2)
+        s = Solver2D(mesh, Config(bc_x="wall", bc_y="fall", dtype=dtype, friction="manning",
+                                  manning_n=0.03, rainfall=80.0 / 3.6e6), q0, bed)
+        calls = []
+        n = s.run(t_end=9.0, callback=(lambda solver, k: calls.append(k)) if host else None)
+        out.append((n, s.t, s.q_interior.cpu().numpy().copy()))
+        if host:
+            assert calls == list(range(1, n + 1))
+    assert out[0][0] == out[1][0] > 20 and out[0][1] == out[1][1] == 9.0
+    assert same(out[0][2], out[1][2])
+
+
 def test_segmented_runs_reuse_one_graph():
     """run() called interval by interval (new t_end each call, odd step counts, so the
     calls start on either buffer) equals one run to the last t_end bit for bit, and
