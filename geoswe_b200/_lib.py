@@ -121,6 +121,12 @@ class GswFlatForcingArgs(C.Structure):
                 ("dr_slots", vp), ("dr_htgt", vp)]
 
 
+class GswSeamArgs(C.Structure):
+    _fields_ = [("abi_version", u32), ("dtype", i32), ("q0", vp), ("q1", vp), ("q2", vp), ("nslots", i64),
+                ("slot", vp), ("pos", vp), ("n", i64), ("dense", vp), ("stride", i64), ("scatter", i32),
+                ("reserved", i32)]
+
+
 class GswMember(C.Structure):
     _fields_ = [("dt", GswDtParams), ("inv_dx", C.c_float), ("g", C.c_float), ("h_min", C.c_float),
                 ("h_min_cfl", C.c_float), ("vcap", C.c_float), ("linf", i32), ("quadratic", i32),
@@ -159,6 +165,7 @@ _PROTOS = {
     "gsw_flat_inflow_apply": [C.POINTER(GswFlatInflowArgs), vp],
     "gsw_flat_forcings": [C.POINTER(GswFlatForcingArgs), vp],
     "gsw_flat_ring_stage": [C.POINTER(GswFlatRingArgs), vp],
+    "gsw_seam_copy": [C.POINTER(GswSeamArgs), vp],
     "gsw_adj_flat_step": [C.POINTER(GswFlatAdjArgs), vp],
     "gsw_adj_flat_inflow": [C.POINTER(GswFlatInflowArgs), vp, vp, vp, vp, vp],
     "gsw_gauge_record": [C.POINTER(GswGaugeArgs), vp],

@@ -198,7 +198,7 @@ class CompressedSolver:
             slot_pad = torch.full((s.nxp * s.nyp,), -1, dtype=torch.int64, device=dev)
             slot_pad[lin] = sl
             self.halo = halo
-            self.flat_halo = FlatHalo(halo, slot_pad.reshape(s.nxp, s.nyp))
+            self.flat_halo = FlatHalo(halo, slot_pad.reshape(s.nxp, s.nyp), nslots=self.nslots)
         self.build_seconds = time.perf_counter() - t0
         if say:
             say(f"[compressed] N_active={self.N_active} N_stored={self.N_stored} bricks={self.n_bricks} "
@@ -839,6 +839,8 @@ class CompressedSolver:
 
         forced = bool(self._forcing)
         per_step = 2 + len(self._inflows) + (self._ring is not None) + 3 * forced
+        if split:
+            per_step += self.flat_halo.launches_per_exchange
 
         def one_step(k_parity):
             s = _stream()

@@ -279,14 +279,20 @@ class FlatHalo:
     arrives as 0, and only at a ghost cell that no active cell of the receiver reads.
 
     ``slot_pad`` is the ``(nxp, nyp)`` map of padded cell -> brick slot (-1 where not
-    stored). The state planes exchanged are flat slot arrays."""
+    stored), ``nslots`` the length of the flat slot arrays exchanged. On the device one
+    libgsw launch (``gsw_seam_copy``) packs or unpacks all three planes of a face; host
+    planes (the CPU tests of this exchange) are indexed in place."""
 
-    def __init__(self, halo: Halo2D, slot_pad):
+    def __init__(self, halo: Halo2D, slot_pad, nslots: Optional[int] = None):
         self.halo = halo
         g, nxp, nyp = halo.ngh, halo.nxp, halo.nyp
         if tuple(slot_pad.shape) != (nxp, nyp):
             raise ValueError(f"FlatHalo: slot map {tuple(slot_pad.shape)} is not ({nxp}, {nyp})")
         dev = slot_pad.device
+        top = int(slot_pad.max()) if slot_pad.numel() else -1
+        if nslots is not None and top >= int(nslots):
+            raise ValueError(f"FlatHalo: slot {top} outside the {int(nslots)} slots of the state")
+        self.nslots = None if nslots is None else int(nslots)
         self.staged = not halo.device_direct and dev.type != "cpu"
         self.faces = {}
         for side in SIDES:
@@ -316,12 +322,39 @@ class FlatHalo:
     def send_cells(self, side):
         return int(self.faces[side]["spos"].numel()) if side in self.faces else 0
 
+    @property
+    def launches_per_exchange(self):
+        """libgsw launches of one exchange of device planes (a pack and an unpack per face)."""
+        return 2 * len(self.faces)
+
+    def _seam(self, planes, slot, pos, dense, scatter):
+        import ctypes as C
+        from . import _lib as L
+        if self.nslots is not None and planes[0].numel() != self.nslots:
+            raise ValueError(f"FlatHalo: planes of {planes[0].numel()} slots, built for {self.nslots}")
+        a = L.GswSeamArgs()
+        a.abi_version = L.ABI_VERSION
+        a.dtype = L.F32 if planes[0].dtype == torch.float32 else L.F64
+        a.q0, a.q1, a.q2 = (C.c_void_p(p.data_ptr()) for p in planes)
+        a.nslots = planes[0].numel()
+        a.slot, a.pos = C.c_void_p(slot.data_ptr()), C.c_void_p(pos.data_ptr())
+        a.n = slot.numel()
+        a.dense, a.stride = C.c_void_p(dense.data_ptr()), dense.shape[1]
+        a.scatter = int(scatter)
+        L.call("gsw_seam_copy", C.byref(a), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+
     def exchange(self, planes):
         """Refresh the stored seam ghost cells of the three flat planes in place."""
+        device = planes[0].device.type != "cpu"
+        if any(p.dtype != torch.float32 for p in planes):
+            raise ValueError("FlatHalo: the compressed state is float32")
         sends, recvs = {}, {}
         for side, f in self.faces.items():
-            for c in range(3):
-                f["sdense"][c].index_copy_(0, f["spos"], planes[c].index_select(0, f["sslot"]))
+            if device:
+                self._seam(planes, f["sslot"], f["spos"], f["sdense"], 0)
+            else:
+                for c in range(3):
+                    f["sdense"][c].index_copy_(0, f["spos"], planes[c].index_select(0, f["sslot"]))
             if self.staged:
                 f["shost"].copy_(f["sdense"])
                 sends[side], recvs[side] = f["shost"], f["rhost"]
@@ -332,6 +365,9 @@ class FlatHalo:
         for side, f in self.faces.items():
             if self.staged:
                 f["rdense"].copy_(f["rhost"])
-            for c in range(3):
-                planes[c].index_copy_(0, f["rslot"], f["rdense"][c].index_select(0, f["rpos"]))
+            if device:
+                self._seam(planes, f["rslot"], f["rpos"], f["rdense"], 1)
+            else:
+                for c in range(3):
+                    planes[c].index_copy_(0, f["rslot"], f["rdense"][c].index_select(0, f["rpos"]))
         self.exchanges += 1

@@ -569,6 +569,31 @@ GSW_API int gsw_flat_autotune(const GswFlatArgs* a, int32_t reps, int32_t use_ca
                               void* stream);
 
 /* ------------------------------------------------------------------------- */
+/* Split runs                                                                 */
+/* ------------------------------------------------------------------------- */
+/* Seam exchange of a compressed mesh split over ranks: the pack and unpack of the
+ * reference's CompressedHalo (geoswe/compressed_solver.py:1069-1132, its per-face
+ * gathers into and scatters out of a dense (3, ngh, P) face buffer), on brick slots.
+ *   scatter = 0: dense[c * stride + pos[k]] = q_c[slot[k]]      (gather, before sending)
+ *   scatter = 1: q_c[slot[k]] = dense[c * stride + pos[k]]      (after receiving)
+ * for k < n and c = 0, 1, 2. An entry with slot outside [0, nslots) or pos outside
+ * [0, stride) is skipped (the caller validates both lists once, when it builds them). */
+typedef struct GswSeamArgs {
+    uint32_t abi_version;
+    int32_t  dtype;          /* GSW_F32 or GSW_F64 */
+    void* q0; void* q1; void* q2;
+    int64_t  nslots;
+    const int64_t* slot;     /* n brick slots */
+    const int64_t* pos;      /* n dense positions */
+    int64_t  n;
+    void*    dense;          /* 3 * stride elements */
+    int64_t  stride;
+    int32_t  scatter;
+    int32_t  reserved;
+} GswSeamArgs;
+GSW_API int gsw_seam_copy(const GswSeamArgs* a, void* stream);
+
+/* ------------------------------------------------------------------------- */
 /* Library                                                                    */
 /* ------------------------------------------------------------------------- */
 /* RN(1/g) when the reciprocal-and-remainder sequence the step uses for the HLLC star

@@ -43,7 +43,8 @@ def test_struct_layouts_match_c(tmp_path):
                               "ny", "n_tab_len", "vcap", "keep_h", "max_h", "warps"],
               "GswMember": ["dt", "inv_dx", "vcap", "linf", "rain_kind", "rain", "n_tab"],
               "GswEnsembleArgs": ["n_bricks", "n_members", "grid", "brick_ij", "flags", "q0", "bed",
-                                  "members", "states", "scratch", "all_done"]}
+                                  "members", "states", "scratch", "all_done"],
+              "GswSeamArgs": ["q0", "nslots", "slot", "pos", "n", "dense", "stride", "scatter", "reserved"]}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{ROOT}/include/gsw.h"', "int main(){"]
     for s, fs in checks.items():
         lines.append(f'printf("{s} %zu\\n", sizeof({s}));')

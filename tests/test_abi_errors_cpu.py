@@ -94,3 +94,15 @@ def test_constant_reciprocal_check():
     assert lib.gsw_div_const_recip(0.0) == 0.0
     assert lib.gsw_div_const_recip(-9.81) == 0.0
     assert lib.gsw_div_const_recip(float("inf")) == 0.0
+
+
+def test_seam_copy_checks():
+    a = L.GswSeamArgs()
+    a.abi_version, a.dtype, a.n, a.stride = L.ABI_VERSION, L.F32, 0, 8
+    assert _call("gsw_seam_copy", C.byref(a), None)[0] == L.OK            # nothing to move
+    a.n = 4
+    rc, msg = _call("gsw_seam_copy", C.byref(a), None)
+    assert rc == L.ERR_INVALID and "null" in msg
+    a.stride = 0
+    rc, msg = _call("gsw_seam_copy", C.byref(a), None)
+    assert rc == L.ERR_INVALID and "stride" in msg
