@@ -108,18 +108,21 @@ def build_case(n, dtype="float32", seed=0):
     return z, cls
 
 
-def make_solver(z, cls, n, dtype="float32", arith="exact"):
+def make_solver(z, cls, n, dtype="float32", arith="exact", block=None, comm=None, dims=None):
+    """The rain-on-terrain solver; with `block` = (x0, x1, y0, y1) and `comm`, this rank's
+    block of the domain split over the ranks of `comm`."""
     from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
     from geoswe_b200.synthetic import MANNING_CLASSES
-    mesh = Mesh2D(nx=n, ny=n, dx=3.0, dy=3.0, ngh=2)
+    x0, x1, y0, y1 = block if block is not None else (0, n, 0, n)
+    mesh = Mesh2D(nx=x1 - x0, ny=y1 - y0, dx=3.0, dy=3.0, ngh=2)
     cfg = Config(bc_x="wall", bc_y="wall", bc={"x+": "fall"}, cfl=0.5, dtype=dtype,
                  friction="manning", arith=arith,
                  rainfall_forcing=RainfallForcing(time_s=[0.0, 1e9], rate_mm_h=[50.0, 50.0]))
-    q0 = np.zeros((3, n, n), np.float32)
-    s = Solver2D(mesh, cfg, q0, z)
+    q0 = np.zeros((3, x1 - x0, y1 - y0), np.float32)
+    s = Solver2D(mesh, cfg, q0, z[x0:x1, y0:y1], comm=comm, dims=dims)
     ngh = mesh.ngh
-    clsp = np.pad(cls, ngh, mode="edge")
-    s.set_manning_table(clsp, MANNING_CLASSES)
+    clsp = np.pad(cls, ngh, mode="edge")[x0:x1 + 2 * ngh, y0:y1 + 2 * ngh]
+    s.set_manning_table(np.ascontiguousarray(clsp), MANNING_CLASSES)
     return s
 
 
@@ -268,6 +271,50 @@ def run_gsw(args, rank, world):
     if rank == 0 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
+
+
+def run_split(args, rank, world):
+    """``--split``: ONE n x n rain-on-terrain domain cut into ``world`` row strips
+    (``Solver2D(comm=...)``): every step each rank fills its seam ghosts from its
+    neighbours and all ranks take the dt of the largest wave speed. Strong scaling:
+    ``value`` is the whole domain's cell-updates/s over the slowest rank's time."""
+    import torch
+    import torch.distributed as dist
+    from geoswe_b200.partition import block_of
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)) % torch.cuda.device_count())
+    n = args.n
+    z, cls = build_case(n)
+    dims = [world, 1]
+    block = block_of(n, n, dims, (rank, 0))
+    s = make_solver(z, cls, n, block=block, comm=dist.group.WORLD if world > 1 else None, dims=dims)
+    s.run(t_end=1e12, max_steps=args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = Clocks(int(os.environ.get("LOCAL_RANK", 0)) % torch.cuda.device_count())
+    clk.start()
+    l0 = s.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    steps = s.run(t_end=1e12, max_steps=args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    assert steps == args.steps, (steps, args.steps)
+    backend = dist.get_backend() if world > 1 else "none"
+    if world > 1:
+        ms = max_over_ranks(ms, "cuda" if backend == "nccl" else "cpu")
+    cfg = dense_config(n, world)
+    cfg["parallelism"] = f"row strips x{world}: halo exchange + wave-speed all-reduce ({backend})"
+    gpus = min(world, torch.cuda.device_count())
+    return {"metric": METRIC, "value": n * n * steps / (ms / 1e3), "unit": UNIT, "n_gpus": gpus, "ranks": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": cfg, "gpu_launches": int(s.kernel_launches - l0),
+            "halo_exchanges": int(s.halo.exchanges) if s.halo is not None else 0,
+            "block": list(block), "clocks": clocks, "mode": "split"}
 
 
 def time_step_kernel(s, reps=20):
@@ -770,7 +817,8 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gsw", choices=["gsw", "reference"])
-    ap.add_argument("--n", type=int, default=8192)
+    ap.add_argument("--n", "--grid", dest="n", type=int, default=8192,
+                    help="grid side (--grid under torchrun, whose own options --n would abbreviate)")
     ap.add_argument("--kernel-reps", type=int, default=20)
     ap.add_argument("--cpu-n", type=int, default=512)
     ap.add_argument("--cpu-steps", type=int, default=20)
@@ -801,6 +849,10 @@ def main():
     ap.add_argument("--ens-window", type=int, default=32)
     ap.add_argument("--ens-warps", type=int, default=0)
     ap.add_argument("--ens-grid", type=int, default=0)
+    ap.add_argument("--split", action="store_true",
+                    help="one domain cut into row strips over the ranks (strong scaling) instead of replicas")
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process group of --split (gloo: host-staged, for several ranks on one GPU)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -816,6 +868,17 @@ def main():
             out = {"ensemble": run_ensemble, "adjoint": run_adjoint, "tidal": run_tidal, "dambreak": run_dambreak,
                    "compressed": run_compressed}[args.case](args)
             print(json.dumps(out), flush=True)
+        return 0
+    if args.split:
+        import datetime
+        import torch
+        if world > 1:
+            torch.distributed.init_process_group(args.dist_backend, timeout=datetime.timedelta(seconds=300))
+        out = run_split(args, rank, world)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        if world > 1:
+            torch.distributed.destroy_process_group()
         return 0
     if world > 1:
         import torch
