@@ -354,3 +354,13 @@ def test_flat_seam_exchange(world, dims):
     for r in range(world):
         assert out[r]["nbad"] == 0, (r, out[r]["bad"])
         assert out[r]["untouched"] and out[r]["sent"] > 0
+
+
+def test_comm_must_be_a_process_group():
+    from geoswe_b200.halo import comm_size
+    assert comm_size(None) == 1
+
+    class MpiLike:
+        size, rank = 4, 0
+    with pytest.raises(TypeError, match="ProcessGroup"):
+        comm_size(MpiLike())
