@@ -11,7 +11,7 @@ from pathlib import Path
 _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / "libgsw.so"
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_ABI, ERR_NONFINITE, ERR_RANGE, ERR_TIMEOUT = -1, -2, -3, -4, -5, -6
@@ -53,7 +53,8 @@ class GswDenseArgs(C.Structure):
                 ("friction_kind", i32), ("n_cls", vp), ("n_cls_pitch", i64), ("n_tab", vp),
                 ("n_tab_len", i32), ("n_field", vp), ("vcap", f64), ("quadratic", i32),
                 ("keep_h", i32), ("max_h", vp), ("cfl_skip", vp), ("h_cfl", f64),
-                ("tile_rows", i32), ("warps", i32), ("min_blocks", i32), ("arith", i32)]
+                ("tile_rows", i32), ("warps", i32), ("min_blocks", i32), ("arith", i32),
+                ("row_lo", i32), ("row_hi", i32), ("col_lo", i32), ("col_hi", i32)]
 
 
 class GswBcArgs(C.Structure):

@@ -24,7 +24,8 @@ struct DenseK {
     T* o0; T* o1; T* o2;
     const T* b;
     const uint8_t* mask; int64_t mpitch;
-    int nxp, nyp, lo;            // cells [lo, n-lo) are computed (lo = ngh, or 2 for the residual)
+    int nxp, nyp, lo;            // cells [lo, n-lo) may be computed (lo = ngh, or 2 for the residual)
+    int row_lo, row_hi, col_lo, col_hi;   // the window computed, inside [lo, n-lo)
     int ngh;
     int64_t pitch;
     T inv_dx, inv_dy, half_dx, half_dy, g, h_min;
@@ -99,14 +100,14 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
     if (STEP && p.st->done) return;                       // grid-uniform
     const int lane = threadIdx.x;
     const int strip = blockIdx.x * blockDim.y + threadIdx.y;
-    const int jend = p.nyp - p.lo;
-    const int col0 = p.lo + strip * 30;
+    const int jend = p.col_hi;
+    const int col0 = p.col_lo + strip * 30;
     const bool warp_active = col0 < jend;
     const int c = col0 - 1 + lane;
     const int cl = min(c, p.nyp - 1);
     const bool out_lane = warp_active && lane >= 1 && lane <= 30 && c < jend;
-    const int i0 = p.lo + blockIdx.y * p.tile_rows;
-    const int i1 = min(i0 + p.tile_rows, p.nxp - p.lo);
+    const int i0 = p.row_lo + blockIdx.y * p.tile_rows;
+    const int i1 = min(i0 + p.tile_rows, p.row_hi);
     unsigned long long lam_local = 0ull;
 
     T dt = (T)0;
@@ -226,6 +227,16 @@ inline int fill_dense(const GswDenseArgs* a, DenseK<T>& k, bool step) {
     k.mask = a->inside_mask; k.mpitch = a->mask_pitch;
     k.nxp = a->nxp; k.nyp = a->nyp; k.ngh = a->ngh; k.pitch = a->pitch;
     k.lo = step ? a->ngh : 2;
+    // the window: 0 at both ends of an axis is the whole range
+    k.row_lo = (a->row_lo == 0 && a->row_hi == 0) ? k.lo : a->row_lo;
+    k.row_hi = (a->row_lo == 0 && a->row_hi == 0) ? a->nxp - k.lo : a->row_hi;
+    k.col_lo = (a->col_lo == 0 && a->col_hi == 0) ? k.lo : a->col_lo;
+    k.col_hi = (a->col_lo == 0 && a->col_hi == 0) ? a->nyp - k.lo : a->col_hi;
+    if (k.row_lo < k.lo || k.row_hi > a->nxp - k.lo || k.row_lo >= k.row_hi ||
+        k.col_lo < k.lo || k.col_hi > a->nyp - k.lo || k.col_lo >= k.col_hi)
+        return set_error(GSW_ERR_INVALID, "dense: window rows [%d, %d) x columns [%d, %d) is empty or leaves "
+                         "[%d, %d) x [%d, %d)", a->row_lo, a->row_hi, a->col_lo, a->col_hi, k.lo,
+                         a->nxp - k.lo, k.lo, a->nyp - k.lo);
     k.inv_dx = (T)a->inv_dx; k.inv_dy = (T)a->inv_dy;
     {   // dx = 1/inv_dx evaluated in T, as the reference kernel does (rhs_cuda.py:925-926)
         const T dx = (T)1 / k.inv_dx, dy = (T)1 / k.inv_dy;
@@ -242,7 +253,7 @@ inline int fill_dense(const GswDenseArgs* a, DenseK<T>& k, bool step) {
     if (a->tile_rows > 0) {
         k.tile_rows = a->tile_rows;
     } else {   // rows per warp: the longest march (<= 32 rows) that still gives twice the resident warps
-        const int64_t strips = (a->nyp - 2 * k.lo + 29) / 30, nrows = a->nxp - 2 * k.lo;
+        const int64_t strips = (k.col_hi - k.col_lo + 29) / 30, nrows = k.row_hi - k.row_lo;
         const int64_t want = 2LL * sm_count() * 24;
         k.tile_rows = 4;
         for (int tr = 32; tr > 4; tr >>= 1)
@@ -272,7 +283,7 @@ inline int launch_march(const GswDenseArgs* a, cudaStream_t s) {
     const int minb = a->min_blocks;
     if (minb != 0 && (minb < 3 || minb > 5)) return set_error(GSW_ERR_INVALID, "dense: min_blocks must be 0, 3, 4 or 5");
     if (W < 1 || W > 8) return set_error(GSW_ERR_INVALID, "dense: warps must be in [1, 8]");
-    const int ncols = k.nyp - 2 * k.lo, nrows = k.nxp - 2 * k.lo;
+    const int ncols = k.col_hi - k.col_lo, nrows = k.row_hi - k.row_lo;
     const int strips = (ncols + 29) / 30;
     dim3 block(32, W);
     dim3 grid((strips + W - 1) / W, (nrows + k.tile_rows - 1) / k.tile_rows);

@@ -544,13 +544,28 @@ class Solver2D:
         src, dst = self._buf[k_parity], self._buf[1 - k_parity]
         s = _stream()
         L.call("gsw_bc_fill", C.byref(self._bc_args(src)), s)
-        if self.halo is not None:
-            self.halo.exchange(src)
         for inl in T.inflows:
             self._launch_inflow(inl, src, s)
         n = 2 + len(T.inflows) + 2 * len(T.stages) + (1 if len(T.stages) > 1 else 0)
+        windows = self._overlap_windows() if self.halo is not None else None
+        if windows is None:
+            if self.halo is not None:
+                self.halo.exchange(src)
+            L.call("gsw_dense_step", C.byref(self._dense_args(src, dst, T)), s)
+        else:
+            # the cells whose stencil reads no seam ghost step while the halo is in
+            # flight; the bands next to the seams step once it has landed
+            inner, bands = windows
+            handle = self.halo.start_exchange(src)
+            a = self._dense_args(src, dst, T)
+            a.row_lo, a.row_hi, a.col_lo, a.col_hi = inner
+            L.call("gsw_dense_step", C.byref(a), s)
+            self.halo.wait_exchange(handle)
+            for w in bands:
+                a.row_lo, a.row_hi, a.col_lo, a.col_hi = w
+                L.call("gsw_dense_step", C.byref(a), s)
+            n += len(bands)
         self._counting += n
-        L.call("gsw_dense_step", C.byref(self._dense_args(src, dst, T)), s)
         multi = len(T.stages) > 1
         for st in T.stages:
             a = L.GswStageArgs()
@@ -581,6 +596,33 @@ class Solver2D:
         self.diagnostics["rhs_calls"] += 1
 
     _counting = 0
+
+    def _overlap_windows(self):
+        """(interior window, band windows) of a split run's step, as (row_lo, row_hi,
+        col_lo, col_hi) of the padded grid: the interior leaves two rows (columns) next to
+        every face that borders another rank -- the reach of the stencil -- and the bands
+        are those rows (x seams, all columns) and columns (y seams, the interior rows).
+        None when the block is too thin to leave an interior."""
+        if getattr(self, "_windows_key", None) != (self.nxp, self.nyp):
+            g, nxp, nyp, h = self.mesh.ngh, self.nxp, self.nyp, self.halo
+            r0 = g + 2 if h.has_neighbor("x-") else g
+            r1 = nxp - g - 2 if h.has_neighbor("x+") else nxp - g
+            c0 = g + 2 if h.has_neighbor("y-") else g
+            c1 = nyp - g - 2 if h.has_neighbor("y+") else nyp - g
+            win = None
+            if r1 > r0 and c1 > c0:
+                bands = []
+                if r0 > g:
+                    bands.append((g, r0, g, nyp - g))
+                if r1 < nxp - g:
+                    bands.append((r1, nxp - g, g, nyp - g))
+                if c0 > g:
+                    bands.append((r0, r1, g, c0))
+                if c1 < nyp - g:
+                    bands.append((r0, r1, c1, nyp - g))
+                win = ((r0, r1, c0, c1), bands)
+            self._windows, self._windows_key = win, (self.nxp, self.nyp)
+        return self._windows
 
     def _dt_params(self, t_end, dt_max=None, max_steps=0, fixed_dt=None):
         T = self._tables()

@@ -39,7 +39,7 @@ extern "C" {
 #define GSW_API
 #endif
 
-#define GSW_ABI_VERSION 1u
+#define GSW_ABI_VERSION 2u
 
 /* return codes */
 #define GSW_OK               0
@@ -170,6 +170,13 @@ typedef struct GswDenseArgs {
     int32_t  warps;            /* warps per block (0: default 4) */
     int32_t  min_blocks;       /* register cap: 0 (compiler's choice), 3 (80 regs), 4 (64 regs) or 5 (48 regs) */
     int32_t  arith;            /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST (GSW_F32 step only) */
+    /* Window of the cells computed: rows [row_lo, row_hi) x columns [col_lo, col_hi) of
+     * the padded grid, inside the usual range (rows and columns [ngh, n - ngh) for the
+     * step, [2, n - 2) for the residual). 0 in both ends of an axis: that whole range.
+     * A run split over ranks steps the cells whose stencil reads no seam ghost while the
+     * halo is in flight, then the bands next to the seams (the reference's interior /
+     * band overlap, geoswe/solver.py:1750-1790). No cell's value depends on the window. */
+    int32_t  row_lo, row_hi, col_lo, col_hi;
 } GswDenseArgs;
 
 /* One fused step over the interior: SRM-HLLC residual, rain, forward Euler,

@@ -106,3 +106,14 @@ def test_seam_copy_checks():
     a.stride = 0
     rc, msg = _call("gsw_seam_copy", C.byref(a), None)
     assert rc == L.ERR_INVALID and "stride" in msg
+
+
+def test_dense_window_is_checked():
+    """A window reaching outside the computed range (or empty) is refused before any
+    launch."""
+    fake = C.c_void_p(256)
+    for w in [(1, 5, 0, 0), (2, 19, 0, 0), (6, 6, 0, 0), (0, 0, 3, 2)]:
+        a = _dense(nxp=20, nyp=20, ngh=2, pitch=32, q0=fake, q1=fake, q2=fake, qn0=fake, qn1=fake, qn2=fake,
+                   bed=fake, row_lo=w[0], row_hi=w[1], col_lo=w[2], col_hi=w[3])
+        rc, msg = _call("gsw_dense_step", C.byref(a), None)
+        assert rc == L.ERR_INVALID and "window" in msg, (w, rc, msg)

@@ -228,6 +228,40 @@ def test_host_loop_equals_device_loop(dtype):
     assert same(out[0][2], out[1][2])
 
 
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_windows_tile_the_step(dtype):
+    """The step launched as an interior window plus four bands (what a split run does
+    around its halo exchange) writes the same state and wave speed as one launch."""
+    import ctypes as C
+    from geoswe_b200 import _lib as L
+    from geoswe_b200.solver import _ptr, _stream
+    q0, bed = flowing(58, 45, seed=8, dtype=np.dtype(dtype))
+    s = _solver(q0, bed, dtype, friction="manning", manning_n=0.03, rainfall=70.0 / 3.6e6)
+    s.run(t_end=1e9, max_steps=9)
+    T = s._tables()
+    s._write_state()
+    p = s._dt_params(t_end=float("inf"), fixed_dt=0.05)
+    L.call("gsw_dt_finalize", C.byref(p), _ptr(s._state), _stream())
+    src = s._buf[s._cur]
+    L.call("gsw_bc_fill", C.byref(s._bc_args(src)), _stream())
+    g, nxp, nyp = 2, s.nxp, s.nyp
+    outs, lams = [], []
+    for windows in ([(0, 0, 0, 0)],
+                    [(g + 2, nxp - g - 2, g + 2, nyp - g - 2), (g, g + 2, g, nyp - g), (nxp - g - 2, nxp - g, g, nyp - g),
+                     (g + 2, nxp - g - 2, g, g + 2), (g + 2, nxp - g - 2, nyp - g - 2, nyp - g)]):
+        out = torch.zeros_like(src)
+        s._lam_view.zero_()
+        a = s._dense_args(src, out, T)
+        a.max_h = None
+        for w in windows:
+            a.row_lo, a.row_hi, a.col_lo, a.col_hi = w
+            L.call("gsw_dense_step", C.byref(a), _stream())
+        outs.append(out[:, g:nxp - g, g:nyp - g].cpu().numpy())
+        lams.append(int(s._lam_view.item()))
+    assert same(outs[0], outs[1]) and lams[0] == lams[1] != 0
+    assert np.abs(outs[0][0]).max() > 0.1
+
+
 def test_segmented_runs_reuse_one_graph():
     """run() called interval by interval (new t_end each call, odd step counts, so the
     calls start on either buffer) equals one run to the last t_end bit for bit, and
