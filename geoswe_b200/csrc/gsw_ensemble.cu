@@ -19,8 +19,10 @@ __global__ void ensemble_finalize_kernel(GswEnsembleArgs a) {
     __syncthreads();
     if (a.run != nullptr) build_run_list(a, threadIdx.x, blockDim.x);
     if (threadIdx.x == 0) {
-        a.scratch[0] = 0u;
-        a.scratch[1] = 0u;
+        if (a.scratch != nullptr) {   // NULL: the static-scratch step keeps its own words at zero
+            a.scratch[0] = 0u;
+            a.scratch[1] = 0u;
+        }
         *a.all_done = (s_open == 0) ? 1 : 0;
     }
 }
@@ -43,12 +45,15 @@ __global__ void __launch_bounds__(256) ensemble_lammax_kernel(GswEnsembleArgs a)
 
 using namespace gsw;
 
-static int check_ens(const GswEnsembleArgs* a) {
+// need_scratch: the caller-scratch step needs a->scratch; the wave speed and the dt rule
+// read none (finalize clears it when given), and the static-scratch step brings its own.
+static int check_ens(const GswEnsembleArgs* a, bool need_scratch) {
     if (a->n_members <= 0 || a->n_members > 65536 || a->brick_h < 2 || a->n_bricks < 0)
         return set_error(GSW_ERR_INVALID, "ensemble: bad sizes");
     if (!a->brick_ij || !a->brick_nbr || !a->brick_member || !a->flags || !a->q0 || !a->q1 || !a->q2 ||
-        !a->bed || !a->members || !a->states || !a->scratch || !a->all_done)
+        !a->bed || !a->members || !a->states || !a->all_done)
         return set_error(GSW_ERR_INVALID, "ensemble: null pointer");
+    if (need_scratch && !a->scratch) return set_error(GSW_ERR_INVALID, "ensemble step: scratch is NULL");
     if (a->run != nullptr && a->member_brick_off == nullptr)
         return set_error(GSW_ERR_INVALID, "ensemble: a running-member list needs member_brick_off");
     return GSW_OK;
@@ -56,7 +61,7 @@ static int check_ens(const GswEnsembleArgs* a) {
 
 extern "C" int gsw_ensemble_lammax(const GswEnsembleArgs* a, void* stream) {
     GSW_CHECK_ABI(a);
-    int rc = check_ens(a);
+    int rc = check_ens(a, false);
     if (rc) return rc;
     const int64_t nslots = a->n_bricks * (int64_t)a->brick_h * GSW_BRICK_PITCH;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(sm_count() * 8, (nslots + 255) / 256));
@@ -66,7 +71,7 @@ extern "C" int gsw_ensemble_lammax(const GswEnsembleArgs* a, void* stream) {
 
 extern "C" int gsw_ensemble_finalize(const GswEnsembleArgs* a, void* stream) {
     GSW_CHECK_ABI(a);
-    int rc = check_ens(a);
+    int rc = check_ens(a, false);
     if (rc) return rc;
     ensemble_finalize_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(*a);
     return check_launch("ensemble_finalize");
@@ -74,11 +79,12 @@ extern "C" int gsw_ensemble_finalize(const GswEnsembleArgs* a, void* stream) {
 
 extern "C" int gsw_ensemble_step(const GswEnsembleArgs* a, void* stream) {
     GSW_CHECK_ABI(a);
-    int rc = check_ens(a);
+    int rc = check_ens(a, true);
     if (rc) return rc;
     if (!a->qn0 || !a->qn1 || !a->qn2) return set_error(GSW_ERR_INVALID, "ensemble step: null output");
     if (a->arith == GSW_ARITH_FAST) return gsw_fast_ensemble_launch(a, (cudaStream_t)stream);
-    if (a->arith != GSW_ARITH_EXACT) return set_error(GSW_ERR_INVALID, "ensemble step: bad arith %d", a->arith);
+    if (a->arith != GSW_ARITH_EXACT && a->arith != GSW_ARITH_PORTABLE)
+        return set_error(GSW_ERR_INVALID, "ensemble step: bad arith %d", a->arith);
     return launch_ensemble_step(a, (cudaStream_t)stream);
 }
 
@@ -119,5 +125,8 @@ extern "C" int gsw_ensemble_step_static(const GswEnsembleArgs* a, void* stream) 
     }
     GswEnsembleArgs b = *a;
     b.scratch = ptr;
-    return gsw_ensemble_step(&b, stream);
+    const int rc = gsw_ensemble_step(&b, stream);
+    // a refused or failed launch must not leave a ticket behind for the next call
+    if (rc != GSW_OK) (void)cudaMemsetAsync(ptr, 0, GSW_ENS_SCRATCH_WORDS * sizeof(unsigned int), (cudaStream_t)stream);
+    return rc;
 }

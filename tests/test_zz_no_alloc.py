@@ -1,9 +1,10 @@
 """gsw_ensemble_step_static (the ensemble step with its ticket counter in the library's
 static device array) against gsw_ensemble_step with caller scratch: two calls in a row
 from the same state give the same states and fields bit for bit, and the caller's
-scratch argument is neither needed nor touched. Collected last on purpose: the static
-variant's first call on a device does its one-time setup here, after whatever the
-other test files ran."""
+scratch argument is neither needed nor touched; and a whole loop (wave speed, dt rule,
+static step) runs with no caller scratch at all, as a host without a device allocator
+runs it. Collected last on purpose: the static variant's first call on a device does
+its one-time setup here, after whatever the other test files ran."""
 import ctypes as C
 
 import numpy as np
@@ -67,3 +68,43 @@ def test_static_scratch_step_matches_caller_scratch_step():
     _two_steps("gsw_ensemble_step", ref)
     _two_steps("gsw_ensemble_step_static", stat)
     assert bytes(ref.read_states()) == bytes(stat.read_states())
+
+
+def _loop_without_scratch(ens, n_steps):
+    """The ensemble loop a host with no allocator runs: the initial wave speed, the dt
+    rule and the static-scratch step, every call with a NULL scratch pointer."""
+    from geoswe_b200 import _lib as L
+    from geoswe_b200.solver import _stream
+    ens._build_members(600.0, 10 ** 9, None)
+    ens._all_done.zero_()
+    q = ens._q
+    for entry in ("gsw_ensemble_lammax", "gsw_ensemble_finalize"):
+        a = ens._args(q[0], q[0])
+        a.scratch = None
+        L.call(entry, C.byref(a), _stream())
+    for k in range(n_steps):
+        a = ens._args(q[k % 2], q[(k + 1) % 2])
+        a.scratch = None
+        L.call("gsw_ensemble_step_static", C.byref(a), _stream())
+    torch.cuda.synchronize()
+
+
+def test_whole_loop_runs_without_caller_scratch():
+    """lammax, finalize and the static step with scratch = NULL give the same states and
+    fields as the caller-scratch loop, over several steps (the static words start and end
+    each step at zero)."""
+    from geoswe_b200 import _lib as L
+    from geoswe_b200.solver import _stream
+    ref, stat = _ensemble(), _ensemble()
+    p0 = ref._prepare(600.0, 10 ** 9, None)
+    assert p0 == 0
+    n = 5
+    for k in range(n):
+        L.call("gsw_ensemble_step", C.byref(ref._args(ref._q[k % 2], ref._q[(k + 1) % 2])), _stream())
+    torch.cuda.synchronize()
+    _loop_without_scratch(stat, n)
+    assert bytes(ref.read_states()) == bytes(stat.read_states())
+    for c in range(3):
+        assert same(ref._q[n % 2][c].cpu().numpy(), stat._q[n % 2][c].cpu().numpy())
+    sts = stat.read_states()
+    assert all(int(sts[k].steps) == n for k in range(2))
