@@ -11,7 +11,7 @@ from pathlib import Path
 _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / "libgsw.so"
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_ABI, ERR_NONFINITE, ERR_RANGE, ERR_TIMEOUT = -1, -2, -3, -4, -5, -6
@@ -21,7 +21,8 @@ BC_EXTRAPOLATE, BC_WALL, BC_FALL, BC_PERIODIC, BC_NONE = 0, 1, 2, 3, 4
 BC_CODES = {"extrapolate": BC_EXTRAPOLATE, "wall": BC_WALL, "fall": BC_FALL,
             "periodic": BC_PERIODIC, "none": BC_NONE}
 RAIN_NONE, RAIN_UNIFORM, RAIN_GRIDDED, RAIN_LOOKUP = 0, 1, 2, 3
-ARITH_EXACT, ARITH_FAST = 0, 1
+ARITH_EXACT, ARITH_FAST, ARITH_PORTABLE = 0, 1, 2
+ARITH_CODES = {"exact": ARITH_EXACT, "fast": ARITH_FAST, "portable": ARITH_PORTABLE}
 FRICTION_NONE, FRICTION_TABLE, FRICTION_FIELD = 0, 1, 2
 NORM_LINF, NORM_L2 = 0, 1
 BRICK_W, BRICK_PITCH = 30, 32

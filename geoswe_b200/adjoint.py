@@ -167,9 +167,9 @@ class FlatAdjoint:
             raise ValueError("window must be in [1, n_steps]")
         if dtype not in ("float32", "float64"):
             raise ValueError("dtype must be float32 or float64")
-        if cs.arith != L.ARITH_EXACT:
+        if cs.arith == L.ARITH_FAST:
             raise ValueError("FlatAdjoint: the adjoint differentiates the exact step; build the solver "
-                             "with arith='exact'")
+                             "with arith='exact' (or 'portable')")
         self.cs = cs
         self.dev = cs.device
         self.adj_min_blocks = 8          # register cap of the binary32 reverse kernels: 0, 6 (80) or 8 (64 regs)

@@ -31,7 +31,7 @@ def _cache_path() -> Path:
 
 def kind(base, arith=0):
     """Cache kind of a kernel family: the fast-arithmetic kernels tune separately."""
-    return base if int(arith) == L.ARITH_EXACT else base + "-fast"
+    return base + "-fast" if int(arith) == L.ARITH_FAST else base
 
 
 def _key(kind, cells):

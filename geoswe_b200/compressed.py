@@ -298,9 +298,9 @@ class CompressedSolver:
     # ------------------------------------------------------------- construction
     def _init_physics(self, *, device, nxp, nyp, ngh, nx, ny, dx, g, cfl, h_min, cfl_linf, vcap, quad, keep_h,
                       dt_max, brick_h, arith="exact"):
-        if arith not in ("exact", "fast"):
-            raise ValueError(f"CompressedSolver: arith={arith!r} invalid; expected 'exact' or 'fast'")
-        self.arith = L.ARITH_FAST if arith == "fast" else L.ARITH_EXACT
+        if arith not in L.ARITH_CODES:
+            raise ValueError(f"CompressedSolver: arith={arith!r} invalid; expected one of {sorted(L.ARITH_CODES)}")
+        self.arith = L.ARITH_CODES[arith]
         self.brick_h = int(brick_h or type(self).brick_h)
         self.device = torch.device(device)
         self.nxp, self.nyp, self.ngh = int(nxp), int(nyp), int(ngh)

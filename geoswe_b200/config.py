@@ -66,9 +66,13 @@ class Config:
     ``{"x-": kind, "x+": kind, "y-": kind, "y+": kind}`` that overrides ``bc_x``/``bc_y``
     face by face (for example one open outflow edge on an otherwise walled domain).
     ``arith`` selects the step's arithmetic: ``"exact"`` (default; separately rounded
-    IEEE operations, bit-identical to the reference kernel compiled without FMA
-    contraction) or ``"fast"`` (binary32 only: FMA contraction, approximate square root
-    and division; held to a depth tolerance against ``"exact"``, not to bit equality).
+    IEEE operations and Manning's h^(-4/3) by CUDA's powf, as the reference kernel text:
+    bit-identical to the reference kernel compiled without FMA contraction, friction
+    included), ``"portable"`` (``"exact"`` with h^(-4/3) by a Newton iteration of IEEE
+    operations, so a CPU reproduces every bit of a friction run; identical to
+    ``"exact"`` without friction) or ``"fast"`` (binary32 only: FMA contraction,
+    approximate square root and division; held to a depth tolerance against
+    ``"exact"``, not to bit equality).
     """
     pde: str = "baseline"
     flux: str = "hllc"
@@ -118,7 +122,7 @@ class Config:
                    "recon": {"first", "muscl", "linear2", "linear3", "linear5", "weno5"},
                    "wb_method": {"audusse", "srm"}, "pde": {"igr", "baseline"},
                    "dtype": {"float32", "float64"}, "bc_x": _BC_OK, "bc_y": _BC_OK,
-                   "friction": {"manning_implicit"}, "arith": {"exact", "fast"}}
+                   "friction": {"manning_implicit"}, "arith": {"exact", "fast", "portable"}}
         for k, ok in enum_ok.items():
             v = getattr(self, k, None)
             if v is None and k == "friction":

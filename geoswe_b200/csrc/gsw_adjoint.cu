@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(128, MINB) adj_tail_kernel(AdjK<T> p) {
                     Bar3<T> in_b;
                     T n_b;
                     wetdry_friction_bwd<T>(h1, hu1, hv1, n, dt, ph.g, ph.h_min, ph.vcap, ph.quad != 0,
-                                           ph.keep_h != 0, out_b, in_b, n_b);
+                                           ph.keep_h != 0, ph.ref_pow != 0, out_b, in_b, n_b);
                     p.lo0[o] = in_b.h; p.lo1[o] = in_b.hu; p.lo2[o] = in_b.hv;
                     p.rb0[o] = dt * in_b.h; p.rb1[o] = dt * in_b.hu; p.rb2[o] = dt * in_b.hv;
                     if (ph.rain_kind == GSW_RAIN_UNIFORM) rate_acc += (double)(dt * in_b.h);
@@ -357,7 +357,8 @@ static int fill_adj(const GswFlatAdjArgs* a, AdjK<T>& k) {
     if (f.n_tab_len > 256) return set_error(GSW_ERR_RANGE, "adjoint: at most 256 Manning classes");
     if (f.rain_kind != GSW_RAIN_NONE && !f.rain) return set_error(GSW_ERR_INVALID, "adjoint: rain is NULL");
     if (f.rain_kind == GSW_RAIN_LOOKUP) return set_error(GSW_ERR_INVALID, "adjoint: lookup rain is not differentiated");
-    if (f.arith != GSW_ARITH_EXACT) return set_error(GSW_ERR_INVALID, "adjoint: the exact step is differentiated (arith)");
+    if (f.arith != GSW_ARITH_EXACT && f.arith != GSW_ARITH_PORTABLE)
+        return set_error(GSW_ERR_INVALID, "adjoint: the exact or portable step is differentiated (arith)");
     if (!a->lam_in0 || !a->lam_in1 || !a->lam_in2 || !a->lam_out0 || !a->lam_out1 || !a->lam_out2 ||
         !a->rbar0 || !a->rbar1 || !a->rbar2 || !a->n_bar)
         return set_error(GSW_ERR_INVALID, "adjoint: null adjoint buffer");
@@ -375,6 +376,7 @@ static int fill_adj(const GswFlatAdjArgs* a, AdjK<T>& k) {
     ph.ntab = (const T*)f.n_tab;
     ph.lookup = f.rain_lookup; ph.ncol = f.rain_ncol;
     ph.g_recip = (T)0;          // the recomputed faces divide (the same bits as the forward's)
+    ph.ref_pow = f.arith == GSW_ARITH_EXACT ? 1 : 0;
     k.st = f.state;
     k.li0 = (const T*)a->lam_in0; k.li1 = (const T*)a->lam_in1; k.li2 = (const T*)a->lam_in2;
     k.lo0 = (T*)a->lam_out0; k.lo1 = (T*)a->lam_out1; k.lo2 = (T*)a->lam_out2;

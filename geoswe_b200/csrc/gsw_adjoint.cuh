@@ -8,7 +8,8 @@
 //   fminf(a, b)   -> a when a <= b;   fmaxf(a, b) -> a when a >= b
 //   sqrt(g x)     -> derivative 0 where x <= 0
 //   u = hu / h    -> only where h > h_min (else u = 0, a constant)
-// h^(-4/3) (pow_m43) is differentiated as the exact power, -4/3 h^(-7/3).
+// h^(-4/3) (powf or pow_m43, as the forward step) is differentiated as the exact power,
+// -4/3 h^(-7/3).
 #pragma once
 #include "gsw_core.cuh"
 
@@ -222,7 +223,7 @@ __device__ __forceinline__ FaceBar<T> face_bar(const Bar3<T>& rL, const Bar3<T>&
 // adjoints of (h1, hu1, hv1) and of the cell's Manning n.
 template <typename T>
 __device__ __forceinline__ void wetdry_friction_bwd(T h1, T hu1, T hv1, T n, T dt, T g, T h_min, T vcap,
-                                                    bool quadratic, bool keep_h, const Bar3<T>& out_b,
+                                                    bool quadratic, bool keep_h, bool ref_pow, const Bar3<T>& out_b,
                                                     Bar3<T>& in_b, T& n_b) {
     const T z = Real<T>::zero();
     n_b = z;
@@ -235,7 +236,7 @@ __device__ __forceinline__ void wetdry_friction_bwd(T h1, T hu1, T hv1, T n, T d
     const T hs = pass ? h1 : h_min;
     const T u = div_z(hu1, hs), v = div_z(hv1, hs);
     const T modU = sqrt_z(u * u + v * v);
-    const T h43 = pow_m43(hs);
+    const T h43 = ref_pow ? pow_m43_ref(hs) : pow_m43(hs);   // the forward step's own value
     T ne = n, K = z, ncri = z;
     bool capped = false;
     if (modU > vcap) {

@@ -160,6 +160,13 @@ __device__ __forceinline__ double pow_m43(double x) {
     return r / x;
 }
 
+// Manning's h^(-4/3) as the reference kernel text evaluates it: powf(hs, -4.0f/3.0f)
+// (rhs_cuda.py:1830, compressed_rhs.py:730), CUDA's own powf, called, not restated; the
+// library is compiled without contraction, as the reference's strict build. The
+// reference's friction is binary32 only; binary64 keeps the iteration above.
+__device__ __forceinline__ float pow_m43_ref(float x) { return powf(x, -4.0f / 3.0f); }
+__device__ __forceinline__ double pow_m43_ref(double x) { return pow_m43(x); }
+
 // HLLC flux in the face frame (rhs_cuda.py:986-1036) with Sigma = 0 (the no-sigma
 // build, rhs_cuda.py:1717-1722): uN normal, uT transverse velocity.
 template <typename T>
@@ -289,10 +296,12 @@ __device__ __forceinline__ void accumulate(const Face<T>& E, const Face<T>& W,
 // Wet/dry floor and point-implicit Manning friction on an updated cell
 // (rhs_cuda.py:1765-1790; solver.py:233-307). friction == false applies the wet/dry
 // floor alone, as the reference does when Config.friction is None (solver.py:2952-2962).
+// ref_pow: h^(-4/3) by pow_m43_ref (GSW_ARITH_EXACT), else by pow_m43 (GSW_ARITH_PORTABLE
+// and the fast arithmetic).
 template <typename T>
 __device__ __forceinline__ void wetdry_friction(T& h, T& hu, T& hv, bool friction, T n,
                                                 T dt, T g, T h_min, T vcap,
-                                                bool quadratic, bool keep_h) {
+                                                bool quadratic, bool keep_h, bool ref_pow) {
     const T z = Real<T>::zero();
     if (h < h_min) {
         h = keep_h ? (h > z ? h : z) : z;
@@ -304,7 +313,7 @@ __device__ __forceinline__ void wetdry_friction(T& h, T& hu, T& hv, bool frictio
     const T u = div_z(hu, hs);
     const T v = div_z(hv, hs);
     const T modU = sqrt_z(u * u + v * v);
-    const T h43 = pow_m43(hs);
+    const T h43 = ref_pow ? pow_m43_ref(hs) : pow_m43(hs);
     if (modU > vcap) {
         const T n_cri = gsqrt(gdiv((T)1.0, ((T)1.0e-10 + dt) * g * h43 * (modU + (T)1.0e-30)));
         if (n_cri > n) n = n_cri;

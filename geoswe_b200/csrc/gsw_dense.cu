@@ -158,9 +158,9 @@ __global__ void lam_cells_kernel(const T* q0, const T* q1, const T* q2, const in
 
 using namespace gsw;
 
-// Exact or fast arithmetic; fast is binary32 only.
+// Exact, portable or fast arithmetic; fast is binary32 only.
 static int check_arith(const GswDenseArgs* a) {
-    if (a->arith != GSW_ARITH_EXACT && a->arith != GSW_ARITH_FAST)
+    if (a->arith != GSW_ARITH_EXACT && a->arith != GSW_ARITH_FAST && a->arith != GSW_ARITH_PORTABLE)
         return set_error(GSW_ERR_INVALID, "dense: bad arith %d", a->arith);
     if (a->arith == GSW_ARITH_FAST && a->dtype != GSW_F32)
         return set_error(GSW_ERR_INVALID, "dense: fast arithmetic is binary32 only");

@@ -39,6 +39,7 @@ struct DenseK {
     T h_cfl;
     int tile_rows;
     T g_recip;                   // RN(1/g) for the star depth's h / g, or 0 (gsw_core.cuh div_g)
+    int ref_pow;                 // 1: Manning's h^(-4/3) by powf (GSW_ARITH_EXACT), 0: by pow_m43
 };
 
 template <typename T>
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
                         n = p.ncls ? p.ntab[p.ncls[(int64_t)r * p.cpitch + c]] : p.ntab[0];
                     else if (p.friction_kind == GSW_FRICTION_FIELD) n = p.nfield[o];
                     wetdry_friction<T>(h, hu, hv, p.friction_kind != GSW_FRICTION_NONE, n, dt, p.g,
-                                       p.h_min, p.vcap, p.quad != 0, p.keep_h != 0);
+                                       p.h_min, p.vcap, p.quad != 0, p.keep_h != 0, p.ref_pow != 0);
                     p.o0[o] = h; p.o1[o] = hu; p.o2[o] = hv;
                     if (p.max_h != nullptr && h > p.max_h[o]) p.max_h[o] = h;
                     if (p.lam != nullptr) {
@@ -244,6 +245,7 @@ inline int fill_dense(const GswDenseArgs* a, DenseK<T>& k, bool step) {
     }
     k.g = (T)a->g; k.h_min = (T)a->h_min;
     k.g_recip = sizeof(T) == 4 ? (T)div_const_recip((float)a->g) : (T)0;
+    k.ref_pow = a->arith == GSW_ARITH_EXACT ? 1 : 0;
     k.st = a->state; k.lam = (unsigned long long*)a->lam_target;
     k.rain_kind = a->rain_kind; k.rain = (const T*)a->rain;
     k.friction_kind = a->friction_kind; k.ncls = a->n_cls; k.cpitch = a->n_cls_pitch;

@@ -19,7 +19,7 @@
 
 namespace gsw {
 
-__device__ __forceinline__ FlatPhys<float> member_phys(const GswMember& mb) {
+__device__ __forceinline__ FlatPhys<float> member_phys(const GswMember& mb, int ref_pow) {
     FlatPhys<float> ph;
     ph.inv_dx = mb.inv_dx; ph.inv_dy = mb.inv_dx;
     ph.half_dx = 0.5f * (1.0f / mb.inv_dx); ph.half_dy = ph.half_dx;
@@ -28,6 +28,7 @@ __device__ __forceinline__ FlatPhys<float> member_phys(const GswMember& mb) {
     ph.rain_kind = mb.rain_kind; ph.rain = mb.rain; ph.ntab = mb.n_tab;
     ph.ngh = 0; ph.nx = 0; ph.ny = 0; ph.lookup = nullptr; ph.ncol = 0;
     ph.g_recip = mb.g_recip; // 0: the member divides
+    ph.ref_pow = ref_pow;
     return ph;
 }
 
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArg
         const GswLoopState* st = a.states + mi;
         if (st->done) continue;                                   // warp-uniform
         const GswMember& mb = a.members[mi];
-        const FlatPhys<float> ph = member_phys(mb);
+        const FlatPhys<float> ph = member_phys(mb, a.arith == GSW_ARITH_EXACT ? 1 : 0);
         const float dt = st->dt_f32;
         const float rate = (mb.rain_kind == GSW_RAIN_UNIFORM) ? mb.rain[st->rain_idx] : 0.0f;
         unsigned long long lam = flat_brick<float, true>(m, ph, b, seg * m.bh / S, (seg + 1) * m.bh / S, dt, rate,

@@ -30,7 +30,7 @@ using namespace gsw;
 
 static int check_dtype(const GswFlatArgs* a) {
     if (a->dtype != GSW_F32 && a->dtype != GSW_F64) return set_error(GSW_ERR_INVALID, "flat: dtype must be F32 or F64");
-    if (a->arith != GSW_ARITH_EXACT && a->arith != GSW_ARITH_FAST)
+    if (a->arith != GSW_ARITH_EXACT && a->arith != GSW_ARITH_FAST && a->arith != GSW_ARITH_PORTABLE)
         return set_error(GSW_ERR_INVALID, "flat: bad arith %d", a->arith);
     if (a->arith == GSW_ARITH_FAST && a->dtype != GSW_F32)
         return set_error(GSW_ERR_INVALID, "flat: fast arithmetic is binary32 only");

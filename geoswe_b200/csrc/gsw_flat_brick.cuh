@@ -27,6 +27,7 @@ struct FlatPhys {
     const int32_t* lookup;   // GSW_RAIN_LOOKUP: per-slot column of the rain row
     int ncol;
     T g_recip;               // RN(1/g) for the star depth's h / g, or 0 (gsw_core.cuh div_g)
+    int ref_pow;             // 1: Manning's h^(-4/3) by powf (GSW_ARITH_EXACT), 0: by pow_m43
 };
 
 // Row segments per brick when the caller leaves the choice to the library: one warp
@@ -186,7 +187,7 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
                     T hv = cur.hv + dt * rhv;
                     const T n = m.ncls ? ph.ntab[m.ncls[o]] : ph.ntab[0];
                     wetdry_friction<T>(h, hu, hv, true, n, dt, ph.g, ph.h_min, ph.vcap,
-                                           ph.quad != 0, ph.keep_h != 0);
+                                           ph.quad != 0, ph.keep_h != 0, ph.ref_pow != 0);
                     m.o0[o] = h; m.o1[o] = hu; m.o2[o] = hv;
                     if (m.max_h != nullptr && h > m.max_h[o]) m.max_h[o] = h;
                     const unsigned long long lb = lam_flat_bits(h, hu, hv, ph.g, ph.h_min, ph.h_min_cfl,

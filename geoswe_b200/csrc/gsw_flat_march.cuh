@@ -54,6 +54,7 @@ inline int fill_flat(const GswFlatArgs* a, FlatK<T>& k, bool step) {
     ph.ntab = (const T*)a->n_tab;
     ph.lookup = a->rain_lookup; ph.ncol = a->rain_ncol;
     ph.g_recip = sizeof(T) == 4 ? (T)div_const_recip((float)a->g) : (T)0;
+    ph.ref_pow = a->arith == GSW_ARITH_EXACT ? 1 : 0;
     k.st = a->state; k.lam = (unsigned long long*)a->lam_target;
     k.segs = a->segments > 0 ? a->segments : auto_segments(a->n_bricks, (int64_t)sm_count() * 24, a->brick_h);
     if (k.segs != 1 && k.segs != 2 && k.segs != 4) return set_error(GSW_ERR_INVALID, "flat: segments must be 0, 1, 2 or 4");

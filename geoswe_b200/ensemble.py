@@ -42,7 +42,7 @@ class Ensemble:
             raise ValueError(f"Ensemble: members must share brick_h (got {sorted(bh)})")
         ar = {m.arith for m in members}
         if len(ar) != 1:
-            raise ValueError("Ensemble: members must share their arithmetic (all 'exact' or all 'fast')")
+            raise ValueError("Ensemble: members must share their arithmetic ('exact', 'portable' or 'fast')")
         self.arith = ar.pop()
         _protos()
         self.members = list(members)

@@ -49,11 +49,12 @@ class _Tables:
 
 
 def _to_device(x, device, dtype):
-    """A host array or tensor on `device` in `dtype`: one copy of the data as given,
-    the dtype conversion on the device."""
+    """A host array or tensor on `device` in `dtype`: one copy of the data as given
+    (asynchronous from page-locked host memory), the dtype conversion on the device."""
     if not torch.is_tensor(x):
         x = torch.from_numpy(np.ascontiguousarray(x))
-    return x.to(device).to(dtype)
+    pinned = x.device.type == "cpu" and x.is_pinned()
+    return x.to(device, non_blocking=pinned).to(dtype)
 
 
 def _cached_graph(cache, key, capture, device, keep=4):
@@ -153,7 +154,7 @@ class Solver2D:
         self.code = L.F32 if self.np_dtype == np.float32 else L.F64
         self.nxp, self.nyp = mesh.padded_shape
         self.pitch = _pitch(self.nyp, self.np_dtype.itemsize)
-        self.arith = L.ARITH_FAST if cfg.arith == "fast" else L.ARITH_EXACT
+        self.arith = L.ARITH_CODES[cfg.arith]
         self._tile_rows, self._warps, self._min_blocks = int(tile_rows), int(warps), int(min_blocks)
         if autotuned and not (tile_rows or warps or min_blocks) and self.np_dtype == np.float32:
             from . import autotune
@@ -171,10 +172,10 @@ class Solver2D:
         # the finiteness check run on the device
         q_dev = _to_device(q0, dev, td)
         b_dev = _to_device(b, dev, td)
-        bad = [what for what, arr in (("the bed", b_dev), ("the initial state q0", q_dev))
-               if not bool(torch.isfinite(arr).all())]
-        if bad:
-            raise ValueError(f"Solver2D: {bad[0]} holds non-finite values (NaN or inf)")
+        fin_b, fin_q = torch.isfinite(b_dev).all(), torch.isfinite(q_dev).all()
+        if not bool(fin_b & fin_q):          # one host synchronisation for both checks
+            bad = "the bed" if not bool(fin_b) else "the initial state q0"
+            raise ValueError(f"Solver2D: {bad} holds non-finite values (NaN or inf)")
         self._buf[0][:, ngh:ngh + mesh.nx, ngh:ngh + mesh.ny] = q_dev
         self._b = torch.zeros((self.nxp, self.pitch), dtype=td, device=dev)
         self._b[ngh:ngh + mesh.nx, ngh:ngh + mesh.ny] = b_dev
@@ -238,9 +239,16 @@ class Solver2D:
         g = self.mesh.ngh
         return self.q[:, g:-g, g:-g]
 
-    def depth(self):
-        """Water depth (nx, ny) as a NumPy array, ghost cells removed."""
-        return self.q_interior[0].detach().cpu().numpy()
+    def depth(self, out=None):
+        """Water depth (nx, ny) as a NumPy array, ghost cells removed. ``out`` (an
+        extension): a float (nx, ny) host array to copy into, e.g. page-locked memory,
+        which is returned."""
+        if out is None:
+            return self.q_interior[0].detach().cpu().numpy()
+        if tuple(out.shape) != (self.mesh.nx, self.mesh.ny):
+            raise ValueError(f"depth(out=...): out must have shape ({self.mesh.nx}, {self.mesh.ny})")
+        torch.from_numpy(out).copy_(self.q_interior[0].detach())
+        return out
 
     def max_depth(self):
         """Running maximum depth after any step so far; depth() before the first step."""
@@ -275,24 +283,30 @@ class Solver2D:
         return None if self._mask is None else self._mask[:, :self.nyp]
 
     def set_manning_table(self, cls_padded, table):
-        cls_padded = np.asarray(cls_padded.detach().cpu() if torch.is_tensor(cls_padded) else cls_padded)
+        if not torch.is_tensor(cls_padded):
+            cls_padded = torch.from_numpy(np.ascontiguousarray(cls_padded))
         table = np.asarray(table.detach().cpu() if torch.is_tensor(table) else table, dtype=np.float64)
         if tuple(cls_padded.shape) != (self.nxp, self.nyp):
             raise ValueError(f"set_manning_table expects a PADDED (nxp, nyp)={(self.nxp, self.nyp)} class "
                              f"array; got {tuple(cls_padded.shape)}")
-        if cls_padded.dtype != np.uint8:
+        if cls_padded.dtype != torch.uint8:
             raise ValueError(f"set_manning_table: cls_padded must be uint8; got {cls_padded.dtype}")
         if table.ndim != 1 or table.size < 1 or table.size > 256:
             raise ValueError("set_manning_table: table must be 1-D with 1..256 entries")
-        if int(cls_padded.max()) >= int(table.size):
-            raise ValueError(f"set_manning_table: class id {int(cls_padded.max())} out of range for a "
+        # one copy to the device (asynchronous from page-locked memory); checked and
+        # pitched there
+        pinned = cls_padded.device.type == "cpu" and cls_padded.is_pinned()
+        cls_dev = cls_padded.to(self.device, non_blocking=pinned)
+        cmax = int(cls_dev.max())
+        if cmax >= int(table.size):
+            raise ValueError(f"set_manning_table: class id {cmax} out of range for a "
                              f"{int(table.size)}-entry table")
         if self.cfg.friction is None:
             warnings.warn("set_manning_table: friction is off (Config.friction is None), so this "
                           "roughness table will not be applied", stacklevel=2)
-        pad = np.zeros((self.nxp, self.pitch), dtype=np.uint8)
-        pad[:, :self.nyp] = cls_padded
-        self._ncls = torch.from_numpy(pad).to(self.device)
+        pad = torch.zeros((self.nxp, self.pitch), dtype=torch.uint8, device=self.device)
+        pad[:, :self.nyp] = cls_dev
+        self._ncls = pad
         self._ntab = torch.from_numpy(table.astype(np.float32).astype(self.np_dtype)).to(self.device)
         self._nfield = None
         self._invalidate()
@@ -778,7 +792,13 @@ class Solver2D:
         K = int(window) if window else self._window_size()
         if self.halo is not None and not window:
             K = min(K, 32)     # launched eagerly: poll often, so few no-op steps follow the end
-        if max_steps and max_steps < K and not window:
+        use_graphs = self._use_graphs
+        if max_steps and max_steps <= 2 * K and K <= 64 and not window:
+            # a short run on a large grid: capturing a graph costs more than the few launches
+            # it would save (each step is far longer than its launches), so launch eagerly
+            use_graphs = False
+            K = int(max_steps)
+        elif max_steps and max_steps < K and not window:
             K = int(max_steps)
         K += K % 2
         self._write_state()
@@ -810,7 +830,7 @@ class Solver2D:
             self._counting = 0
             one_step(1)
             lead = self._counting
-        if self._use_graphs:
+        if use_graphs:
             g, per = _cached_graph(self._graph_cache, (K, self._tile_rows, self._warps, self._min_blocks),
                                    one_window, self.device)
 

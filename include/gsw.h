@@ -39,7 +39,7 @@ extern "C" {
 #define GSW_API
 #endif
 
-#define GSW_ABI_VERSION 2u
+#define GSW_ABI_VERSION 3u
 
 /* return codes */
 #define GSW_OK               0
@@ -68,13 +68,21 @@ extern "C" {
 #define GSW_RAIN_LOOKUP   3    /* flat: rate_table[frame*ncol + lookup[cell]] */
 
 /* step arithmetic (the `arith` field of the step argument structs)
- *   EXACT: separately rounded IEEE operations in the reference kernel's operand order;
- *          bit-identical to the reference kernel text compiled without FMA contraction.
- *   FAST:  binary32 only; FMA contraction, flush-to-zero, approximate square root and
- *          division. Held to a depth tolerance against EXACT (stated by the tests and
- *          the benchmark), not to bit equality. */
-#define GSW_ARITH_EXACT 0
-#define GSW_ARITH_FAST  1
+ *   EXACT:    separately rounded IEEE operations in the reference kernel's operand order,
+ *             and Manning's h^(-4/3) by CUDA's powf(h, -4.0f/3.0f) as the reference
+ *             kernel text evaluates it (geoswe/rhs_cuda.py:1830,
+ *             geoswe/compressed_rhs.py:730); bit-identical to the reference kernel text
+ *             compiled without FMA contraction, friction included.
+ *   FAST:     binary32 only; FMA contraction, flush-to-zero, approximate square root and
+ *             division. Held to a depth tolerance against EXACT (stated by the tests and
+ *             the benchmark), not to bit equality.
+ *   PORTABLE: EXACT with h^(-4/3) by a Newton iteration of IEEE +, -, *, / only (within
+ *             1.85 ulp of the exact power), so that any IEEE host reproduces every bit of
+ *             a friction run (the CPU oracle restates it). Binary64 steps always use the
+ *             iteration (the reference's friction is binary32 only). */
+#define GSW_ARITH_EXACT    0
+#define GSW_ARITH_FAST     1
+#define GSW_ARITH_PORTABLE 2
 
 /* friction kinds */
 #define GSW_FRICTION_NONE  0
@@ -169,7 +177,7 @@ typedef struct GswDenseArgs {
                                   twice the warps the GPU runs at once */
     int32_t  warps;            /* warps per block (0: default 4) */
     int32_t  min_blocks;       /* register cap: 0 (compiler's choice), 3 (80 regs), 4 (64 regs) or 5 (48 regs) */
-    int32_t  arith;            /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST (GSW_F32 step only) */
+    int32_t  arith;            /* GSW_ARITH_EXACT (default), GSW_ARITH_PORTABLE, or GSW_ARITH_FAST (GSW_F32 step only) */
     /* Window of the cells computed: rows [row_lo, row_hi) x columns [col_lo, col_hi) of
      * the padded grid, inside the usual range (rows and columns [ngh, n - ngh) for the
      * step, [2, n - 2) for the residual). 0 in both ends of an axis: that whole range.
@@ -269,7 +277,7 @@ typedef struct GswFlatArgs {
     int32_t  brick_h;          /* rows per brick (>= 2) */
     int32_t  warps;            /* warps per block (0: 4) */
     int32_t  min_blocks;       /* fp32 step register cap: 0 (compiler's choice), 3 (80 regs), 4 (64 regs) or 5 (48 regs) */
-    int32_t  arith;            /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST (GSW_F32 step only) */
+    int32_t  arith;            /* GSW_ARITH_EXACT (default), GSW_ARITH_PORTABLE, or GSW_ARITH_FAST (GSW_F32 step only) */
     int64_t  n_bricks;         /* brick n_bricks is the all-zero brick (a missing neighbour) */
     const int32_t* brick_ij;   /* (n_bricks, 2) brick row, brick column */
     const int32_t* brick_nbr;  /* (n_bricks, 4) up, down, left, right */
@@ -478,7 +486,7 @@ typedef struct GswEnsembleArgs {
     int32_t  warps;              /* warps per block (0: 4) */
     int32_t  grid;               /* persistent blocks (0: 2 per SM) */
     int32_t  min_blocks;         /* register cap: 0 (compiler's choice), 3 (80 regs), 4 (64 regs) or 5 (48 regs) */
-    int32_t  arith;              /* GSW_ARITH_EXACT (default) or GSW_ARITH_FAST */
+    int32_t  arith;              /* GSW_ARITH_EXACT (default), GSW_ARITH_PORTABLE or GSW_ARITH_FAST */
     int32_t  segments;           /* warps per brick: 1, 2 or 4 (as GswFlatArgs.segments), or 0: chosen per
                                     launch from the running members' bricks against the grid's warps */
     const int32_t* brick_ij;     /* (n_bricks, 2) */
@@ -492,7 +500,10 @@ typedef struct GswEnsembleArgs {
     float*   max_h;              /* per slot, or NULL */
     const GswMember* members;    /* device, n_members */
     GswLoopState* states;        /* device, n_members */
-    uint32_t* scratch;           /* device, >= 4 words, zero before the first step: block and work counters */
+    uint32_t* scratch;           /* device, GSW_ENS_SCRATCH_WORDS (2) words, zero before the first step: the
+                                    block ticket and the work-item counter. Read by gsw_ensemble_step only
+                                    (gsw_ensemble_finalize zeroes it when non-NULL); may be NULL for
+                                    gsw_ensemble_lammax, gsw_ensemble_finalize and gsw_ensemble_step_static */
     int32_t* all_done;           /* device int: 1 once every member is done */
     /* Running-member brick list (optional; NULL: every launch scans all bricks and skips
        finished members brick by brick). member_brick_off: device, n_members + 1, member
@@ -524,9 +535,13 @@ GSW_API int gsw_ensemble_step(const GswEnsembleArgs* a, void* stream);
  * words per device) and ignores a->scratch; a requirement above that size is refused
  * with GSW_ERR_RANGE. It allocates nothing: on the first call on a device it looks the
  * array up (cudaGetSymbolAddress) and zeroes it on `stream`, so make that first call
- * outside any stream capture. The array is shared by all callers on a device: calls
- * whose launches overlap in time (other streams, other threads) race on the ticket
- * counter and must be serialised by the caller. */
+ * outside any stream capture. With gsw_ensemble_lammax and gsw_ensemble_finalize, which
+ * accept a->scratch == NULL, a whole ensemble loop runs on caller state and fields alone.
+ * When the step returns an error, the words are zeroed again on `stream`. The address is
+ * looked up once per device and process: a cudaDeviceReset after the first call is not
+ * supported. The array is shared by all callers on a device: calls whose launches
+ * overlap in time (other streams, other threads) race on the ticket counter and must be
+ * serialised by the caller. */
 #define GSW_ENS_SCRATCH_WORDS        2
 #define GSW_ENS_STATIC_SCRATCH_WORDS 64
 GSW_API int gsw_ensemble_step_static(const GswEnsembleArgs* a, void* stream);

@@ -3,7 +3,7 @@ in tests/golden/reference_cache/ was written by the reference's own save_cache
 (tests/golden/make_golden.py): a wet state, three Manning classes, a two-column rain
 table with a per-cell lookup and a two-gauge ring stage. CompressedSolver.from_cache
 loads it, runs it bit for bit as the oracle's restatement of the flat loop does on the
-cache's arrays, writes it back in the same format, and a run interrupted and resumed
+cache's arrays (with the oracle's portable Manning power), writes it back in the same format, and a run interrupted and resumed
 from a checkpoint equals the uninterrupted run."""
 import json
 from pathlib import Path
@@ -39,7 +39,7 @@ def _oracle_from_cache():
 
 def test_from_cache_tables_state_and_run_bitwise():
     from geoswe_b200.compressed import CompressedSolver
-    cs = CompressedSolver.from_cache(CACHE)
+    cs = CompressedSolver.from_cache(CACHE, arith="portable")     # the oracle's Manning power
     assert np.array_equal(cs.nbr, _ld("nbr")) and np.array_equal(cs.is_active, _ld("is_active"))
     assert np.array_equal(cs.ij_active, _ld("ij_active"))
     for c in range(3):

@@ -2,7 +2,11 @@
 
 The oracle (oracle/gsw_oracle.c) evaluates the reference kernel text per cell with
 four faces; the kernel shares each face between its two cells. Both use separately
-rounded IEEE operations, so every comparison here is exact equality (-0 == +0).
+rounded IEEE operations, so every comparison here is exact equality (-0 == +0). The
+solvers run with arith="portable": the oracle restates Manning's h^(-4/3) as the
+portable Newton iteration (a CPU cannot reproduce CUDA's powf); the default "exact"
+arithmetic, powf included, is checked against the reference's own kernel in
+test_reference_gpu.py.
 """
 
 import numpy as np
@@ -20,7 +24,7 @@ def _solver(q0, bed, dtype, ngh=2, dx=2.0, dy=2.0, **cfgkw):
     from geoswe_b200 import Config, Mesh2D, Solver2D
     nx, ny = bed.shape
     mesh = Mesh2D(nx=nx, ny=ny, dx=dx, dy=dy, ngh=ngh)
-    kw = dict(bc_x="wall", bc_y="wall", dtype=dtype, h_min=1e-6)
+    kw = dict(bc_x="wall", bc_y="wall", dtype=dtype, h_min=1e-6, arith="portable")
     kw.update(cfgkw)
     cfg = Config(**kw)
     return Solver2D(mesh, cfg, q0, bed)
@@ -328,7 +332,7 @@ def test_stage_boundary_and_inflow_match_oracle():
     edge = np.zeros((nx, ny), bool)
     edge[0, :] = True
     sb = StageBoundary.from_mask(edge, mesh, z, time_s=[0.0, 600.0], stage_m=[1.0, 1.4])
-    cfg = Config(bc_x="wall", bc_y="wall", stage_boundary=sb, friction="manning", manning_n=0.03)
+    cfg = Config(bc_x="wall", bc_y="wall", stage_boundary=sb, friction="manning", manning_n=0.03, arith="portable")
     s = Solver2D(mesh, cfg, q0, z)
     ii = np.full(6, nx - 1 + ngh)
     jj = np.arange(20, 26) + ngh

@@ -13,7 +13,7 @@ torch = pytest.importorskip("torch")
 def _dense(q0, bed, mask, dx=2.0, **cfgkw):
     from geoswe_b200 import Config, Mesh2D, Solver2D
     nx, ny = bed.shape
-    kw = dict(bc_x="fall", bc_y="fall")
+    kw = dict(bc_x="fall", bc_y="fall", arith="portable")   # the oracle's Manning power
     kw.update(cfgkw)
     s = Solver2D(Mesh2D(nx=nx, ny=ny, dx=dx, dy=dx, ngh=2), Config(**kw), q0, bed)
     if mask is not None:

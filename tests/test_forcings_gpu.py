@@ -29,7 +29,7 @@ def _solver(seed=5, nx=52, ny=60, dx=4.0):
     rng = np.random.default_rng(seed)
     h = np.where(mask, np.maximum(np.quantile(z, 0.5) - z, 0.0) + 0.02 * rng.random(z.shape), 0.0)
     q0 = np.stack([h, 0.05 * (rng.random(z.shape) - 0.5) * (h > 0), 0.05 * (rng.random(z.shape) - 0.5) * (h > 0)])
-    s = Solver2D(Mesh2D(nx=nx, ny=ny, dx=dx, dy=dx, ngh=2), Config(bc_x="fall", bc_y="fall", friction="manning"),
+    s = Solver2D(Mesh2D(nx=nx, ny=ny, dx=dx, dy=dx, ngh=2), Config(bc_x="fall", bc_y="fall", friction="manning", arith="portable"),
                  q0.astype(np.float32), z)
     s.set_inside_mask(mask)
     cls = voronoi_classes(nx, ny, n_seeds=10, seed=seed)
