@@ -75,6 +75,20 @@ def voronoi_classes_fast(nx, ny, n_seeds=256, n_classes=4, seed=0):
     return out
 
 
+def voronoi_classes_window(nx, ny, i0, i1, j0, j1, n_seeds=256, n_classes=4, seed=0):
+    """Classes of the cells [i0, i1) x [j0, j1) of voronoi_classes(nx, ny, ...): the same
+    seeds and nearest-seed rule, evaluated on the window only (a crop of a large case
+    without classifying the whole grid)."""
+    from scipy.spatial import cKDTree
+    rng = np.random.default_rng(seed + 7919)
+    pts = rng.random((n_seeds, 2)) * np.array([nx, ny], dtype=np.float64)
+    cls_of_seed = rng.integers(n_classes, size=n_seeds).astype(np.uint8)
+    ci, cj = np.meshgrid(np.arange(i0, i1, dtype=np.float64) + 0.5, np.arange(j0, j1, dtype=np.float64) + 0.5,
+                         indexing="ij")
+    _, idx = cKDTree(pts).query(np.stack([ci.ravel(), cj.ravel()], axis=1))
+    return cls_of_seed[idx].reshape(i1 - i0, j1 - j0)
+
+
 def dilate_cross(mask, iterations):
     """scipy.ndimage.binary_dilation(mask, iterations=k) with the default cross."""
     m = np.asarray(mask, dtype=bool).copy()

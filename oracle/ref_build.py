@@ -1,6 +1,9 @@
 """Compile the reference's own dense-step CUDA kernels for sm_100a -- TEST INFRASTRUCTURE.
 
-    python oracle/ref_build.py [--ref /root/reference/src]
+    python oracle/ref_build.py [--ref <reference checkout>/src]
+
+The reference tree is taken from --ref, else from $GEOSWE_REFERENCE_SRC, else from the
+standard checkout location of this build host (reference_src() below).
 
 The reference keeps its GPU kernels as CUDA C text inside Python and assembles the
 production variants at import (geoswe/rhs_cuda.py:1698-2192, geoswe/solver.py:152-205).
@@ -8,14 +11,16 @@ This recipe imports the reference package with a recording stand-in for CuPy, so
 exact text the reference would hand to NVRTC is captured, and compiles it with nvcc:
 
   oracle/_ref/ref_kernels.cu          the captured reference text + C launch wrappers
-                                      (the dense fused step, the residual, lammax, and
-                                      the flat loop's per-step forcing kernels)
+                                      (the dense fused step, the residual, lammax, the
+                                      flat fused step + CFL and the flat lammax (L2 and
+                                      Linf norms), and the flat loop's per-step forcing
+                                      kernels)
   oracle/_ref/libref_fma.so           nvcc defaults (FMA contraction on, as NVRTC)
   oracle/_ref/libref_strict.so        --fmad=false (every operation rounded separately)
 
 oracle/_ref/ is git-ignored (the reference's source is not committed) but travels to
 the GPU box with the other built libraries; oracle/ref_runner.py drives the kernels
-there as the reference's dense solver does. Nothing in the product uses them.
+there as the reference's dense and flat solvers do. Nothing in the product uses them.
 """
 from __future__ import annotations
 
@@ -66,7 +71,14 @@ def _fake_cupy():
 
 
 def capture(ref_src):
-    """Return {kernel_name: source} of the production dense kernels of the reference."""
+    """Return {kernel_name: source} of the reference's production kernels: the dense fused
+    step and residual (rhs_cuda.py:2095-2192, 900-1207), lammax (solver.py:152-205), the
+    flat fused step + CFL as CompressedStepper assembles it with the chained neighbour
+    preamble (compressed_rhs.py:1082-1118 over :92-112, :716-748, :1027-1039; the reg2
+    preambles index the same cells by arithmetic, compressed_rhs.py:867-877), in its no-sigma
+    build with the L2 and the Linf wave-speed norm (compressed_solver.py:819-843), the flat
+    lammax kernel used for a run's first dt (compressed_solver.py:200-244, 655-668), and
+    the flat loop's per-step forcing kernels."""
     os.environ["GEOSWE_BACKEND"] = "cupy"
     for k in ("SWE_DENSE_XY", "SWE_BED_GRAD_LIMITER", "SWE_DRY_SKIP", "SWE_WETDRY_ZERO_H",
               "SWE_DENSE_MAXRREG"):
@@ -79,7 +91,18 @@ def capture(ref_src):
     kres = R._build_srm_hllc_ns("float", "fused_rhs_wb_srm_hllc_2d_ns_fp32")
     kres64 = R._build_srm_hllc_ns("double", "fused_rhs_wb_srm_hllc_2d_ns_fp64")
     from geoswe import compressed_solver as CS
+    from geoswe import compressed_rhs as CR
+    keep_h = int(CS._WETDRY_KEEP_H)
+    kfl = CR.build_flat_fused_step_cfl_kernel(CR._PRE_B_FLAT, keep_h, no_sigma=True, tag="chained", linf=False)
+    kfl_inf = CR.build_flat_fused_step_cfl_kernel(CR._PRE_B_FLAT, keep_h, no_sigma=True, tag="chained", linf=True)
+    # the Linf lammax is the reference's own rewrite of its L2 text (compressed_solver.py:664-666),
+    # renamed so both live in one module
+    lam_inf = CS._CFL_LAMMAX_FLAT_BLK_NS_SRC.replace("sqrtf(u*u + v*v)", "fmaxf(fabsf(u), fabsf(v))").replace(
+        "cfl_lammax_flat_blk_ns", "cfl_lammax_flat_blk_ns_linf")
+    assert "fmaxf(fabsf(u), fabsf(v))" in lam_inf
     return {k2d.name: k2d.code, kres.name: kres.code, kres64.name: kres64.code,
+            kfl.name: kfl.code, kfl_inf.name: kfl_inf.code,
+            "cfl_lammax_flat_blk_ns": CS._CFL_LAMMAX_FLAT_BLK_NS_SRC, "cfl_lammax_flat_blk_ns_linf": lam_inf,
             "lammax_fp32_lean": S._CFL_LAMMAX_SRC_LEAN,
             # the flat loop's per-step forcings (compressed_solver.py:143-158, 268-283, 313-437, 1320-1328)
             "infiltrate_flat": CS._INFILTRATE_SRC, "drain_cap": CS._DRAIN_CAP_SRC,
@@ -138,6 +161,36 @@ extern "C" int ref_forcing(int which, float* q0, float* q1, float* q2, const uns
     }
     return (int)cudaGetLastError();
 }
+// the flat fused step + CFL (signature: rhs_cuda.py:900-914 with compressed_rhs.py:44-47,
+// 687-694, 1100-1102; launched as CompressedStepper.rhs_fused, compressed_solver.py:880-905:
+// 256 threads, region_mode 0, no sigma, inv_sig = a length-1 array of ones with stride 0)
+extern "C" int ref_flat_fstep(int linf, const float* q0, const float* q1, const float* q2, const float* b,
+    float* qn0, float* qn1, float* qn2, int N, float inv_dx, float g, float h_min, const short* nbr,
+    const unsigned char* is_active, const float* rate_row, const int* lk, int have_rain, const float* ones1,
+    const unsigned char* n_cls, const float* n_tab, float* max_h, int have_max, float dt, float vcap,
+    int use_quadratic, unsigned int* cfl_bits, float h_min_cfl, float* dummy, void* stream) {
+    const int grid = (N + 255) / 256;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (linf)
+        flat_srm_hllc_fstepcfl_chained_linf_ns_float<<<grid, 256, 0, s>>>(q0, q1, q2, dummy, b, dummy, dummy, dummy,
+            N, 0, inv_dx, inv_dx, g, h_min, nbr, is_active, is_active, 0, qn0, qn1, qn2, rate_row, lk, have_rain,
+            ones1, 0, n_cls, n_tab, max_h, have_max, dt, vcap, use_quadratic, cfl_bits, h_min_cfl, 0);
+    else
+        flat_srm_hllc_fstepcfl_chained_ns_float<<<grid, 256, 0, s>>>(q0, q1, q2, dummy, b, dummy, dummy, dummy,
+            N, 0, inv_dx, inv_dx, g, h_min, nbr, is_active, is_active, 0, qn0, qn1, qn2, rate_row, lk, have_rain,
+            ones1, 0, n_cls, n_tab, max_h, have_max, dt, vcap, use_quadratic, cfl_bits, h_min_cfl, 0);
+    return (int)cudaGetLastError();
+}
+// the flat lammax (compressed_solver.py:200-244), launched as CompressedStepper.cfl_dt does
+// (2048 blocks of 256, compressed_solver.py:735-739)
+extern "C" int ref_flat_lammax(int linf, const float* q0, const float* q1, const float* q2,
+    const unsigned char* act, int N, float g, float h_min, float h_min_cfl, unsigned int* out_bits,
+    const float* dummy, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if (linf) cfl_lammax_flat_blk_ns_linf<<<2048, 256, 0, s>>>(q0, q1, q2, dummy, act, N, g, h_min, h_min_cfl, out_bits);
+    else cfl_lammax_flat_blk_ns<<<2048, 256, 0, s>>>(q0, q1, q2, dummy, act, N, g, h_min, h_min_cfl, out_bits);
+    return (int)cudaGetLastError();
+}
 extern "C" int ref_lammax(const float* q0, const float* q1, const float* q2, int nx, int ny,
     int nyp, int ngh, float g, float h_cfl, unsigned int* out_bits, const unsigned char* ghost,
     void* stream) {
@@ -150,7 +203,14 @@ extern "C" int ref_lammax(const float* q0, const float* q1, const float* q2, int
 """
 
 
-def build(ref_src="/root/reference/src"):
+def reference_src():
+    """The reference package's source directory: $GEOSWE_REFERENCE_SRC when set, else the
+    checkout location of this build host. The GPU box has neither; nothing there needs it."""
+    return Path(os.environ.get("GEOSWE_REFERENCE_SRC", "/root/reference/src"))
+
+
+def build(ref_src=None):
+    ref_src = Path(ref_src) if ref_src is not None else reference_src()
     if not Path(ref_src).exists():
         raise FileNotFoundError(f"reference tree {ref_src} not found (the recipe runs where it is)")
     srcs = capture(ref_src)
@@ -160,7 +220,7 @@ def build(ref_src="/root/reference/src"):
         parts.append(f"// ---- {name} (captured from the reference) ----\n")
         # each captured text defines its own macros (WETDRY_KEEP_H); keep them per kernel
         parts.append(code)
-        parts.append("\n#undef WETDRY_KEEP_H\n#undef BSIZE\n")
+        parts.append("\n#undef WETDRY_KEEP_H\n#undef BSIZE\n#undef _RSTRIDE\n")
     cu = OUT / "ref_kernels.cu"
     cu.write_text("".join(parts) + _WRAPPERS)
     nvcc = "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc"
@@ -173,6 +233,6 @@ def build(ref_src="/root/reference/src"):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference/src")
+    ap.add_argument("--ref", default=None, help="reference src directory (default: reference_src())")
     a = ap.parse_args()
     print(build(a.ref))

@@ -194,3 +194,104 @@ def ref_forcing(which, q, *, cls=None, t0=None, t1=None, t2=None, F=None, Fmax=N
                        C.c_float(dt), C.c_float(h_min), _stream())
     if rc != 0:
         raise RuntimeError(f"ref_forcing({which}): CUDA error {rc}")
+
+
+class RefFlatGPU:
+    """fp32 compressed-mesh run of the reference GPU path: its flat fused step + CFL kernel
+    (chained neighbour preamble, no sigma, L2 or Linf wave-speed norm) on the canonical
+    tables, driven by the reference's flat loop (geoswe/compressed_solver.py:2133-2400):
+    the first dt from the standalone flat lammax (cfl_dt, :721-748), every later dt from the
+    lambda the fused step reduced over the new state (dt_from_lam, :713-719), dt =
+    min(dt, t_end - t), the rain row by searchsorted(right) - 1 clamped, t += dt, while
+    t < t_end - 1e-9; rain on a dry bed bounds dt by (cfl dx)^(2/3) / (g R_max)^(1/3)
+    (:3426-3431). No forcings, ring or inlets (the loop's fused-CFL path, :2100-2103).
+
+    Arrays are canonical-order NumPy: nbr (N, 4) int16 deltas, is_active (N,) uint8,
+    q (3, N) float32, bed (N,) float32, n_cls (N,) uint8, n_tab; rain_table (nt, ncol)
+    float32 in m/s with rain_times (nt,) and rain_lookup (N,) int32."""
+
+    def __init__(self, nbr, is_active, q, bed, dx, *, n_cls, n_tab, g=9.81, h_min=1e-6, cfl=0.5, linf=False,
+                 vcap=15.0, quad=True, rain_times=None, rain_table=None, rain_lookup=None, dt_max=None,
+                 variant="fma"):
+        import torch
+        self.L = _lib(variant)
+        self.L.ref_flat_fstep.restype = C.c_int
+        self.L.ref_flat_lammax.restype = C.c_int
+        dev = "cuda"
+        self.N = int(np.asarray(is_active).shape[0])
+        self.nbr = torch.from_numpy(np.ascontiguousarray(nbr, dtype=np.int16).reshape(-1)).to(dev)
+        self.act = torch.from_numpy(np.ascontiguousarray(is_active, dtype=np.uint8)).to(dev)
+        self.q = [torch.from_numpy(np.ascontiguousarray(q[c], dtype=np.float32)).to(dev) for c in range(3)]
+        self.qn = [torch.zeros_like(self.q[0]) for _ in range(3)]
+        self.b = torch.from_numpy(np.ascontiguousarray(bed, dtype=np.float32)).to(dev)
+        self.ncls = torch.from_numpy(np.ascontiguousarray(n_cls, dtype=np.uint8)).to(dev)
+        self.ntab = torch.from_numpy(np.asarray(n_tab, dtype=np.float32)).to(dev)
+        self.max_h = torch.zeros(self.N, dtype=torch.float32, device=dev)
+        self.bits = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.ones1 = torch.ones(1, dtype=torch.float32, device=dev)
+        self.dummy = torch.zeros(4, dtype=torch.float32, device=dev)
+        self.dx, self.g, self.h_min, self.cfl, self.linf = float(dx), float(g), float(h_min), float(cfl), int(bool(linf))
+        self.h_min_cfl = max(float(h_min), 1.0e-6)
+        self.vcap, self.quad = float(vcap), int(bool(quad))
+        self.rain_on = rain_table is not None
+        self.dt_max = dt_max
+        if self.rain_on:
+            tab = np.ascontiguousarray(rain_table, dtype=np.float32)
+            self.rain_t = np.asarray(rain_times, dtype=np.float64)
+            self.rate = torch.from_numpy(tab).to(dev)
+            self.lk = torch.from_numpy(np.ascontiguousarray(rain_lookup, dtype=np.int32)).to(dev)
+            rmax = float(tab.max())
+            if rmax > 0.0:
+                lim = (self.cfl * self.dx) ** (2.0 / 3.0) / (self.g * rmax) ** (1.0 / 3.0)
+                self.dt_max = lim if self.dt_max is None else min(self.dt_max, lim)
+        self.t = 0.0
+        self.nsteps = 0
+
+    def _float_bits(self):
+        return float(self.bits.cpu().numpy().view(np.float32)[0])
+
+    def cfl_dt(self):
+        self.bits.zero_()
+        rc = self.L.ref_flat_lammax(self.linf, _p(self.q[0]), _p(self.q[1]), _p(self.q[2]), _p(self.act),
+                                    C.c_int(self.N), C.c_float(self.g), C.c_float(self.h_min),
+                                    C.c_float(self.h_min_cfl), _p(self.bits), _p(self.dummy), _stream())
+        assert rc == 0, rc
+        lam = self._float_bits()
+        if not (lam == lam and lam < float("inf")):
+            return 0.0
+        return self.dt_from_lam(lam)
+
+    def dt_from_lam(self, lam):
+        floor = (self.g * self.h_min) ** 0.5
+        if lam < floor:
+            lam = floor
+        dt = self.cfl * self.dx / (lam + 1e-12)
+        return dt if self.dt_max is None else min(dt, self.dt_max)
+
+    def run(self, t_end, max_steps=10 ** 9):
+        steps = 0
+        lam_next = None
+        while self.t < t_end - 1e-9 and steps < max_steps:
+            dtl = self.dt_from_lam(lam_next) if lam_next is not None else self.cfl_dt()
+            if not (dtl > 0.0):
+                raise FloatingPointError("non-finite max wave speed")
+            dt = min(dtl, t_end - self.t)
+            if self.rain_on:
+                it = max(0, min(self.rate.shape[0] - 1, int(np.searchsorted(self.rain_t, self.t, "right") - 1)))
+                row, lk = self.rate[it], self.lk
+            else:
+                row, lk = self.dummy, self.dummy
+            self.bits.zero_()
+            rc = self.L.ref_flat_fstep(
+                self.linf, _p(self.q[0]), _p(self.q[1]), _p(self.q[2]), _p(self.b), _p(self.qn[0]), _p(self.qn[1]),
+                _p(self.qn[2]), C.c_int(self.N), C.c_float(1.0 / self.dx), C.c_float(self.g), C.c_float(self.h_min),
+                _p(self.nbr), _p(self.act), _p(row), _p(lk), int(self.rain_on), _p(self.ones1), _p(self.ncls),
+                _p(self.ntab), _p(self.max_h), 1, C.c_float(dt), C.c_float(self.vcap), self.quad, _p(self.bits),
+                C.c_float(self.h_min_cfl), _p(self.dummy), _stream())
+            assert rc == 0, rc
+            self.q, self.qn = self.qn, self.q
+            lam_next = self._float_bits()
+            self.t += dt
+            self.nsteps += 1
+            steps += 1
+        return steps

@@ -1,6 +1,9 @@
 """Generate the golden fixtures of tests/golden/ by running the reference itself.
 
-    python tests/golden/make_golden.py [--ref /root/reference/src]
+    python tests/golden/make_golden.py [--ref <reference checkout>/src]
+
+(default: oracle.ref_build.reference_src(), i.e. $GEOSWE_REFERENCE_SRC or the build
+host's checkout)
 
 Imports the reference package (geoswe) with its NumPy backend from the read-only
 reference tree and records, for small seeded inputs, what its own CPU path computes:
@@ -256,9 +259,9 @@ def cache_cases(G, out_dir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference/src")
+    ap.add_argument("--ref", default=None)
     a = ap.parse_args()
-    G = _import_reference(a.ref)
+    G = _import_reference(a.ref or _default_ref())
     out = {}
     residual_cases(G, out)
     run_cases(G, out)
@@ -271,9 +274,15 @@ def main():
         print(f, (HERE / f).stat().st_size, "bytes")
 
 
-def main_mesh(ref="/root/reference/src"):
+def _default_ref():
+    sys.path.insert(0, str(HERE.parents[1]))
+    from oracle.ref_build import reference_src
+    return str(reference_src())
+
+
+def main_mesh(ref=None):
     """Only the mesh tables (reference_mesh.npz)."""
-    G = _import_reference(ref)
+    G = _import_reference(ref or _default_ref())
     mesh_out = {}
     mesh_cases(G, mesh_out)
     np.savez_compressed(HERE / "reference_mesh.npz", **mesh_out)
