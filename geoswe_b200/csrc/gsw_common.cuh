@@ -21,6 +21,15 @@ float div_const_recip(float g);
 
 namespace gsw {
 
+// Whether this compilation's binary32 step kernels may evaluate Manning's power by powf
+// (GSW_ARITH_EXACT): the exact compilation yes, the fast one never (it keeps pow_m43).
+// The choice is a template parameter of the step kernels, so each kernel holds one path.
+#ifdef GSW_FAST_ARITH
+constexpr bool kRefPowBuild = false;
+#else
+constexpr bool kRefPowBuild = true;
+#endif
+
 using gsw_rt::set_error;
 using gsw_rt::check_launch;
 using gsw_rt::sm_count;

@@ -39,7 +39,6 @@ struct DenseK {
     T h_cfl;
     int tile_rows;
     T g_recip;                   // RN(1/g) for the star depth's h / g, or 0 (gsw_core.cuh div_g)
-    int ref_pow;                 // 1: Manning's h^(-4/3) by powf (GSW_ARITH_EXACT), 0: by pow_m43
 };
 
 template <typename T>
@@ -96,7 +95,8 @@ template <> __device__ __forceinline__ float  dt_of<float>(const GswLoopState* s
 template <> __device__ __forceinline__ double dt_of<double>(const GswLoopState* st) { return st->dt; }
 
 // STEP = false: residual into o0..o2. STEP = true: updated state into o0..o2.
-template <typename T, bool STEP, int MINB>
+// REFPOW: Manning's h^(-4/3) by powf (GSW_ARITH_EXACT) instead of pow_m43.
+template <typename T, bool STEP, int MINB, bool REFPOW>
 __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
     if (STEP && p.st->done) return;                       // grid-uniform
     const int lane = threadIdx.x;
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
                         n = p.ncls ? p.ntab[p.ncls[(int64_t)r * p.cpitch + c]] : p.ntab[0];
                     else if (p.friction_kind == GSW_FRICTION_FIELD) n = p.nfield[o];
                     wetdry_friction<T>(h, hu, hv, p.friction_kind != GSW_FRICTION_NONE, n, dt, p.g,
-                                       p.h_min, p.vcap, p.quad != 0, p.keep_h != 0, p.ref_pow != 0);
+                                       p.h_min, p.vcap, p.quad != 0, p.keep_h != 0, REFPOW);
                     p.o0[o] = h; p.o1[o] = hu; p.o2[o] = hv;
                     if (p.max_h != nullptr && h > p.max_h[o]) p.max_h[o] = h;
                     if (p.lam != nullptr) {
@@ -245,7 +245,6 @@ inline int fill_dense(const GswDenseArgs* a, DenseK<T>& k, bool step) {
     }
     k.g = (T)a->g; k.h_min = (T)a->h_min;
     k.g_recip = sizeof(T) == 4 ? (T)div_const_recip((float)a->g) : (T)0;
-    k.ref_pow = a->arith == GSW_ARITH_EXACT ? 1 : 0;
     k.st = a->state; k.lam = (unsigned long long*)a->lam_target;
     k.rain_kind = a->rain_kind; k.rain = (const T*)a->rain;
     k.friction_kind = a->friction_kind; k.ncls = a->n_cls; k.cpitch = a->n_cls_pitch;
@@ -276,6 +275,16 @@ inline int fill_dense(const GswDenseArgs* a, DenseK<T>& k, bool step) {
     return GSW_OK;
 }
 
+template <typename T, bool STEP, bool REFPOW>
+inline void launch_march_shape(const DenseK<T>& k, int minb, dim3 grid, dim3 block, cudaStream_t s) {
+    // register caps apply to the binary32 step; the residual and binary64 use the compiler's choice
+    constexpr bool capped = STEP && sizeof(T) == 4;
+    if (capped && minb == 3) dense_march_kernel<T, STEP, capped ? 3 : 1, REFPOW><<<grid, block, 0, s>>>(k);
+    else if (capped && minb == 4) dense_march_kernel<T, STEP, capped ? 4 : 1, REFPOW><<<grid, block, 0, s>>>(k);
+    else if (capped && minb == 5) dense_march_kernel<T, STEP, capped ? 5 : 1, REFPOW><<<grid, block, 0, s>>>(k);
+    else dense_march_kernel<T, STEP, 1, REFPOW><<<grid, block, 0, s>>>(k);
+}
+
 template <typename T, bool STEP>
 inline int launch_march(const GswDenseArgs* a, cudaStream_t s) {
     DenseK<T> k;
@@ -290,12 +299,9 @@ inline int launch_march(const GswDenseArgs* a, cudaStream_t s) {
     dim3 block(32, W);
     dim3 grid((strips + W - 1) / W, (nrows + k.tile_rows - 1) / k.tile_rows);
     if (grid.y > 65535u) return set_error(GSW_ERR_INVALID, "dense: too many row tiles (%u); raise tile_rows", grid.y);
-    // register caps apply to the binary32 step; the residual and binary64 use the compiler's choice
-    constexpr bool capped = STEP && sizeof(T) == 4;
-    if (capped && minb == 3) dense_march_kernel<T, STEP, capped ? 3 : 1><<<grid, block, 0, s>>>(k);
-    else if (capped && minb == 4) dense_march_kernel<T, STEP, capped ? 4 : 1><<<grid, block, 0, s>>>(k);
-    else if (capped && minb == 5) dense_march_kernel<T, STEP, capped ? 5 : 1><<<grid, block, 0, s>>>(k);
-    else dense_march_kernel<T, STEP, 1><<<grid, block, 0, s>>>(k);
+    constexpr bool can_refpow = kRefPowBuild && STEP && sizeof(T) == 4;
+    if (can_refpow && a->arith == GSW_ARITH_EXACT) launch_march_shape<T, STEP, can_refpow>(k, minb, grid, block, s);
+    else launch_march_shape<T, STEP, false>(k, minb, grid, block, s);
     return check_launch("dense_march");
 }
 

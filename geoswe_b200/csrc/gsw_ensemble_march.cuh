@@ -73,7 +73,7 @@ __device__ __forceinline__ void build_run_list(const GswEnsembleArgs& a, int tid
         }
 }
 
-template <int MINB>
+template <int MINB, bool REFPOW>
 __global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArgs a, FlatMesh<float> m) {
     if (*a.all_done) return;
     const int lane = threadIdx.x;
@@ -111,10 +111,10 @@ __global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArg
         const GswLoopState* st = a.states + mi;
         if (st->done) continue;                                   // warp-uniform
         const GswMember& mb = a.members[mi];
-        const FlatPhys<float> ph = member_phys(mb, a.arith == GSW_ARITH_EXACT ? 1 : 0);
+        const FlatPhys<float> ph = member_phys(mb, REFPOW ? 1 : 0);
         const float dt = st->dt_f32;
         const float rate = (mb.rain_kind == GSW_RAIN_UNIFORM) ? mb.rain[st->rain_idx] : 0.0f;
-        unsigned long long lam = flat_brick<float, true>(m, ph, b, seg * m.bh / S, (seg + 1) * m.bh / S, dt, rate,
+        unsigned long long lam = flat_brick<float, true, REFPOW>(m, ph, b, seg * m.bh / S, (seg + 1) * m.bh / S, dt, rate,
                                                          nullptr);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -156,6 +156,14 @@ __global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArg
     }
 }
 
+template <bool REFPOW>
+inline void launch_ensemble_shape(const GswEnsembleArgs* a, const FlatMesh<float>& m, int grid, int W, cudaStream_t st) {
+    if (a->min_blocks == 3) ensemble_step_kernel<3, REFPOW><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else if (a->min_blocks == 4) ensemble_step_kernel<4, REFPOW><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else if (a->min_blocks == 5) ensemble_step_kernel<5, REFPOW><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else ensemble_step_kernel<1, REFPOW><<<grid, dim3(32, W), 0, st>>>(*a, m);
+}
+
 // Launch of the step over checked arguments (outputs non-null).
 inline int launch_ensemble_step(const GswEnsembleArgs* a, cudaStream_t st) {
     const int W = a->warps > 0 ? a->warps : 4;
@@ -170,11 +178,10 @@ inline int launch_ensemble_step(const GswEnsembleArgs* a, cudaStream_t st) {
     m.o0 = a->qn0; m.o1 = a->qn1; m.o2 = a->qn2;
     m.b = a->bed; m.flags = a->flags; m.ncls = a->n_cls; m.max_h = a->max_h;
     m.bij = a->brick_ij; m.bnbr = a->brick_nbr; m.nb = a->n_bricks; m.bh = a->brick_h;
-    if (a->min_blocks == 3) ensemble_step_kernel<3><<<grid, dim3(32, W), 0, st>>>(*a, m);
-    else if (a->min_blocks == 4) ensemble_step_kernel<4><<<grid, dim3(32, W), 0, st>>>(*a, m);
-    else if (a->min_blocks == 5) ensemble_step_kernel<5><<<grid, dim3(32, W), 0, st>>>(*a, m);
-    else if (a->min_blocks == 0) ensemble_step_kernel<1><<<grid, dim3(32, W), 0, st>>>(*a, m);
-    else return set_error(GSW_ERR_INVALID, "ensemble: min_blocks must be 0, 3, 4 or 5");
+    if (a->min_blocks != 0 && (a->min_blocks < 3 || a->min_blocks > 5))
+        return set_error(GSW_ERR_INVALID, "ensemble: min_blocks must be 0, 3, 4 or 5");
+    if (kRefPowBuild && a->arith == GSW_ARITH_EXACT) launch_ensemble_shape<kRefPowBuild>(a, m, grid, W, st);
+    else launch_ensemble_shape<false>(a, m, grid, W, st);
     return check_launch("ensemble_step");
 }
 

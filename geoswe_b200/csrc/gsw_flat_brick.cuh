@@ -27,7 +27,8 @@ struct FlatPhys {
     const int32_t* lookup;   // GSW_RAIN_LOOKUP: per-slot column of the rain row
     int ncol;
     T g_recip;               // RN(1/g) for the star depth's h / g, or 0 (gsw_core.cuh div_g)
-    int ref_pow;             // 1: Manning's h^(-4/3) by powf (GSW_ARITH_EXACT), 0: by pow_m43
+    int ref_pow;             // 1: Manning's h^(-4/3) by powf (GSW_ARITH_EXACT), 0: by pow_m43 (read by
+                             // the adjoint; the step kernels take it as their REFPOW parameter)
 };
 
 // Row segments per brick when the caller leaves the choice to the library: one warp
@@ -108,8 +109,9 @@ __device__ __forceinline__ Face<T> shfl_up_face(const Face<T>& f) {
 // above and below past the brick's edge) and recomputes the x-face above row r0 from
 // the same inputs as the face below row r0-1, so splitting a brick's rows among warps
 // changes no value. STEP: the fused step (returns this lane's wave speed bits);
-// otherwise the residual. `frame` is the gridded rain frame, or null.
-template <typename T, bool STEP>
+// otherwise the residual. `frame` is the gridded rain frame, or null. REFPOW: Manning's
+// h^(-4/3) by powf (GSW_ARITH_EXACT) instead of pow_m43.
+template <typename T, bool STEP, bool REFPOW>
 __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, const FlatPhys<T>& ph, int64_t bidx,
                                                          int r0, int r1, T dt, T rate, const T* frame) {
     const int lane = threadIdx.x;
@@ -187,7 +189,7 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
                     T hv = cur.hv + dt * rhv;
                     const T n = m.ncls ? ph.ntab[m.ncls[o]] : ph.ntab[0];
                     wetdry_friction<T>(h, hu, hv, true, n, dt, ph.g, ph.h_min, ph.vcap,
-                                           ph.quad != 0, ph.keep_h != 0, ph.ref_pow != 0);
+                                           ph.quad != 0, ph.keep_h != 0, REFPOW);
                     m.o0[o] = h; m.o1[o] = hu; m.o2[o] = hv;
                     if (m.max_h != nullptr && h > m.max_h[o]) m.max_h[o] = h;
                     const unsigned long long lb = lam_flat_bits(h, hu, hv, ph.g, ph.h_min, ph.h_min_cfl,

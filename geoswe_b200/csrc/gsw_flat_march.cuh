@@ -14,7 +14,7 @@
 
 namespace gsw {
 
-template <typename T, bool STEP, int MINB>
+template <typename T, bool STEP, int MINB, bool REFPOW>
 __global__ void __launch_bounds__(256, MINB) flat_march_kernel(FlatK<T> p) {
     if (STEP && p.st->done) return;
     const int64_t item = (int64_t)blockIdx.x * blockDim.y + threadIdx.y;   // (brick, row segment)
@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(256, MINB) flat_march_kernel(FlatK<T> p) {
         if (p.ph.rain_kind == GSW_RAIN_LOOKUP) frame = p.ph.rain + (int64_t)p.st->rain_idx * p.ph.ncol;
     }
     if (bidx < p.m.nb)
-        lam_local = flat_brick<T, STEP>(p.m, p.ph, bidx, seg * p.m.bh / p.segs, (seg + 1) * p.m.bh / p.segs,
+        lam_local = flat_brick<T, STEP, REFPOW>(p.m, p.ph, bidx, seg * p.m.bh / p.segs, (seg + 1) * p.m.bh / p.segs,
                                         dt, rate, frame);
     if (STEP && p.lam != nullptr) block_max_to(lam_local, p.lam);
 }
@@ -72,6 +72,15 @@ inline int fill_flat(const GswFlatArgs* a, FlatK<T>& k, bool step) {
     return GSW_OK;
 }
 
+template <typename T, bool STEP, bool REFPOW>
+inline void launch_flat_shape(const FlatK<T>& k, int mb, unsigned blocks, int W, cudaStream_t s) {
+    constexpr bool capped = STEP && sizeof(T) == 4;   // register caps apply to the binary32 step
+    if (capped && mb == 3) flat_march_kernel<T, STEP, capped ? 3 : 1, REFPOW><<<blocks, dim3(32, W), 0, s>>>(k);
+    else if (capped && mb == 4) flat_march_kernel<T, STEP, capped ? 4 : 1, REFPOW><<<blocks, dim3(32, W), 0, s>>>(k);
+    else if (capped && mb == 5) flat_march_kernel<T, STEP, capped ? 5 : 1, REFPOW><<<blocks, dim3(32, W), 0, s>>>(k);
+    else flat_march_kernel<T, STEP, 1, REFPOW><<<blocks, dim3(32, W), 0, s>>>(k);
+}
+
 template <typename T, bool STEP>
 inline int launch_flat(const GswFlatArgs* a, cudaStream_t s) {
     FlatK<T> k;
@@ -84,11 +93,9 @@ inline int launch_flat(const GswFlatArgs* a, cudaStream_t s) {
     if (blocks > 0x7fffffffLL) return set_error(GSW_ERR_INVALID, "flat: too many bricks");
     const int mb = a->min_blocks;
     if (mb != 0 && (mb < 3 || mb > 5)) return set_error(GSW_ERR_INVALID, "flat: min_blocks must be 0, 3, 4 or 5");
-    constexpr bool capped = STEP && sizeof(T) == 4;   // register caps apply to the binary32 step
-    if (capped && mb == 3) flat_march_kernel<T, STEP, capped ? 3 : 1><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
-    else if (capped && mb == 4) flat_march_kernel<T, STEP, capped ? 4 : 1><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
-    else if (capped && mb == 5) flat_march_kernel<T, STEP, capped ? 5 : 1><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
-    else flat_march_kernel<T, STEP, 1><<<(unsigned)blocks, dim3(32, W), 0, s>>>(k);
+    constexpr bool can_refpow = kRefPowBuild && STEP && sizeof(T) == 4;
+    if (can_refpow && a->arith == GSW_ARITH_EXACT) launch_flat_shape<T, STEP, can_refpow>(k, mb, (unsigned)blocks, W, s);
+    else launch_flat_shape<T, STEP, false>(k, mb, (unsigned)blocks, W, s);
     return check_launch("flat_march");
 }
 

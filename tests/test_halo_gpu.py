@@ -1,7 +1,7 @@
 """A dense run split over ranks equals the single-domain run bit for bit.
 
-Two processes share the one GPU, each a rank of a gloo group running ``Solver2D`` on
-its block (faces staged through host memory, as the exchange does for any backend but
+Two (or, for a 2 x 2 split, four) processes share the one GPU, each a rank of a gloo
+group running ``Solver2D`` on its block (faces staged through host memory, as the exchange does for any backend but
 NCCL); the kernels of the two processes never wait on each other -- every wait is on
 the host, in the gloo calls. The single-domain run is this process's own.
 """
@@ -67,6 +67,8 @@ def _rank(rank, world, port, out, dims, bc, dtype, host_loop):
     ([2, 1], ("wall", "extrapolate"), "float32", False),
     ([1, 2], ("wall", "wall"), "float32", False),
     ([2, 1], ("periodic", "wall"), "float64", True),
+    # four bands around the interior window, the y-bands limited to the rows between the x-bands
+    ([2, 2], ("wall", "extrapolate"), "float32", False),
 ])
 def test_split_run_equals_single_domain(dims, bc, dtype, host_loop):
     q0, bed = flowing(NX, NY, seed=5, dtype=np.dtype(dtype))
@@ -74,14 +76,15 @@ def test_split_run_equals_single_domain(dims, bc, dtype, host_loop):
     ref_steps = ref.run(T_END, callback=(lambda solver, k: None) if host_loop else None)
     want = ref.q_interior.detach().cpu().numpy()
     torch.cuda.synchronize()
+    world = dims[0] * dims[1]
     ctx = mp.get_context("spawn")
     with ctx.Manager() as m:
         out = m.dict()
-        mp.start_processes(_rank, args=(2, _free_port(), out, dims, bc, dtype, host_loop), nprocs=2,
+        mp.start_processes(_rank, args=(world, _free_port(), out, dims, bc, dtype, host_loop), nprocs=world,
                            start_method="spawn", join=True)
         out = dict(out)
     assert ref_steps > 20
-    for r in range(2):
+    for r in range(world):
         o = out[r]
         x0, x1, y0, y1 = o["block"]
         assert o["refused"], "add_inflow on a split run must raise"
