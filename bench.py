@@ -41,54 +41,104 @@ def _peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (SM MHz, throttle reasons)."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled during a timed region. NVML is polled
+    from a thread every 5 ms, with one sample at start() and one at stop(), so a region
+    of a few tens of milliseconds is covered too; nvidia-smi (200 ms) is the fallback.
+    Reads only: no clock or other GPU setting is changed."""
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
 
     def __init__(self, index=0):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.samples = []            # (sm MHz, reasons bitmask)
+        self.smax = None
+        self._h = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._smi = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:   # the CUDA device's own NVML handle (CUDA_VISIBLE_DEVICES may renumber)
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid) if not uuid.startswith("GPU-") else uuid)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _sample(self):
+        import pynvml
+        sm = pynvml.nvmlDeviceGetClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+        self.samples.append((float(sm), int(rs)))
+
+    def _poll(self):
+        while not self._stop.wait(0.005):
+            try:
+                self._sample()
+            except Exception:
+                return
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+            import pynvml
+            self._h = self._handle()
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM))
+            self._sample()
+            self._thread = threading.Thread(target=self._poll, daemon=True)
+            self._thread.start()
+        except Exception:
+            self._h = None
+            self._start_smi()
+
+    def _start_smi(self):
+        q = ("index,clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._smi = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            self._lines = []
+            self._thread = threading.Thread(target=lambda: self._lines.extend(ln.strip() for ln in self._smi.stdout),
+                                            daemon=True)
+            self._thread.start()
         except Exception:
-            self.proc = None
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self._smi = None
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
+        if self._h is not None:
+            self._stop.set()
+            self._thread.join(timeout=1.0)
             try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                self._sample()
+            except Exception:
+                pass
+        elif self._smi is not None:
+            self._smi.terminate()
+            try:
+                self._smi.wait(timeout=5)
+            except Exception:
+                self._smi.kill()
+            bits = [self.REASONS[k] for k in ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                              "sw_power_cap")]
+            for ln in self._lines:
+                f = [x.strip() for x in ln.split(",")]
+                try:
+                    sm, self.smax = float(f[1]), float(f[2])
+                except (ValueError, IndexError):
+                    continue
+                self.samples.append((sm, sum(b for b, v in zip(bits, f[3:7]) if v.lower().startswith("active"))))
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no NVML or nvidia-smi"], "samples": 0}
+        sm = [s for s, _ in self.samples]
+        mask = 0
+        for _, r in self.samples:
+            mask |= r
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.smax,
+                "reasons": sorted(k for k, b in self.REASONS.items() if mask & b), "samples": len(sm),
+                "source": "nvml" if self._h is not None else "nvidia-smi"}
 
 
 def build_case(n, dtype="float32", seed=0):
@@ -108,9 +158,12 @@ def build_case(n, dtype="float32", seed=0):
     return z, cls
 
 
-def make_solver(z, cls, n, dtype="float32", arith="exact", block=None, comm=None, dims=None):
+def make_solver(z, cls, n, dtype="float32", arith="exact", block=None, comm=None, dims=None, q0=None,
+                clsp=None):
     """The rain-on-terrain solver; with `block` = (x0, x1, y0, y1) and `comm`, this rank's
-    block of the domain split over the ranks of `comm`."""
+    block of the domain split over the ranks of `comm`. `q0` and `clsp` (the padded
+    classes) may be given as the caller holds them (the end-to-end measurement passes
+    page-locked arrays)."""
     from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
     from geoswe_b200.synthetic import MANNING_CLASSES
     x0, x1, y0, y1 = block if block is not None else (0, n, 0, n)
@@ -118,25 +171,45 @@ def make_solver(z, cls, n, dtype="float32", arith="exact", block=None, comm=None
     cfg = Config(bc_x="wall", bc_y="wall", bc={"x+": "fall"}, cfl=0.5, dtype=dtype,
                  friction="manning", arith=arith,
                  rainfall_forcing=RainfallForcing(time_s=[0.0, 1e9], rate_mm_h=[50.0, 50.0]))
-    q0 = np.zeros((3, x1 - x0, y1 - y0), np.float32)
-    s = Solver2D(mesh, cfg, q0, z[x0:x1, y0:y1], comm=comm, dims=dims)
+    if q0 is None:
+        q0 = np.zeros((3, x1 - x0, y1 - y0), np.float32)
+    zb = z if block is None else z[x0:x1, y0:y1]
+    s = Solver2D(mesh, cfg, q0, zb, comm=comm, dims=dims)
     ngh = mesh.ngh
-    clsp = np.pad(cls, ngh, mode="edge")[x0:x1 + 2 * ngh, y0:y1 + 2 * ngh]
-    s.set_manning_table(np.ascontiguousarray(clsp), MANNING_CLASSES)
+    if clsp is None:
+        clsp = np.ascontiguousarray(np.pad(cls, ngh, mode="edge")[x0:x1 + 2 * ngh, y0:y1 + 2 * ngh])
+    s.set_manning_table(clsp, MANNING_CLASSES)
     return s
 
 
-# DRAM bytes per cell and launch of the step kernels, measured with ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of one launch) on the 4096 x 4096 case of
-# the same workload and scaled to a launch here by the cells it processes (the traffic
-# is proportional to the cells: no re-reads beyond the bricks' halo rows).
-DRAM_BYTES_PER_CELL = {"dense": 36.66, "flat": 32.13, "flat_compressed": 48.89}
+def counters():
+    """Per-kernel ncu counters from profiles/counters.json: DRAM bytes per updated cell
+    (dram__bytes_read.sum + dram__bytes_write.sum of one launch / its cells; the traffic
+    is proportional to the cells, so it scales to a launch of another size) and warp
+    instructions per updated cell (smsp__inst_executed.sum / cells; with the SM clock,
+    the instruction-issue roofline: one warp instruction per scheduler per cycle, four
+    schedulers per SM). Each entry names the library sources it was captured on;
+    `current_build` says whether that is the library measured here."""
+    p = ROOT / "profiles" / "counters.json"
+    d = json.loads(p.read_text()) if p.exists() else {}
+    try:
+        from geoswe_b200.build import source_hash
+        cur = source_hash()
+    except Exception:
+        cur = None
+    for v in d.values():
+        v["current_build"] = cur is not None and v.get("sources") == cur
+    return d
 
-# Warp instructions per updated cell of the step kernels: ncu smsp__inst_executed.sum of
-# one launch at 4096 x 4096 (tuned shape) divided by the cells it updates. With the SM
-# clock they give the instruction-issue roofline the step kernels are bound by: one warp
-# instruction per scheduler per cycle, four schedulers per SM.
-INST_PER_CELL = {"dense": 38.73, "dense_fast": 22.68, "flat_tidal": 34.23, "flat_compressed": 46.88}
+
+def _traffic(kind, cells):
+    c = counters().get(kind)
+    if not c or c.get("dram_bytes_per_cell") is None:
+        return None, None
+    return (c["dram_bytes_per_cell"] * cells / 1e9,
+            {"unit": "GB per launch", "source": f"profiles/counters.json[{kind}] ({c.get('workload')})",
+             "dram_bytes_per_cell": c["dram_bytes_per_cell"], "captured_on_sources": c.get("sources"),
+             "current_build": c["current_build"]})
 
 
 def issue_roofline(kind, cells, kern_ms, clocks):
@@ -144,13 +217,18 @@ def issue_roofline(kind, cells, kern_ms, clocks):
     ncu count per cell x cells / the CUDA-event launch time) against 4 x SMs x the
     sampled SM clock (max clock when no sample)."""
     import torch
+    c = counters().get(kind)
+    if not c or c.get("warp_inst_per_cell") is None:
+        return None
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz") or 1965.0
     peak = 4.0 * sms * mhz * 1e6
-    achieved = INST_PER_CELL[kind] * cells / (kern_ms / 1e3)
-    return {"bound": "instruction issue", "warp_inst_per_cell": INST_PER_CELL[kind],
+    ipc = c["warp_inst_per_cell"]
+    achieved = ipc * cells / (kern_ms / 1e3)
+    return {"bound": "instruction issue", "warp_inst_per_cell": ipc,
             "achieved": achieved, "peak": peak, "unit": "warp instructions/s", "frac": achieved / peak,
-            "sm_mhz": mhz, "source": "ncu smsp__inst_executed.sum per cell (4096 x 4096, profiles/)"}
+            "sm_mhz": mhz, "source": f"profiles/counters.json[{kind}] ({c.get('workload')})",
+            "captured_on_sources": c.get("sources"), "current_build": c["current_build"]}
 
 
 def max_over_ranks(x, device):
@@ -226,7 +304,7 @@ def run_gsw(args, rank, world):
     z, cls = build_case(n)
     cells = n * n
     # ---------------- device-resident throughput (value), exact arithmetic ----------------
-    m = measure_dense(args, z, cls, n, world, "exact")
+    m = measure_dense(args, z, cls, n, world, args.dense_arith)
     ms, kern_ms = m["ms"], m["kern_ms"]
     # ---------------- end to end through the public API ----------------
     e2e = run_e2e(args, z, cls, n, world)
@@ -243,13 +321,14 @@ def run_gsw(args, rank, world):
         "e2e": e2e,
         "gpu_launches": int(m["launches"]),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": DRAM_BYTES_PER_CELL["dense"] * cells / 1e9,
-                     "traffic_unit": "GB per launch (ncu, 4096x4096 capture scaled by cells)",
+                     "frac": achieved / peak, "traffic": _traffic("dense", cells)[0],
+                     "traffic_from": _traffic("dense", cells)[1],
                      "kernel": "dense_march_kernel<float,true>", "kernel_ms": kern_ms,
                      "bytes_per_cell": bpc, "peak_source": peak_kind},
         "issue": issue_roofline("dense", cells, kern_ms, m["clocks"]),
         "clocks": m["clocks"],
-        "arith": "exact (IEEE, bit-identical to the reference kernel without FMA contraction)",
+        "arith": ("exact (IEEE, powf Manning power: bit-identical to the reference kernel without FMA contraction)"
+                  if args.dense_arith == "exact" else "portable (IEEE, Newton Manning power)"),
         "launch_shape": m["shape"],
     }
     if m["tune"] is not None:
@@ -270,6 +349,58 @@ def run_gsw(args, rank, world):
             "clocks": f["clocks"], "launch_shape": f["shape"]}
     if rank == 0 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args)
+    if world == 1 and not args.no_extras:
+        out.update(extras(args))
+    return out
+
+
+def extras(args):
+    """The rest of the metric on one GPU, each with its own workload and clock record:
+    `batched` (64-member ensemble vs a loop of the plain solver, one simulated hour),
+    `adjoint` (reverse step / forward step of the calibration case), `compressed` (the
+    rain-on-terrain case on the compressed mesh, dense/compressed residual identity) and
+    `tidal` (640 M everywhere-wet cells on the compressed mesh)."""
+    import argparse as _ap
+    import torch
+    out = {}
+    t0 = time.perf_counter()
+    e = run_ensemble(args)
+    out["batched"] = {
+        "what": f"{e['members']} uneven members (sides log-uniform 256-4096, active 0.3-0.9, triangular "
+                f"hyetographs, Manning scale 0.7-1.3), {e['t_end_s']:g} simulated s each, one persistent "
+                f"launch per step in CUDA graphs vs a loop of the plain compressed solver over the same members",
+        "value": e["value"], "unit": UNIT, "plain_loop_value": e["plain_loop_value"],
+        "ratio": e["speedup_vs_plain_loop"], "target": ">= 3x", "target_met": e["speedup_vs_plain_loop"] >= 3.0,
+        "ms_batched": e["ms_batched"], "ms_plain_loop": e["ms_plain_loop"],
+        "active_cells": e["active_total"], "steps_per_member": e["steps_per_member"],
+        "identical_steps_to_plain": e["identical_steps_to_plain"], "gpu_launches": e["gpu_launches"],
+        "clocks_batched": e["clocks_batched"], "clocks_plain_loop": e["clocks_plain_loop"],
+        "schedule": e["schedule"], "seconds": time.perf_counter() - t0}
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    a = run_adjoint(args, caps=(8,))
+    out["adjoint"] = {
+        "what": a["config"]["workload"], "ratio": a["value"], "unit": "reverse step / forward step",
+        "target": "<= 4x", "target_met": a["value"] <= 4.0,
+        "forward_ms_per_step": a["forward_ms_per_step"], "reverse_ms_per_step": a["reverse_ms_per_step"],
+        "recompute_steps": a["recompute_steps"], "recompute_ms": a["recompute_ms"],
+        "total_gradient_cost_in_forward_passes": a["total_gradient_cost_in_forward_passes"],
+        "max_live_snapshots": a["max_live_snapshots"], "clocks_forward": a["clocks_forward"],
+        "clocks_sweep": a["clocks_sweep"], "seconds": time.perf_counter() - t0}
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    c = run_compressed(_ap.Namespace(**{**vars(args), "steps": max(args.steps, 200)}))
+    out["compressed"] = {k: c[k] for k in ("value", "unit", "steps", "ms_per_step", "config",
+                                           "residual_bit_identical_to_dense", "residual_nonzero_fraction",
+                                           "roofline", "clocks", "gpu_launches", "launch_shape")}
+    out["compressed"]["seconds"] = time.perf_counter() - t0
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    t = run_tidal(_ap.Namespace(**{**vars(args), "steps": max(args.steps, 200)}))
+    out["tidal"] = {k: t[k] for k in ("value", "unit", "steps", "ms_per_step", "config", "roofline", "issue",
+                                      "clocks", "gpu_launches", "launch_shape", "build_s")}
+    out["tidal"]["seconds"] = time.perf_counter() - t0
+    torch.cuda.empty_cache()
     return out
 
 
@@ -328,26 +459,35 @@ def time_step_kernel(s, reps=20):
 def run_e2e(args, z, cls, n, world=1):
     """Public API from host buffers: construct (H2D of state, bed, classes), run the
     timed steps, read the depth back (D2H), all inside the timed region; with several
-    ranks, the whole job's cell-updates over the slowest rank's time."""
+    ranks, the whole job's cell-updates over the slowest rank's time. The host arrays
+    sit in page-locked memory, as a pipeline feeding the solver holds them (allocated
+    and filled before the timed region). One untimed call of the same path comes first,
+    as the warm-up steps do for the device-resident measurement."""
     import torch
+    q0 = torch.zeros((3, n, n), dtype=torch.float32).pin_memory().numpy()
+    zb = torch.from_numpy(np.ascontiguousarray(z, dtype=np.float32)).pin_memory().numpy()
+    clsp = torch.from_numpy(np.ascontiguousarray(np.pad(cls, 2, mode="edge"))).pin_memory().numpy()
+    hout = torch.empty((n, n), dtype=torch.float32).pin_memory().numpy()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    t0 = time.perf_counter()
-    s = make_solver(z, cls, n)
-    s.run(t_end=1e12, max_steps=args.steps)
-    h = s.depth()
-    e1.record()
-    torch.cuda.synchronize()
+    for timed in (False, True):
+        torch.cuda.synchronize()
+        e0.record()
+        s = make_solver(zb, None, n, q0=q0, clsp=clsp)
+        s.run(t_end=1e12, max_steps=args.steps if timed else max(args.warmup, 1))
+        h = s.depth(out=hout)
+        e1.record()
+        torch.cuda.synchronize()
+        del s
     ms = e0.elapsed_time(e1)
-    h2d = 3 * n * n * 4 + (n + 4) * (n + 4) * 4 + (n + 4) * (n + 4)
+    h2d = q0.nbytes + zb.nbytes + clsp.nbytes
     d2h = h.nbytes
-    del s
     if world > 1:
         ms = max_over_ranks(ms, "cuda")
     return {"value": n * n * args.steps * world / (ms / 1e3), "unit": UNIT,
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-            "what": "Solver2D(host arrays) + run(steps) + depth(); bytes per step = total / steps"}
+            "ms": ms, "copies_declared": True,
+            "what": "Solver2D(page-locked host arrays: state, bed, padded classes) + run(steps) + "
+                    "depth(out=page-locked); bytes per step = total / steps"}
 
 
 def build_member(spec, brick_h=16, device="cuda", arith="exact"):
@@ -379,7 +519,10 @@ def build_member(spec, brick_h=16, device="cuda", arith="exact"):
 def run_ensemble(args):
     """Batched ensemble vs looping the plain compressed solver over the same members, for
     the same simulated window; cell-updates/s = sum over members of active cells x steps.
-    Both timed regions include their own CUDA-graph captures."""
+    The members are built once: the ensemble copies their initial states into its own
+    storage, the plain loop then runs the members themselves. Both timed regions include
+    their own CUDA-graph captures, each with its own tuned launch shape, and each has
+    its clock record."""
     import torch
     from geoswe_b200 import autotune
     from geoswe_b200.ensemble import Ensemble
@@ -394,37 +537,43 @@ def run_ensemble(args):
         t_end=t_end, max_steps=max(args.warmup, 3), window=8)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    loop_members = [build_member(sp, arith=args.arith) for sp in specs]
+    members = [build_member(sp, arith=args.arith) for sp in specs]
+    ens = Ensemble(members, warps=args.ens_warps, grid=args.ens_grid)      # copies the initial states
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
     loop_shape = None
     if not args.no_tune:                     # the plain solver gets its own tuned launch shape
-        big = max(loop_members, key=lambda m: m.nslots)
+        big = max(members, key=lambda m: m.nslots)
         best, _ = autotune.tune_flat(big, store=False)
-        for m in loop_members:       # warps per brick stay automatic: they follow each member's size
+        for m in members:       # warps per brick stay automatic: they follow each member's size
             m.warps, m.min_blocks = best["warps"], best["min_blocks"]
         loop_shape = best
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = Clocks(0)
+    clk.start()
     e0.record()
-    steps_loop = [m.run(t_end=t_end) for m in loop_members]
+    steps_loop = [m.run(t_end=t_end) for m in members]
     e1.record()
     torch.cuda.synchronize()
+    clocks_loop = clk.stop()
     ms_loop = e0.elapsed_time(e1)
-    loop_launches = int(sum(m.kernel_launches for m in loop_members))
-    work = sum(m.N_active * n for m, n in zip(loop_members, steps_loop))
-    del loop_members
-    torch.cuda.empty_cache()
-    ens = Ensemble([build_member(sp, arith=args.arith) for sp in specs], warps=args.ens_warps, grid=args.ens_grid)
+    loop_launches = int(sum(m.kernel_launches for m in members))
+    work = sum(m.N_active * n for m, n in zip(members, steps_loop))
+    for m in members:                        # the ensemble starts the members at t = 0 again
+        m.t, m.nsteps = 0.0, 0
     tune = None
     if not args.no_tune and args.ens_warps == 0 and args.ens_grid == 0:
         best, table = autotune.tune_ensemble(ens, t_end)
         tune = {"best": best, "table": table}
     n0 = ens.kernel_launches
     torch.cuda.synchronize()
+    clk = Clocks(0)
+    clk.start()
     e0.record()
     steps_ens = ens.run(t_end=t_end, window=args.ens_window)
     e1.record()
     torch.cuda.synchronize()
+    clocks_ens = clk.stop()
     ms_ens = e0.elapsed_time(e1)
     out = {"metric": METRIC + " [batched ensemble]", "value": work / (ms_ens / 1e3), "unit": UNIT,
            "n_gpus": 1, "members": len(specs), "cells_total": int(sum(sp["nx"] * sp["ny"] for sp in specs)),
@@ -435,6 +584,7 @@ def run_ensemble(args):
            "plain_loop_value": work / (ms_loop / 1e3), "speedup_vs_plain_loop": ms_loop / ms_ens,
            "identical_steps_to_plain": bool(steps_ens == steps_loop),
            "gpu_launches": int(ens.kernel_launches - n0), "gpu_launches_plain_loop": loop_launches,
+           "clocks_batched": clocks_ens, "clocks_plain_loop": clocks_loop,
            "schedule": {"warps": ens.warps or 4, "grid": ens.grid, "min_blocks": ens.min_blocks,
                         "segments": ens.segments or 1,
                         "brick_h": ens.brick_h}, "autotune": tune, "plain_loop_shape": loop_shape,
@@ -442,13 +592,14 @@ def run_ensemble(args):
     return out
 
 
-def run_adjoint(args):
+def run_adjoint(args, caps=(0, 6, 8)):
     """Calibration gradients on the compressed mesh (fp32): a 2048 x 2048 fractal terrain
     with ~70 % active cells, 4 Manning classes, rain 40 mm/h x scale, a point inlet with a
     16-knot hydrograph (20 m^3/s peak), 32 gauges, loss over the last 1000 of 3000 steps
     against a run with n x 1.2 and rain x 0.9, 55 snapshots of binomial checkpointing.
     The reported value is the cost of one reverse step over one forward step (both as
-    the driver runs them, device time); recomputation is reported beside it."""
+    the driver runs them, device time); recomputation is reported beside it. `caps`:
+    the reverse kernels' register caps timed on the full sweep (the fastest is kept)."""
     import torch
     from geoswe_b200.adjoint import FlatAdjoint
     from geoswe_b200.synthetic import calibration_case
@@ -480,10 +631,13 @@ def run_adjoint(args):
     prob.forward(snapshots=False)                     # records the base dt schedule
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    clk = Clocks(0)
+    clk.start()
     e0.record()
     prob.forward(replay=True, snapshots=False)
     e1.record()
     torch.cuda.synchronize()
+    clocks_fwd = clk.stop()
     fwd_ms = e0.elapsed_time(e1)
     e0.record()
     prob.forward()                                     # recording pass that keeps snapshots
@@ -493,20 +647,22 @@ def run_adjoint(args):
     loss = prob.loss(target)
     # the reverse kernels' register cap, tried on the full sweep (the gradients must not change)
     sweeps = {}
-    for i, mb in enumerate((0, 6, 8)):
+    for i, mb in enumerate(caps):
         prob.adj_min_blocks = mb
         if i:
             prob.forward()                             # the sweep uses up the snapshots
             torch.cuda.synchronize()
         l0 = prob.kernel_launches
+        clk = Clocks(0)
+        clk.start()
         e0.record()
         g = prob.gradients(target, timing=True)
         e1.record()
         torch.cuda.synchronize()
         tm = dict(prob.timing)
         sweeps[mb] = dict(grad_ms=e0.elapsed_time(e1), tm=tm, g=g, launches=int(prob.kernel_launches - l0),
-                          rev_step=tm["reverse_ms"] / max(tm["reverse_steps"], 1))
-    ref_g = sweeps[0]["g"]
+                          rev_step=tm["reverse_ms"] / max(tm["reverse_steps"], 1), clocks=clk.stop())
+    ref_g = sweeps[caps[0]]["g"]
     for mb, sw in sweeps.items():       # equal up to the order of the per-class atomic sums
         assert torch.allclose(sw["g"][0], ref_g[0], rtol=1e-6, atol=0) and abs(sw["g"][1] - ref_g[1]) <= \
             1e-6 * abs(ref_g[1]) and torch.allclose(sw["g"][2], ref_g[2], rtol=1e-6, atol=1e-12), mb
@@ -531,6 +687,7 @@ def run_adjoint(args):
             "max_live_snapshots": prob.max_snapshots, "gpu_launches_sweep": best["launches"],
             "reverse_register_cap": {"chosen": best_mb, "reverse_ms_per_step": {str(k): v["rev_step"]
                                                                                 for k, v in sweeps.items()}},
+            "clocks_forward": clocks_fwd, "clocks_sweep": best["clocks"],
             "loss": loss, "grad_n": [float(x) for x in gn.cpu()], "grad_rain_scale": gs,
             "grad_knots": [float(x) for x in gk], "knot_times_s": [float(x) for x in kt],
             "knot_values": [float(x) for x in k0], "simulated_s": prob.t_end, "build_s": build_s}
@@ -635,10 +792,13 @@ def run_compressed(args):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = cs.kernel_launches
+    clk = Clocks(0)
+    clk.start()
     e0.record()
     steps = cs.run(t_end=1e12, max_steps=args.steps)
     e1.record()
     torch.cuda.synchronize()
+    clocks = clk.stop()
     ms = e0.elapsed_time(e1)
     torch.cuda.nvtx.range_push("kernel_timing")        # the launches an ncu capture targets
     kern_ms = autotune.time_flat_step(cs, reps=args.kernel_reps)
@@ -646,7 +806,7 @@ def run_compressed(args):
     cells = int(cs.N_active)
     peak, peak_kind = _peaks()
     achieved = 38.0 * cells / (kern_ms / 1e3) / 1e9
-    return {"metric": METRIC + " [compressed rain-on-terrain]", "value": cells * steps / (ms / 1e3), "unit": UNIT,
+    return {"metric": METRIC + " [compressed rain-on-terrain]", "clocks": clocks, "value": cells * steps / (ms / 1e3), "unit": UNIT,
             "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
             "higher_is_better": True, "dtype": "f32", "arith": args.arith, "data": "synthetic",
             "config": {"workload": f"rain-on-terrain {n}x{n} on the compressed mesh, active z < p60 dilated 8 "
@@ -655,8 +815,8 @@ def run_compressed(args):
             "residual_bit_identical_to_dense": identical, "residual_nonzero_fraction": wet,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "kernel_ms": kern_ms, "bytes_per_cell": 38,
-                         "traffic": DRAM_BYTES_PER_CELL["flat_compressed"] * cells / 1e9,
-                         "traffic_unit": "GB per launch (ncu, 4096x4096 capture scaled by active cells)",
+                         "traffic": _traffic("flat_compressed", cells)[0],
+                         "traffic_from": _traffic("flat_compressed", cells)[1],
                          "peak_source": peak_kind},
             "issue": issue_roofline("flat_compressed", cells, kern_ms, None),
             "gpu_launches": int(cs.kernel_launches - l0),
@@ -745,8 +905,8 @@ def run_tidal(args):
                        "active_cells": cells, "stored_slots": int(cs.nslots), "bricks": int(cs.n_bricks),
                        "l2": "inputs larger than L2 (no flush)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": DRAM_BYTES_PER_CELL["flat"] * cells / 1e9,
-                         "traffic_unit": "GB per launch (ncu, 4096x4096 capture scaled by cells)",
+                         "frac": achieved / peak, "traffic": _traffic("flat_tidal", cells)[0],
+                         "traffic_from": _traffic("flat_tidal", cells)[1],
                          "kernel": "flat_march_kernel<float,1>",
                          "kernel_ms": kern_ms, "bytes_per_cell": 38, "peak_source": peak_kind,
                          "brick_bytes_GBs": stored_bytes / (kern_ms / 1e3) / 1e9},
@@ -824,7 +984,12 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fast", action="store_true", help="skip the fast-arithmetic measurement")
-    ap.add_argument("--arith", default="exact", choices=["exact", "fast"],
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched / adjoint / compressed / tidal objects of the default line")
+    ap.add_argument("--dense-arith", default="exact", choices=["exact", "portable"],
+                    help="arithmetic of the headline dense measurement (portable: Manning power by the "
+                         "Newton iteration instead of powf)")
+    ap.add_argument("--arith", default="exact", choices=["exact", "fast", "portable"],
                     help="step arithmetic of the tidal and ensemble cases")
     ap.add_argument("--exact-shape", default="", help="dense launch shape 'tile_rows,warps,min_blocks' (no tuning)")
     ap.add_argument("--fast-shape", default="", help="the same for the fast arithmetic")

@@ -40,6 +40,17 @@ def headers():
     return sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + sorted(INCLUDE.glob("*.h"))
 
 
+def source_hash() -> str:
+    """First 16 hex digits of the SHA-256 over the library's sources and headers (path
+    and content, in name order): names the build a profile was captured on."""
+    import hashlib
+    h = hashlib.sha256()
+    for p in sorted(sources() + headers(), key=lambda q: q.name):
+        h.update(p.name.encode())
+        h.update(p.read_bytes())
+    return h.hexdigest()[:16]
+
+
 def _nvcc():
     for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
         if cand and (os.path.sep not in cand or os.path.exists(cand)):
