@@ -96,7 +96,11 @@ template <> __device__ __forceinline__ double dt_of<double>(const GswLoopState* 
 
 // STEP = false: residual into o0..o2. STEP = true: updated state into o0..o2.
 // REFPOW: Manning's h^(-4/3) by powf (GSW_ARITH_EXACT) instead of pow_m43.
-template <typename T, bool STEP, int MINB, bool REFPOW>
+// LEAN: the kernel of the production configuration (no inside mask, no CFL skip mask,
+// the wave speed reduced, a Manning class table, quadratic friction, keep-h; rain none
+// or uniform), with those choices compiled in rather than tested per cell: 6 % of the
+// 8192^2 step. Any other configuration takes the general kernel; both give the same bits.
+template <typename T, bool STEP, int MINB, bool REFPOW, bool LEAN>
 __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
     if (STEP && p.st->done) return;                       // grid-uniform
     const int lane = threadIdx.x;
@@ -164,15 +168,23 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
 
             Face<T> Ef;
             srm_face<T, true>(cur, nx, p.half_dx, p.inv_dx, p.g, p.h_min, Ef, p.g_recip);
+            // the residual in the reference's order (E, W, N, S per component; accumulate() in
+            // gsw_core.cuh), the E and W parts before the y-face so that W is released early
+            T rh = (T)0, rhu = (T)0, rhv = (T)0;
+            if (Ef.wet) { rh = rh - Ef.Fh; rhu = rhu - Ef.Fn; rhv = rhv - Ef.Ft; rhu = rhu - Ef.srcL; }
+            if (Wf.wet) { rh = rh + Wf.Fh; rhu = rhu + Wf.Fn; rhv = rhv + Wf.Ft; rhu = rhu + Wf.srcR; }
+            Wf = Ef;
             const Cell<T> rn = shfl_cell_down(cur);
-            Face<T> Nf;
-            srm_face<T, false>(cur, rn, p.half_dy, p.inv_dy, p.g, p.h_min, Nf, p.g_recip);
-            const Face<T> Sf = shfl_face_up(Nf);
+            {
+                Face<T> Nf;
+                srm_face<T, false>(cur, rn, p.half_dy, p.inv_dy, p.g, p.h_min, Nf, p.g_recip);
+                const Face<T> Sf = shfl_face_up(Nf);
+                if (Nf.wet) { rh = rh - Nf.Fh; rhu = rhu - Nf.Ft; rhv = rhv - Nf.Fn; rhv = rhv - Nf.srcL; }
+                if (Sf.wet) { rh = rh + Sf.Fh; rhu = rhu + Sf.Ft; rhv = rhv + Sf.Fn; rhv = rhv + Sf.srcR; }
+            }
 
             if (out_lane) {
-                T rh, rhu, rhv;
-                accumulate(Ef, Wf, Nf, Sf, rh, rhu, rhv);
-                const bool inside = (p.mask == nullptr) || (p.mask[(int64_t)r * p.mpitch + c] != 0);
+                const bool inside = LEAN || (p.mask == nullptr) || (p.mask[(int64_t)r * p.mpitch + c] != 0);
                 if (!inside) { rh = (T)0; rhu = (T)0; rhv = (T)0; }
                 const int64_t o = (int64_t)r * p.pitch + c;
                 if (!STEP) {
@@ -181,22 +193,23 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
                     T rr0 = rh;
                     if (inside) {
                         if (p.rain_kind == GSW_RAIN_UNIFORM) rr0 = rh + rate;
-                        else if (p.rain_kind == GSW_RAIN_GRIDDED)
+                        else if (!LEAN && p.rain_kind == GSW_RAIN_GRIDDED)
                             rr0 = rh + frame[(int64_t)(r - p.ngh) * (p.nyp - 2 * p.ngh) + (c - p.ngh)];
                     }
                     T h = cur.h + dt * rr0;
-                    T hu = cur.hu + dt * rhu;
-                    T hv = cur.hv + dt * rhv;
+                    T hu = ldg_at(p.q1, p.pitch, r, c) + dt * rhu;     // reloaded: not carried down the march
+                    T hv = ldg_at(p.q2, p.pitch, r, c) + dt * rhv;
                     T n = (T)0;
-                    if (p.friction_kind == GSW_FRICTION_TABLE)
+                    if (LEAN) n = p.ntab[p.ncls[(int64_t)r * p.cpitch + c]];
+                    else if (p.friction_kind == GSW_FRICTION_TABLE)
                         n = p.ncls ? p.ntab[p.ncls[(int64_t)r * p.cpitch + c]] : p.ntab[0];
                     else if (p.friction_kind == GSW_FRICTION_FIELD) n = p.nfield[o];
-                    wetdry_friction<T>(h, hu, hv, p.friction_kind != GSW_FRICTION_NONE, n, dt, p.g,
-                                       p.h_min, p.vcap, p.quad != 0, p.keep_h != 0, REFPOW);
+                    wetdry_friction<T>(h, hu, hv, LEAN || p.friction_kind != GSW_FRICTION_NONE, n, dt, p.g,
+                                       p.h_min, p.vcap, LEAN || p.quad != 0, LEAN || p.keep_h != 0, REFPOW);
                     p.o0[o] = h; p.o1[o] = hu; p.o2[o] = hv;
                     if (p.max_h != nullptr && h > p.max_h[o]) p.max_h[o] = h;
-                    if (p.lam != nullptr) {
-                        const bool skip = (p.cfl_skip != nullptr) &&
+                    if (LEAN || p.lam != nullptr) {
+                        const bool skip = !LEAN && (p.cfl_skip != nullptr) &&
                             p.cfl_skip[(int64_t)(r - p.ngh) * (p.nyp - 2 * p.ngh) + (c - p.ngh)] != 0;
                         if (!skip) {
                             const unsigned long long lb = lam_dense_bits(h, hu, hv, p.g, p.h_cfl);
@@ -205,12 +218,11 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
                     }
                 }
             }
-            Wf = Ef;
             cur = nx;
             b_next = b_p2;
         }
     }
-    if (STEP && p.lam != nullptr) block_max_to(lam_local, p.lam);
+    if (STEP && (LEAN || p.lam != nullptr)) block_max_to(lam_local, p.lam);
 }
 
 template <typename T>
@@ -275,14 +287,28 @@ inline int fill_dense(const GswDenseArgs* a, DenseK<T>& k, bool step) {
     return GSW_OK;
 }
 
-template <typename T, bool STEP, bool REFPOW>
-inline void launch_march_shape(const DenseK<T>& k, int minb, dim3 grid, dim3 block, cudaStream_t s) {
+template <typename T, bool STEP, bool REFPOW, bool LEAN>
+inline void launch_march_caps(const DenseK<T>& k, int minb, dim3 grid, dim3 block, cudaStream_t s) {
     // register caps apply to the binary32 step; the residual and binary64 use the compiler's choice
     constexpr bool capped = STEP && sizeof(T) == 4;
-    if (capped && minb == 3) dense_march_kernel<T, STEP, capped ? 3 : 1, REFPOW><<<grid, block, 0, s>>>(k);
-    else if (capped && minb == 4) dense_march_kernel<T, STEP, capped ? 4 : 1, REFPOW><<<grid, block, 0, s>>>(k);
-    else if (capped && minb == 5) dense_march_kernel<T, STEP, capped ? 5 : 1, REFPOW><<<grid, block, 0, s>>>(k);
-    else dense_march_kernel<T, STEP, 1, REFPOW><<<grid, block, 0, s>>>(k);
+    if (capped && minb == 3) dense_march_kernel<T, STEP, capped ? 3 : 1, REFPOW, LEAN><<<grid, block, 0, s>>>(k);
+    else if (capped && minb == 4) dense_march_kernel<T, STEP, capped ? 4 : 1, REFPOW, LEAN><<<grid, block, 0, s>>>(k);
+    else if (capped && minb == 5) dense_march_kernel<T, STEP, capped ? 5 : 1, REFPOW, LEAN><<<grid, block, 0, s>>>(k);
+    else dense_march_kernel<T, STEP, 1, REFPOW, LEAN><<<grid, block, 0, s>>>(k);
+}
+
+// The production configuration (the LEAN kernel) or the general kernel.
+template <typename T>
+inline bool lean_config(const DenseK<T>& k) {
+    return k.mask == nullptr && k.cfl_skip == nullptr && k.lam != nullptr && k.friction_kind == GSW_FRICTION_TABLE &&
+           k.ncls != nullptr && k.rain_kind != GSW_RAIN_GRIDDED && k.quad != 0 && k.keep_h != 0;
+}
+
+template <typename T, bool STEP, bool REFPOW>
+inline void launch_march_shape(const DenseK<T>& k, int minb, dim3 grid, dim3 block, cudaStream_t s) {
+    constexpr bool can_lean = STEP && sizeof(T) == 4;
+    if (can_lean && lean_config(k)) launch_march_caps<T, STEP, REFPOW, can_lean>(k, minb, grid, block, s);
+    else launch_march_caps<T, STEP, REFPOW, false>(k, minb, grid, block, s);
 }
 
 template <typename T, bool STEP>

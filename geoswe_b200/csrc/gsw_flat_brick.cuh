@@ -110,8 +110,10 @@ __device__ __forceinline__ Face<T> shfl_up_face(const Face<T>& f) {
 // the same inputs as the face below row r0-1, so splitting a brick's rows among warps
 // changes no value. STEP: the fused step (returns this lane's wave speed bits);
 // otherwise the residual. `frame` is the gridded rain frame, or null. REFPOW: Manning's
-// h^(-4/3) by powf (GSW_ARITH_EXACT) instead of pow_m43.
-template <typename T, bool STEP, bool REFPOW>
+// h^(-4/3) by powf (GSW_ARITH_EXACT) instead of pow_m43. LEAN: the production
+// configuration compiled in (rain none or uniform, a class per slot, quadratic friction,
+// keep-h, the L2 wave-speed norm); the same bits as the general path.
+template <typename T, bool STEP, bool REFPOW, bool LEAN = false>
 __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, const FlatPhys<T>& ph, int64_t bidx,
                                                          int r0, int r1, T dt, T rate, const T* frame) {
     const int lane = threadIdx.x;
@@ -157,48 +159,54 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
         nx.gy = grad_y_flat<T>(m, ph, v, nx.b, r + 1, lane);
         Face<T> Ef;
         srm_face<T, true>(cur, nx, ph.half_dx, ph.inv_dx, ph.g, ph.h_min, Ef, ph.g_recip);
+        // the residual in the reference's order (E, W, N, S per component; accumulate() in
+        // gsw_core.cuh), the E and W parts before the y-face so that W is released early
+        T rh = (T)0, rhu = (T)0, rhv = (T)0;
+        if (Ef.wet) { rh = rh - Ef.Fh; rhu = rhu - Ef.Fn; rhv = rhv - Ef.Ft; rhu = rhu - Ef.srcL; }
+        if (Wf.wet) { rh = rh + Wf.Fh; rhu = rhu + Wf.Fn; rhv = rhv + Wf.Ft; rhu = rhu + Wf.srcR; }
+        Wf = Ef;
         const Cell<T> rn = shfl_down_cell<T>(cur);
-        Face<T> Nf;
-        srm_face<T, false>(cur, rn, ph.half_dy, ph.inv_dy, ph.g, ph.h_min, Nf, ph.g_recip);
-        const Face<T> Sf = shfl_up_face<T>(Nf);
+        {
+            Face<T> Nf;
+            srm_face<T, false>(cur, rn, ph.half_dy, ph.inv_dy, ph.g, ph.h_min, Nf, ph.g_recip);
+            const Face<T> Sf = shfl_up_face<T>(Nf);
+            if (Nf.wet) { rh = rh - Nf.Fh; rhu = rhu - Nf.Ft; rhv = rhv - Nf.Fn; rhv = rhv - Nf.srcL; }
+            if (Sf.wet) { rh = rh + Sf.Fh; rhu = rhu + Sf.Ft; rhv = rhv + Sf.Fn; rhv = rhv + Sf.srcR; }
+        }
         if (lane >= 1 && lane <= 30) {
             const int64_t o = bidx * v.BS + (int64_t)r * GSW_BRICK_PITCH + (lane - 1);
             const uint8_t f = m.flags[o];
             if (f & GSW_SLOT_STORED) {
                 const bool active = (f & GSW_SLOT_ACTIVE) != 0;
                 if (!STEP) {
-                    T rh = (T)0, rhu = (T)0, rhv = (T)0;
-                    if (active) accumulate(Ef, Wf, Nf, Sf, rh, rhu, rhv);
+                    if (!active) { rh = (T)0; rhu = (T)0; rhv = (T)0; }
                     m.o0[o] = rh; m.o1[o] = rhu; m.o2[o] = rhv;
                 } else if (!active) {
-                    m.o0[o] = cur.h; m.o1[o] = cur.hu; m.o2[o] = cur.hv;
+                    m.o0[o] = cur.h; m.o1[o] = __ldg(m.q1 + o); m.o2[o] = __ldg(m.q2 + o);
                     if (m.max_h != nullptr && cur.h > m.max_h[o]) m.max_h[o] = cur.h;
                 } else {
-                    T rh, rhu, rhv;
-                    accumulate(Ef, Wf, Nf, Sf, rh, rhu, rhv);
                     T rr0 = rh;
                     if (ph.rain_kind == GSW_RAIN_UNIFORM) rr0 = rr0 + rate;
-                    else if (ph.rain_kind == GSW_RAIN_GRIDDED) {
+                    else if (!LEAN && ph.rain_kind == GSW_RAIN_GRIDDED) {
                         const int i = bi * bh + r, j = bj * GSW_BRICK_W + (lane - 1);
                         rr0 = rr0 + frame[(int64_t)(i - ph.ngh) * ph.ny + (j - ph.ngh)];
-                    } else if (ph.rain_kind == GSW_RAIN_LOOKUP) {
+                    } else if (!LEAN && ph.rain_kind == GSW_RAIN_LOOKUP) {
                         rr0 = rr0 + frame[ph.lookup[o]];
                     }
                     T h = cur.h + dt * rr0;
-                    T hu = cur.hu + dt * rhu;
-                    T hv = cur.hv + dt * rhv;
-                    const T n = m.ncls ? ph.ntab[m.ncls[o]] : ph.ntab[0];
+                    T hu = __ldg(m.q1 + o) + dt * rhu;       // reloaded: not carried down the march
+                    T hv = __ldg(m.q2 + o) + dt * rhv;
+                    const T n = (LEAN || m.ncls) ? ph.ntab[m.ncls[o]] : ph.ntab[0];
                     wetdry_friction<T>(h, hu, hv, true, n, dt, ph.g, ph.h_min, ph.vcap,
-                                           ph.quad != 0, ph.keep_h != 0, REFPOW);
+                                       LEAN || ph.quad != 0, LEAN || ph.keep_h != 0, REFPOW);
                     m.o0[o] = h; m.o1[o] = hu; m.o2[o] = hv;
                     if (m.max_h != nullptr && h > m.max_h[o]) m.max_h[o] = h;
                     const unsigned long long lb = lam_flat_bits(h, hu, hv, ph.g, ph.h_min, ph.h_min_cfl,
-                                                                ph.linf != 0);
+                                                                !LEAN && ph.linf != 0);
                     lam_local = lb > lam_local ? lb : lam_local;
                 }
             }
         }
-        Wf = Ef;
         cur = nx;
         b_next = b_p2;
     }

@@ -14,7 +14,7 @@
 
 namespace gsw {
 
-template <typename T, bool STEP, int MINB, bool REFPOW>
+template <typename T, bool STEP, int MINB, bool REFPOW, bool LEAN>
 __global__ void __launch_bounds__(256, MINB) flat_march_kernel(FlatK<T> p) {
     if (STEP && p.st->done) return;
     const int64_t item = (int64_t)blockIdx.x * blockDim.y + threadIdx.y;   // (brick, row segment)
@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(256, MINB) flat_march_kernel(FlatK<T> p) {
         if (p.ph.rain_kind == GSW_RAIN_LOOKUP) frame = p.ph.rain + (int64_t)p.st->rain_idx * p.ph.ncol;
     }
     if (bidx < p.m.nb)
-        lam_local = flat_brick<T, STEP, REFPOW>(p.m, p.ph, bidx, seg * p.m.bh / p.segs, (seg + 1) * p.m.bh / p.segs,
+        lam_local = flat_brick<T, STEP, REFPOW, LEAN>(p.m, p.ph, bidx, seg * p.m.bh / p.segs, (seg + 1) * p.m.bh / p.segs,
                                         dt, rate, frame);
     if (STEP && p.lam != nullptr) block_max_to(lam_local, p.lam);
 }
@@ -72,13 +72,24 @@ inline int fill_flat(const GswFlatArgs* a, FlatK<T>& k, bool step) {
     return GSW_OK;
 }
 
+template <typename T, bool STEP, bool REFPOW, bool LEAN>
+inline void launch_flat_caps(const FlatK<T>& k, int mb, unsigned blocks, int W, cudaStream_t s) {
+    constexpr bool capped = STEP && sizeof(T) == 4;   // register caps apply to the binary32 step
+    if (capped && mb == 3) flat_march_kernel<T, STEP, capped ? 3 : 1, REFPOW, LEAN><<<blocks, dim3(32, W), 0, s>>>(k);
+    else if (capped && mb == 4) flat_march_kernel<T, STEP, capped ? 4 : 1, REFPOW, LEAN><<<blocks, dim3(32, W), 0, s>>>(k);
+    else if (capped && mb == 5) flat_march_kernel<T, STEP, capped ? 5 : 1, REFPOW, LEAN><<<blocks, dim3(32, W), 0, s>>>(k);
+    else flat_march_kernel<T, STEP, 1, REFPOW, LEAN><<<blocks, dim3(32, W), 0, s>>>(k);
+}
+
+// The production configuration (the LEAN kernel: rain none or uniform, a class per slot,
+// quadratic friction, keep-h, the L2 norm) or the general kernel.
 template <typename T, bool STEP, bool REFPOW>
 inline void launch_flat_shape(const FlatK<T>& k, int mb, unsigned blocks, int W, cudaStream_t s) {
-    constexpr bool capped = STEP && sizeof(T) == 4;   // register caps apply to the binary32 step
-    if (capped && mb == 3) flat_march_kernel<T, STEP, capped ? 3 : 1, REFPOW><<<blocks, dim3(32, W), 0, s>>>(k);
-    else if (capped && mb == 4) flat_march_kernel<T, STEP, capped ? 4 : 1, REFPOW><<<blocks, dim3(32, W), 0, s>>>(k);
-    else if (capped && mb == 5) flat_march_kernel<T, STEP, capped ? 5 : 1, REFPOW><<<blocks, dim3(32, W), 0, s>>>(k);
-    else flat_march_kernel<T, STEP, 1, REFPOW><<<blocks, dim3(32, W), 0, s>>>(k);
+    constexpr bool can_lean = STEP && sizeof(T) == 4;
+    const bool lean = k.ph.rain_kind != GSW_RAIN_GRIDDED && k.ph.rain_kind != GSW_RAIN_LOOKUP && k.m.ncls != nullptr &&
+                      k.ph.quad != 0 && k.ph.keep_h != 0 && k.ph.linf == 0;
+    if (can_lean && lean) launch_flat_caps<T, STEP, REFPOW, can_lean>(k, mb, blocks, W, s);
+    else launch_flat_caps<T, STEP, REFPOW, false>(k, mb, blocks, W, s);
 }
 
 template <typename T, bool STEP>
