@@ -188,16 +188,17 @@ def counters():
     is proportional to the cells, so it scales to a launch of another size) and warp
     instructions per updated cell (smsp__inst_executed.sum / cells; with the SM clock,
     the instruction-issue roofline: one warp instruction per scheduler per cycle, four
-    schedulers per SM). Each entry names the library sources it was captured on;
-    `current_build` says whether that is the library measured here."""
+    schedulers per SM). Each entry names the sources its kernel is compiled from and
+    their hash when it was captured; `current_build` says whether those sources are the
+    ones measured here."""
     p = ROOT / "profiles" / "counters.json"
     d = json.loads(p.read_text()) if p.exists() else {}
     try:
         from geoswe_b200.build import source_hash
-        cur = source_hash()
     except Exception:
-        cur = None
+        source_hash = None
     for v in d.values():
+        cur = source_hash(v.get("files")) if source_hash is not None else None
         v["current_build"] = cur is not None and v.get("sources") == cur
     return d
 

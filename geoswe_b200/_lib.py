@@ -11,7 +11,7 @@ from pathlib import Path
 _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / "libgsw.so"
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_ABI, ERR_NONFINITE, ERR_RANGE, ERR_TIMEOUT = -1, -2, -3, -4, -5, -6
@@ -75,7 +75,7 @@ class GswInflowArgs(C.Structure):
     _fields_ = [("abi_version", u32), ("dtype", i32), ("pitch", i64), ("q0", vp), ("q1", vp),
                 ("q2", vp), ("bed", vp), ("inlet_off", vp), ("n", i32), ("ngh", i32),
                 ("step_off", i64), ("nx_n", f64), ("ny_n", f64), ("ds", f64), ("dry_frac", f64),
-                ("t_knots", vp), ("q_knots", vp), ("n_knots", i32), ("state", vp)]
+                ("t_knots", vp), ("q_knots", vp), ("n_knots", i32), ("state", vp), ("hsum", vp)]
 
 
 class GswFlatArgs(C.Structure):
@@ -93,7 +93,7 @@ class GswFlatArgs(C.Structure):
 class GswFlatInflowArgs(C.Structure):
     _fields_ = [("abi_version", u32), ("dtype", i32), ("q0", vp), ("q1", vp), ("q2", vp), ("bed", vp),
                 ("ghost_slot", vp), ("nbr_slot", vp), ("n", i32), ("n_knots", i32), ("nx_n", f64),
-                ("ny_n", f64), ("ds", f64), ("t_knots", vp), ("q_knots", vp), ("state", vp)]
+                ("ny_n", f64), ("ds", f64), ("t_knots", vp), ("q_knots", vp), ("state", vp), ("hsum", vp)]
 
 
 class GswFlatAdjArgs(C.Structure):
@@ -158,6 +158,7 @@ _PROTOS = {
     "gsw_stage_apply": [C.POINTER(GswStageArgs), vp],
     "gsw_lam_cells": [C.POINTER(GswStageArgs), vp],
     "gsw_inflow_apply": [C.POINTER(GswInflowArgs), vp],
+    "gsw_inflow_depth_sum": [C.POINTER(GswInflowArgs), vp, vp],
     "gsw_dt_finalize": [C.POINTER(GswDtParams), vp, vp],
     "gsw_dt_params_upload": [C.POINTER(GswDtParams), vp, vp],
     "gsw_dense_autotune": [C.POINTER(GswDenseArgs), C.c_int32, C.c_int32, C.POINTER(GswTuneResult), vp],
@@ -165,6 +166,7 @@ _PROTOS = {
     "gsw_dt_finalize_dev": [vp, vp, vp],
     "gsw_loop_commit": [vp, vp],
     "gsw_flat_inflow_apply": [C.POINTER(GswFlatInflowArgs), vp],
+    "gsw_flat_inflow_depth_sum": [C.POINTER(GswFlatInflowArgs), vp, vp],
     "gsw_flat_forcings": [C.POINTER(GswFlatForcingArgs), vp],
     "gsw_flat_ring_stage": [C.POINTER(GswFlatRingArgs), vp],
     "gsw_seam_copy": [C.POINTER(GswSeamArgs), vp],

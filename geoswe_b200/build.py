@@ -40,12 +40,16 @@ def headers():
     return sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + sorted(INCLUDE.glob("*.h"))
 
 
-def source_hash() -> str:
-    """First 16 hex digits of the SHA-256 over the library's sources and headers (path
-    and content, in name order): names the build a profile was captured on."""
+def source_hash(names=None) -> str:
+    """First 16 hex digits of the SHA-256 over the library's sources and headers (name
+    and content, in name order), or over the files called `names` only (the sources a
+    kernel is compiled from): names the build a profile was captured on."""
     import hashlib
     h = hashlib.sha256()
-    for p in sorted(sources() + headers(), key=lambda q: q.name):
+    files = sources() + headers()
+    if names is not None:
+        files = [p for p in files if p.name in set(names)]
+    for p in sorted(files, key=lambda q: q.name):
         h.update(p.name.encode())
         h.update(p.read_bytes())
     return h.hexdigest()[:16]

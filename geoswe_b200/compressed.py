@@ -651,7 +651,7 @@ class CompressedSolver:
         a.state = _ptr(self._state)
         return a
 
-    def _inflow_args(self, f, q):
+    def _inflow_args(self, f, q, hsum=None):
         a = L.GswFlatInflowArgs()
         a.abi_version = L.ABI_VERSION
         a.dtype = L.F32
@@ -660,6 +660,7 @@ class CompressedSolver:
         a.nx_n, a.ny_n, a.ds = f["nx"], f["ny"], f["ds"]
         a.t_knots, a.q_knots, a.n_knots = _ptr(f["t"]), _ptr(f["q"]), int(f["t"].numel())
         a.state = _ptr(self._state)
+        a.hsum = hsum
         return a
 
     # ---------------------------------------------------------------- views
@@ -817,9 +818,13 @@ class CompressedSolver:
                           "to set_rain().", stacklevel=2)
         dm = dt_max if dt_max is not None else self.dt_max_user
         split = self.flat_halo is not None
-        if split and (self._inflows or self._ring is not None or self._forcing or every > 0.0):
-            raise NotImplementedError("CompressedSolver.run: a run split over ranks takes rain and friction "
-                                      "only (no inlets, ring stage, flat-loop forcings or checkpoints)")
+        inlet_sums = None
+        if split:
+            # one sum collective per step when there are inlets: every rank must list the
+            # same inlets (compressed_solver.py:2117-2121; entries may hold no local cells)
+            self.halo.check_same(len(self._inflows), "CompressedSolver: discharge inlets")
+            if self._inflows:
+                inlet_sums = torch.zeros(len(self._inflows), dtype=torch.float64, device=self.device)
         K = int(window) if window else self._window_size()
         if split and not window:
             K = min(K, 32)     # launched eagerly: poll often, so few no-op steps follow the end
@@ -840,7 +845,7 @@ class CompressedSolver:
         forced = bool(self._forcing)
         per_step = 2 + len(self._inflows) + (self._ring is not None) + 3 * forced
         if split:
-            per_step += self.flat_halo.launches_per_exchange
+            per_step += self.flat_halo.launches_per_exchange + (len(self._inflows) if inlet_sums is not None else 0)
 
         def one_step(k_parity):
             s = _stream()
@@ -850,8 +855,15 @@ class CompressedSolver:
             src, dst = self._q[k_parity], self._q[1 - k_parity]
             if split:                           # seam ghosts from the neighbours, before the step
                 self.flat_halo.exchange(src)
-            for f in self._inflows:             # inlet ghosts at t_n, before the step
-                L.call("gsw_flat_inflow_apply", C.byref(self._inflow_args(f, src)), s)
+            sums = [None] * len(self._inflows)
+            if inlet_sums is not None:          # an inlet may span ranks: one batched sum of
+                base = inlet_sums.data_ptr()    # every inlet's depth over the ranks (:2145-2153)
+                sums = [C.c_void_p(base + 8 * k) for k in range(len(self._inflows))]
+                for f, p in zip(self._inflows, sums):
+                    L.call("gsw_flat_inflow_depth_sum", C.byref(self._inflow_args(f, src)), p, s)
+                self.halo.allreduce_sum_(inlet_sums)
+            for f, p in zip(self._inflows, sums):   # inlet ghosts at t_n, before the step
+                L.call("gsw_flat_inflow_apply", C.byref(self._inflow_args(f, src, p)), s)
             a = self._args(src, dst)
             if forced:                          # the wave speed is taken after the forcings
                 a.lam_target = None
@@ -928,32 +940,50 @@ class CompressedSolver:
             arrays["max_h"] = self._max_h[self._slot].cpu().numpy()
         if "ga" in self._forcing:                  # Green-Ampt's cumulative infiltration is state
             arrays["F"] = self._forcing["ga"]["F"][self._slot].cpu().numpy()
-        tmp = os.path.join(ckpt_dir, "ckpt_r00_tmp")
+        rank, nranks = self._rank_and_size()
+        tmp = os.path.join(ckpt_dir, f"ckpt_r{rank:02d}_tmp")
         np.savez(tmp, t=np.float64(t), steps=np.int64(steps), **arrays)
-        os.replace(tmp + ".npz", os.path.join(ckpt_dir, "ckpt_r00.npz"))
-        meta = dict(t=float(t), steps=int(steps), fidx=0, next_frame=0.0, nranks=1)
-        mt = os.path.join(ckpt_dir, "ckpt_meta.json.tmp")
-        with open(mt, "w") as f:
-            json.dump(meta, f)
-        os.replace(mt, os.path.join(ckpt_dir, "ckpt_meta.json"))
+        os.replace(tmp + ".npz", os.path.join(ckpt_dir, f"ckpt_r{rank:02d}.npz"))
+        # a split run: every rank's state file is in place before rank 0 publishes the
+        # meta (compressed_solver.py:1861-1866), so the pair on disk is never torn
+        if nranks > 1:
+            self._barrier()
+        if rank == 0:
+            meta = dict(t=float(t), steps=int(steps), fidx=0, next_frame=0.0, nranks=nranks)
+            mt = os.path.join(ckpt_dir, "ckpt_meta.json.tmp")
+            with open(mt, "w") as f:
+                json.dump(meta, f)
+            os.replace(mt, os.path.join(ckpt_dir, "ckpt_meta.json"))
+        if nranks > 1:
+            self._barrier()
+
+    def _rank_and_size(self):
+        if self.flat_halo is None:
+            return 0, 1
+        return int(self.halo.rank), int(self.halo.size)
+
+    def _barrier(self):
+        import torch.distributed as dist
+        dist.barrier(group=self.halo.group)
 
     def load_checkpoint(self, ckpt_dir, missing_ok: bool = False):
         """Restore state, time and step count from a checkpoint in the reference's format
-        (ckpt_meta.json + ckpt_r00.npz). Returns False when there is none and
-        `missing_ok`."""
+        (ckpt_meta.json + ckpt_r##.npz, one state file per rank of a split run; resumed with
+        the same rank count, compressed_solver.py:1881-1895). Returns False when there is
+        none and `missing_ok`."""
         import json
         import os
-        if self.flat_halo is not None:
-            raise NotImplementedError("load_checkpoint: checkpoints of a run split over ranks are not supported")
+        rank, nranks = self._rank_and_size()
         mp = os.path.join(ckpt_dir, "ckpt_meta.json")
         if not os.path.exists(mp):
             if missing_ok:
                 return False
             raise FileNotFoundError(mp)
         meta = json.load(open(mp))
-        if int(meta.get("nranks", 1)) != 1:
-            raise RuntimeError(f"checkpoint nranks={meta['nranks']} != 1; resume with the same rank count")
-        z = np.load(os.path.join(ckpt_dir, "ckpt_r00.npz"))
+        if int(meta.get("nranks", 1)) != nranks:
+            raise RuntimeError(f"checkpoint nranks={meta['nranks']} != current nranks={nranks}; resume with the "
+                               f"same rank count (per-rank states are tied to the partition)")
+        z = np.load(os.path.join(ckpt_dir, f"ckpt_r{rank:02d}.npz"))
         if "t" in z.files and (abs(float(z["t"]) - float(meta["t"])) > 1e-9 or int(z["steps"]) != int(meta["steps"])):
             raise RuntimeError("torn checkpoint: the state file and ckpt_meta.json disagree on (t, steps)")
         for c in range(3):

@@ -75,6 +75,36 @@ __device__ __forceinline__ T div_z(T a, T b) {
     const T q = one_if(zr, a) / b;
     return zr ? a * b : q;
 }
+// Binary32, the whole guard in one asm block: the zero test feeds both selects as a
+// predicate, where the forms above pass it through an integer register (a select and
+// an integer compare more per guard, 14 guards per cell). sqrt.rn and div.rn are the
+// IEEE operations the C operators compile to.
+template <>
+__device__ __forceinline__ float sqrt_z<float>(float x) {
+    float r;
+    asm("{\n\t.reg .pred p;\n\t.reg .f32 t;\n\t"
+        "setp.eq.f32 p, %1, 0f00000000;\n\t"
+        "selp.f32 t, 0f3F800000, %1, p;\n\t"
+        "sqrt.rn.f32 t, t;\n\t"
+        "selp.f32 %0, %1, t, p;\n\t}"
+        : "=f"(r) : "f"(x));
+    return r;
+}
+template <>
+__device__ __forceinline__ float div_z<float>(float a, float b) {
+    float r;
+    asm("{\n\t.reg .pred p;\n\t.reg .f32 t, m;\n\t"
+        "abs.f32 m, %2;\n\t"
+        "setp.eq.f32 p, %1, 0f00000000;\n\t"
+        "setp.lt.and.f32 p, m, 0f7F800000, p;\n\t"
+        "setp.gt.and.f32 p, m, 0f00000000, p;\n\t"
+        "selp.f32 t, 0f3F800000, %1, p;\n\t"
+        "div.rn.f32 t, t, %2;\n\t"
+        "mul.rn.f32 m, %1, %2;\n\t"
+        "selp.f32 %0, m, t, p;\n\t}"
+        : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
 #else
 // Fast arithmetic (gsw_fast.cu, compiled with FMA contraction and flush-to-zero):
 // binary32 square root and division by the hardware approximations, sqrt.approx
@@ -213,34 +243,36 @@ __device__ __forceinline__ void hllc(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
     } else {
         SM = half * (uNL + uNR);
     }
-    const T huNL = hL * uNL, huNR = hR * uNR;
-    const T huTL = hL * uTL, huTR = hR * uTR;
-    const T pL = half * g * hL * hL;
-    const T pR = half * g * hR * hR;
-    const T FL_h = huNL;
-    const T FL_N = huNL * uNL + pL;
-    const T FL_T = huNL * uTL;
-    const T FR_h = huNR;
-    const T FR_N = huNR * uNR + pR;
-    const T FR_T = huNR * uTR;
-    // One star state, on the side of the contact the reference selects (SM >= 0: left),
-    // with the reference's own expressions for that side: a single division and no
-    // divergent branches, and the same values where the reference's select uses them.
+    // The reference returns F_L where SL >= 0, the star flux of the side of the contact
+    // (SM >= 0: left) where SL < 0 <= SR or that side is left, else F_R. Each of these
+    // reads one side's physical flux only: side P is L where SL >= 0, else the star side
+    // K. So the physical flux is evaluated for side P alone, with the reference's
+    // expressions for that side (huN = h uN, F_N = huN uN + 0.5 g h h, F_T = huN uT),
+    // and one star state for side K: one division, no divergent branches, and the same
+    // values wherever the reference's select uses them.
     const bool left = SM >= z;
+    const bool useL = SL >= z;
+    const bool sideL = useL || left;
+    const T hP = sideL ? hL : hR, uNP = sideL ? uNL : uNR, uTP = sideL ? uTL : uTR;
+    const T huNP = hP * uNP;
+    const T huTP = hP * uTP;
+    const T pP = half * g * hP * hP;
+    const T FP_h = huNP;
+    const T FP_N = huNP * uNP + pP;
+    const T FP_T = huNP * uTP;
+    // star state of side K (= P wherever it is used: SL < 0 there)
     const T S = left ? SL : SR;
-    const T hK = left ? hL : hR, uNK = left ? uNL : uNR, uTK = left ? uTL : uTR;
-    const T huNK = left ? huNL : huNR, huTK = left ? huTL : huTR;
-    const T FK_h = left ? FL_h : FR_h, FK_N = left ? FL_N : FR_N, FK_T = left ? FL_T : FR_T;
-    const T fac = gdiv(S - uNK, S - SM + (T)1.0e-30);
-    const T hKs = hK * fac;
+    const T fac = gdiv(S - uNP, S - SM + (T)1.0e-30);
+    const T hKs = hP * fac;
     const T huNKs = hKs * SM;
-    const T huTKs = hKs * uTK;
-    const T Fs_h = FK_h + S * (hKs - hK);
-    const T Fs_N = FK_N + S * (huNKs - huNK);
-    const T Fs_T = FK_T + S * (huTKs - huTK);
-    if (SL >= z)           { Fh = FL_h; FN = FL_N; FT = FL_T; }
-    else if (left || SR >= z) { Fh = Fs_h; FN = Fs_N; FT = Fs_T; }
-    else                   { Fh = FR_h; FN = FR_N; FT = FR_T; }
+    const T huTKs = hKs * uTP;
+    const T Fs_h = FP_h + S * (hKs - hP);
+    const T Fs_N = FP_N + S * (huNKs - huNP);
+    const T Fs_T = FP_T + S * (huTKs - huTP);
+    const bool star = !useL && (left || SR >= z);
+    Fh = star ? Fs_h : FP_h;
+    FN = star ? Fs_N : FP_N;
+    FT = star ? Fs_T : FP_T;
 }
 
 // One face between cell L (lower index) and cell R (upper index) along one axis.

@@ -111,8 +111,8 @@ __device__ __forceinline__ Face<T> shfl_up_face(const Face<T>& f) {
 // changes no value. STEP: the fused step (returns this lane's wave speed bits);
 // otherwise the residual. `frame` is the gridded rain frame, or null. REFPOW: Manning's
 // h^(-4/3) by powf (GSW_ARITH_EXACT) instead of pow_m43. LEAN: the production
-// configuration compiled in (rain none or uniform, a class per slot, quadratic friction,
-// keep-h, the L2 wave-speed norm); the same bits as the general path.
+// configuration compiled in (rain none or uniform, quadratic friction, keep-h, the L2
+// wave-speed norm); the same bits as the general path.
 template <typename T, bool STEP, bool REFPOW, bool LEAN = false>
 __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, const FlatPhys<T>& ph, int64_t bidx,
                                                          int r0, int r1, T dt, T rate, const T* frame) {
@@ -196,7 +196,7 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
                     T h = cur.h + dt * rr0;
                     T hu = __ldg(m.q1 + o) + dt * rhu;       // reloaded: not carried down the march
                     T hv = __ldg(m.q2 + o) + dt * rhv;
-                    const T n = (LEAN || m.ncls) ? ph.ntab[m.ncls[o]] : ph.ntab[0];
+                    const T n = m.ncls ? ph.ntab[m.ncls[o]] : ph.ntab[0];
                     wetdry_friction<T>(h, hu, hv, true, n, dt, ph.g, ph.h_min, ph.vcap,
                                        LEAN || ph.quad != 0, LEAN || ph.keep_h != 0, REFPOW);
                     m.o0[o] = h; m.o1[o] = hu; m.o2[o] = hv;

@@ -81,12 +81,12 @@ inline void launch_flat_caps(const FlatK<T>& k, int mb, unsigned blocks, int W, 
     else flat_march_kernel<T, STEP, 1, REFPOW, LEAN><<<blocks, dim3(32, W), 0, s>>>(k);
 }
 
-// The production configuration (the LEAN kernel: rain none or uniform, a class per slot,
-// quadratic friction, keep-h, the L2 norm) or the general kernel.
+// The production configuration (the LEAN kernel: rain none or uniform, quadratic
+// friction, keep-h, the L2 norm) or the general kernel.
 template <typename T, bool STEP, bool REFPOW>
 inline void launch_flat_shape(const FlatK<T>& k, int mb, unsigned blocks, int W, cudaStream_t s) {
     constexpr bool can_lean = STEP && sizeof(T) == 4;
-    const bool lean = k.ph.rain_kind != GSW_RAIN_GRIDDED && k.ph.rain_kind != GSW_RAIN_LOOKUP && k.m.ncls != nullptr &&
+    const bool lean = k.ph.rain_kind != GSW_RAIN_GRIDDED && k.ph.rain_kind != GSW_RAIN_LOOKUP &&
                       k.ph.quad != 0 && k.ph.keep_h != 0 && k.ph.linf == 0;
     if (can_lean && lean) launch_flat_caps<T, STEP, REFPOW, can_lean>(k, mb, blocks, W, s);
     else launch_flat_caps<T, STEP, REFPOW, false>(k, mb, blocks, W, s);

@@ -19,8 +19,7 @@ __global__ void inflow_kernel(GswInflowArgs a) {
     __shared__ int s_wet, s_nlow, s_flat;
     if (threadIdx.x == 0) {
         s_Q = np_interp(a.state->t, a.t_knots, a.q_knots, a.n_knots);
-        const T sum = pairwise_sum<T>(q0, a.inlet_off, 0, a.n);
-        s_sum = (double)sum;
+        s_sum = a.hsum != nullptr ? *a.hsum : (double)pairwise_sum<T>(q0, a.inlet_off, 0, a.n);
         s_wet = s_sum > 0.0;
         if (!s_wet) {
             T zmin = bed[a.inlet_off[0]], zmax = zmin;
@@ -82,6 +81,19 @@ __global__ void inflow_kernel(GswInflowArgs a) {
     }
 }
 
+// This rank's share of an inlet's depth sum (a split run all-reduces these).
+template <typename T>
+__global__ void inflow_depth_sum_kernel(GswInflowArgs a, double* out) {
+    if (threadIdx.x == 0)
+        *out = a.n > 0 ? (double)pairwise_sum<T>((const T*)a.q0, a.inlet_off, 0, a.n) : 0.0;
+}
+
+template <typename T>
+__global__ void flat_inflow_depth_sum_kernel(GswFlatInflowArgs a, double* out) {
+    if (threadIdx.x == 0)
+        *out = a.n > 0 ? (double)pairwise_sum<T>((const T*)a.q0, a.nbr_slot, 0, a.n) : 0.0;
+}
+
 // Flat-tier inlet (compressed_solver.py:2144-2167, dry seed :1559-1594). One block per
 // inlet; thread 0 evaluates Q, the depth sum and the dry seed, all threads write ghosts.
 template <typename T>
@@ -94,8 +106,7 @@ __global__ void flat_inflow_kernel(GswFlatInflowArgs a) {
     __shared__ int s_wet, s_flat;
     if (threadIdx.x == 0) {
         s_Q = np_interp(a.state->t, a.t_knots, a.q_knots, a.n_knots);
-        const T sum = pairwise_sum<T>(q0, a.nbr_slot, 0, a.n);
-        s_sum = (double)sum;
+        s_sum = a.hsum != nullptr ? *a.hsum : (double)pairwise_sum<T>(q0, a.nbr_slot, 0, a.n);
         s_wet = s_sum > 0.0;
         if (!s_wet) {
             T zmin = bed[a.nbr_slot[0]], zmax = zmin;
@@ -302,6 +313,28 @@ extern "C" int gsw_inflow_apply(const GswInflowArgs* a, void* stream) {
     else if (a->dtype == GSW_F64) inflow_kernel<double><<<1, 256, 0, s>>>(*a);
     else return set_error(GSW_ERR_INVALID, "inflow: bad dtype");
     return check_launch("inflow");
+}
+
+extern "C" int gsw_inflow_depth_sum(const GswInflowArgs* a, double* out, void* stream) {
+    GSW_CHECK_ABI(a);
+    if (!out || !a->q0 || (a->n > 0 && !a->inlet_off) || a->n < 0)
+        return set_error(GSW_ERR_INVALID, "inflow depth sum: null pointer or negative count");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (a->dtype == GSW_F32) inflow_depth_sum_kernel<float><<<1, 32, 0, s>>>(*a, out);
+    else if (a->dtype == GSW_F64) inflow_depth_sum_kernel<double><<<1, 32, 0, s>>>(*a, out);
+    else return set_error(GSW_ERR_INVALID, "inflow depth sum: bad dtype");
+    return check_launch("inflow_depth_sum");
+}
+
+extern "C" int gsw_flat_inflow_depth_sum(const GswFlatInflowArgs* a, double* out, void* stream) {
+    GSW_CHECK_ABI(a);
+    if (!out || !a->q0 || (a->n > 0 && !a->nbr_slot) || a->n < 0)
+        return set_error(GSW_ERR_INVALID, "flat inflow depth sum: null pointer or negative count");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (a->dtype == GSW_F32) flat_inflow_depth_sum_kernel<float><<<1, 32, 0, s>>>(*a, out);
+    else if (a->dtype == GSW_F64) flat_inflow_depth_sum_kernel<double><<<1, 32, 0, s>>>(*a, out);
+    else return set_error(GSW_ERR_INVALID, "flat inflow depth sum: bad dtype");
+    return check_launch("flat_inflow_depth_sum");
 }
 
 extern "C" int gsw_flat_inflow_apply(const GswFlatInflowArgs* a, void* stream) {

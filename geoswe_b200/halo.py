@@ -265,6 +265,28 @@ class Halo2D:
         t.copy_(h)
         return t
 
+    def allreduce_sum_(self, t):
+        """In-place sum over the ranks of a small tensor (the inlets' depth sums, float64,
+        one batched collective for all inlets as the reference's Allreduce)."""
+        if t.device.type == "cpu" or self.device_direct:
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+            return t
+        h = t.cpu()
+        dist.all_reduce(h, op=dist.ReduceOp.SUM, group=self.group)
+        t.copy_(h)
+        return t
+
+    def check_same(self, value: int, what: str):
+        """Raise on every rank unless every rank passes the same integer: a count that
+        decides how many collectives a step posts (the number of discharge inlets)."""
+        dev = self._comm_device()
+        t = torch.tensor([int(value), -int(value)], dtype=torch.int64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.group)
+        hi, lo = int(t[0]), -int(t[1])
+        if hi != lo:
+            raise RuntimeError(f"{what} differ across ranks (between {lo} and {hi}): pass the same list on "
+                               f"every rank (entries may hold no local cells)")
+
 
 class FlatHalo:
     """Seam exchange of the compressed mesh, the reference's ``CompressedHalo``

@@ -351,10 +351,6 @@ class Solver2D:
     def add_inflow(self, idx_i, idx_j, normal, ds, t_series, q_series, dry_frac=0.10):
         """One discharge inlet on padded cells (idx_i, idx_j) along a physical edge;
         ``normal`` is the inward unit normal (axis-aligned)."""
-        if self.halo is not None:
-            raise NotImplementedError("add_inflow: discharge inlets are not supported on a run split "
-                                      "over several ranks (the inlet's depth sum would need a sum over "
-                                      "the ranks every step); run the inlet's domain on one rank")
         ii = np.asarray(idx_i, dtype=np.int64).ravel()
         jj = np.asarray(idx_j, dtype=np.int64).ravel()
         if ii.shape != jj.shape:
@@ -474,6 +470,13 @@ class Solver2D:
                                   step=-(f["si"] * self.pitch + f["sj"]),
                                   t=torch.from_numpy(f["t"].copy()).to(dev),
                                   q=torch.from_numpy(f["q"].copy()).to(dev), nk=int(len(f["t"])), f=f))
+        T.inlet_sums = None
+        if self.halo is not None:
+            # every rank posts one sum collective per step when there are inlets: the
+            # counts must agree (a rank holding none of an inlet's cells lists it empty)
+            self.halo.check_same(len(self._inflows), "Solver2D: discharge inlets")
+            if self._inflows:
+                T.inlet_sums = torch.zeros(len(self._inflows), dtype=torch.float64, device=dev)
         # friction
         if cfg.friction is None:
             T.fkind, T.ntab, T.ncls, T.nfield = L.FRICTION_NONE, None, None, None
@@ -537,7 +540,7 @@ class Solver2D:
         a.state = _ptr(self._state)
         return a
 
-    def _launch_inflow(self, inl, src, s):
+    def _inflow_args(self, inl, src, hsum=None):
         f = inl["f"]
         a = L.GswInflowArgs()
         a.abi_version = L.ABI_VERSION
@@ -551,16 +554,33 @@ class Solver2D:
         a.nx_n, a.ny_n, a.ds, a.dry_frac = f["nx"], f["ny"], f["ds"], f["dry_frac"]
         a.t_knots, a.q_knots, a.n_knots = _ptr(inl["t"]), _ptr(inl["q"]), inl["nk"]
         a.state = _ptr(self._state)
-        L.call("gsw_inflow_apply", C.byref(a), s)
+        a.hsum = hsum
+        return a
+
+    def _apply_inflows(self, T, src, s):
+        """Inflow ghosts of every inlet on `src`; returns the kernels launched. On a split
+        run an inlet may span ranks: each rank's depth sum, then one batched sum over the
+        ranks for every inlet (solver.py:1956-1966), which the inflow kernels then use."""
+        sums = [None] * len(T.inflows)
+        n = len(T.inflows)
+        if self.halo is not None and T.inflows:
+            base = T.inlet_sums.data_ptr()
+            sums = [C.c_void_p(base + 8 * k) for k in range(len(T.inflows))]
+            for inl, p in zip(T.inflows, sums):
+                L.call("gsw_inflow_depth_sum", C.byref(self._inflow_args(inl, src)), p, s)
+            self.halo.allreduce_sum_(T.inlet_sums)
+            n += len(T.inflows)
+        for inl, p in zip(T.inflows, sums):
+            L.call("gsw_inflow_apply", C.byref(self._inflow_args(inl, src, p)), s)
+        return n
 
     def _launch_step(self, k_parity: int, T):
         """Ghost fill, inflow, fused step and stage for the buffer pair (k, 1-k)."""
         src, dst = self._buf[k_parity], self._buf[1 - k_parity]
         s = _stream()
         L.call("gsw_bc_fill", C.byref(self._bc_args(src)), s)
-        for inl in T.inflows:
-            self._launch_inflow(inl, src, s)
-        n = 2 + len(T.inflows) + 2 * len(T.stages) + (1 if len(T.stages) > 1 else 0)
+        n = 2 + 2 * len(T.stages) + (1 if len(T.stages) > 1 else 0)
+        n += self._apply_inflows(T, src, s)
         windows = self._overlap_windows() if self.halo is not None else None
         if windows is None:
             if self.halo is not None:
@@ -687,8 +707,7 @@ class Solver2D:
         L.call("gsw_bc_fill", C.byref(self._bc_args(src)), s)
         if self.halo is not None:
             self.halo.exchange(src)
-        for inl in T.inflows:
-            self._launch_inflow(inl, src, s)
+        self._apply_inflows(T, src, s)
 
     def residual(self):
         """SRM-HLLC residual (3, nxp, nyp) of the current state on cells [2, n-3]^2, zero

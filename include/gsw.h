@@ -39,7 +39,7 @@ extern "C" {
 #define GSW_API
 #endif
 
-#define GSW_ABI_VERSION 3u
+#define GSW_ABI_VERSION 4u
 
 /* return codes */
 #define GSW_OK               0
@@ -261,8 +261,18 @@ typedef struct GswInflowArgs {
     double   nx_n, ny_n, ds, dry_frac;
     const double* t_knots; const double* q_knots; int32_t n_knots;
     const GswLoopState* state;  /* Q is taken at state->t (pre-step) */
+    const double* hsum;         /* device; NULL: the depth sum of the cells above. Non-NULL: the inlet's
+                                   depth sum over every rank of a split run (the per-rank sums of
+                                   gsw_inflow_depth_sum added by an all-reduce), as the reference's
+                                   hsum argument (geoswe/solver.py:1956-1966, geoswe/bc.py:207); the
+                                   dry-inlet seed still uses this rank's cells, as there */
 } GswInflowArgs;
 GSW_API int gsw_inflow_apply(const GswInflowArgs* a, void* stream);
+/* *out = this rank's depth sum over the inlet's cells (the pairwise float sum of
+ * gsw_inflow_apply, widened to double; 0 for no cells), on the device. A split run adds
+ * these over the ranks and passes the total as hsum. Replaces the per-rank sum the
+ * reference's split loop feeds its Allreduce (geoswe/solver.py:1958-1963). */
+GSW_API int gsw_inflow_depth_sum(const GswInflowArgs* a, double* out, void* stream);
 
 /* ------------------------------------------------------------------------- */
 /* Compressed (flat) mesh.                                                    */
@@ -328,8 +338,16 @@ typedef struct GswFlatInflowArgs {
     double   nx_n, ny_n, ds;      /* inward unit normal (axis-aligned) and cell width */
     const double* t_knots; const double* q_knots;
     const GswLoopState* state;    /* Q is taken at state->t; nothing is written when done */
+    const double* hsum;           /* device; NULL: the neighbours' depth sum above. Non-NULL: the inlet's
+                                     depth sum over every rank of a split run (the per-rank sums of
+                                     gsw_flat_inflow_depth_sum added by an all-reduce), as the
+                                     reference's split loop does (geoswe/compressed_solver.py:2145-2153) */
 } GswFlatInflowArgs;
 GSW_API int gsw_flat_inflow_apply(const GswFlatInflowArgs* a, void* stream);
+/* *out = this rank's depth sum over the inlet's active neighbours (the pairwise float sum
+ * of gsw_flat_inflow_apply, widened to double; 0 for none), on the device. Replaces the
+ * per-rank sum of the reference's split flat loop (geoswe/compressed_solver.py:2147). */
+GSW_API int gsw_flat_inflow_depth_sum(const GswFlatInflowArgs* a, double* out, void* stream);
 
 /* Stage on ghost-ring cells of the compressed mesh, applied after the step at the
  * step's start time state->t: per gauge g the stage is interpolated in the (NG, n_t)

@@ -38,7 +38,8 @@ def test_struct_layouts_match_c(tmp_path):
                                "max_h", "cfl_skip", "h_cfl", "warps"],
               "GswBcArgs": ["pitch", "kinds", "state"],
               "GswStageArgs": ["pitch", "bed_is_f32", "time_s", "lam_target", "g", "h_cfl"],
-              "GswInflowArgs": ["pitch", "step_off", "nx_n", "t_knots", "state"],
+              "GswInflowArgs": ["pitch", "step_off", "nx_n", "t_knots", "state", "hsum"],
+              "GswFlatInflowArgs": ["n_knots", "nx_n", "t_knots", "state", "hsum"],
               "GswFlatArgs": ["n_bricks", "flags", "bed", "inv_dx", "h_min_cfl", "linf", "state", "rain",
                               "ny", "n_tab_len", "vcap", "keep_h", "max_h", "warps"],
               "GswMember": ["dt", "inv_dx", "vcap", "linf", "rain_kind", "rain", "n_tab"],

@@ -198,6 +198,34 @@ def test_face_extent_mismatch_raises_on_both_ranks():
     assert "nyp=12" in out[1] and "nyp=10" in out[1] and "rank 0" in out[1]
 
 
+def _inlet_count_rank(rank, world, port, out):
+    _init(rank, world, port)
+    try:
+        h = Halo2D(None, 20, 10, G, dtype="float32", dims=[world, 1])
+        sums = torch.tensor([1.5 * (rank + 1), 0.0 if rank else 2.25], dtype=torch.float64)
+        h.allreduce_sum_(sums)
+        h.check_same(2, "inlets")                       # every rank lists two inlets
+        res = [float(x) for x in sums]
+        try:
+            h.check_same(2 + rank, "inlets")            # rank 1 lists one more
+            res.append("accepted")
+        except RuntimeError as e:
+            res.append(str(e))
+        out[rank] = res
+    finally:
+        dist.destroy_process_group()
+
+
+def test_inlet_sums_and_counts_over_ranks():
+    """The per-inlet depth sums of a split run are added over the ranks in one collective,
+    and a rank listing a different number of inlets (so a different number of
+    collectives per step) is refused on every rank instead of hanging."""
+    out = _spawn(_inlet_count_rank, 2)
+    for r in range(2):
+        assert out[r][:2] == [1.5 + 3.0, 2.25]
+        assert "differ across ranks" in out[r][2] and "between 2 and 3" in out[r][2]
+
+
 # ------------------------------------------------------------------ split oracle run
 NSTEPS = 25
 

@@ -46,17 +46,12 @@ def _rank(rank, world, port, out, dims, bc, dtype, host_loop):
         x0, x1, y0, y1 = block_of(NX, NY, dims, (rank // dims[1], rank % dims[1]))
         s = _make((x1 - x0, y1 - y0), bc, dtype, q0[:, x0:x1, y0:y1].copy(), bed[x0:x1, y0:y1].copy(),
                   comm=dist.group.WORLD, dims=dims)
-        refused = False
-        try:
-            s.add_inflow([2], [3], (1.0, 0.0), 2.0, [0.0, 1.0], [1.0, 1.0])
-        except NotImplementedError:
-            refused = True
         if host_loop:
             steps = s.run(T_END, callback=lambda solver, k: None)
         else:
             steps = s.run(T_END)
         q = s.q_interior.detach().cpu().numpy().copy()
-        out[rank] = dict(block=(x0, x1, y0, y1), steps=steps, t=s.t, q=q, refused=refused,
+        out[rank] = dict(block=(x0, x1, y0, y1), steps=steps, t=s.t, q=q,
                          exchanges=s.halo.exchanges, launches=s.kernel_launches)
         torch.cuda.synchronize()
     finally:
@@ -87,10 +82,75 @@ def test_split_run_equals_single_domain(dims, bc, dtype, host_loop):
     for r in range(world):
         o = out[r]
         x0, x1, y0, y1 = o["block"]
-        assert o["refused"], "add_inflow on a split run must raise"
         assert o["steps"] == ref_steps and o["t"] == ref.t, (r, o["steps"], ref_steps, o["t"], ref.t)
         assert o["exchanges"] >= ref_steps and o["launches"] > 0
         np.testing.assert_array_equal(o["q"], want[:, x0:x1, y0:y1])
+
+
+# Two discharge inlets (global padded indices, inward normal, hydrograph): one on the x-
+# face, inside rank 0's block; one on the y- face, across the x seam of a [2, 1] split.
+INLETS = [(np.full(6, 2), np.arange(6, 12), (1.0, 0.0), [0.0, 3.0, 6.0], [0.0, 4.0, 1.0]),
+          (np.arange(12, 34), np.full(22, 2), (0.0, 1.0), [0.0, 6.0], [2.0, 0.5])]
+
+
+def _add_inlets(s, block):
+    """The inlets' cells inside `block` (unpadded [x0, x1) x [y0, y1)), in local padded
+    indices; an inlet with no cells here is added empty, as every rank must list it."""
+    x0, x1, y0, y1 = block
+    for ii, jj, nrm, tq, q in INLETS:
+        keep = (ii - 2 >= x0) & (ii - 2 < x1) & (jj - 2 >= y0) & (jj - 2 < y1)
+        s.add_inflow(ii[keep] - x0, jj[keep] - y0, nrm, 2.0, tq, q)
+
+
+def _inlet_rank(rank, world, port, out, dims):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        torch.cuda.set_device(0)
+        from geoswe_b200.partition import block_of
+        q0, bed = flowing(NX, NY, seed=5, dtype=np.float32)
+        blk = block_of(NX, NY, dims, (rank // dims[1], rank % dims[1]))
+        x0, x1, y0, y1 = blk
+        s = _make((x1 - x0, y1 - y0), ("wall", "wall"), "float32", q0[:, x0:x1, y0:y1].copy(),
+                  bed[x0:x1, y0:y1].copy(), comm=dist.group.WORLD, dims=dims)
+        _add_inlets(s, blk)
+        steps = s.run(T_END)
+        out[rank] = dict(block=blk, steps=steps, t=s.t, q=s.q_interior.detach().cpu().numpy().copy())
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("dims", [[1, 2], [2, 1]])
+def test_split_run_with_inlets(dims):
+    """Discharge inlets on a split run: each rank's share of an inlet's depth is summed
+    over the ranks every step (the reference's batched Allreduce). An inlet within one
+    rank gives the single-domain run bit for bit ([1, 2]: both inlets lie in rank 0's
+    columns); an inlet across a seam adds the ranks' partial sums, which may round
+    differently from the single-domain sum, so the [2, 1] split is held to the same
+    steps and a relative tolerance of 1e-5."""
+    q0, bed = flowing(NX, NY, seed=5, dtype=np.float32)
+    ref = _make((NX, NY), ("wall", "wall"), "float32", q0, bed)
+    _add_inlets(ref, (0, NX, 0, NY))
+    ref_steps = ref.run(T_END)
+    want = ref.q_interior.detach().cpu().numpy()
+    torch.cuda.synchronize()
+    world = dims[0] * dims[1]
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_inlet_rank, args=(world, _free_port(), out, dims), nprocs=world,
+                           start_method="spawn", join=True)
+        out = dict(out)
+    assert ref_steps > 20
+    for r in range(world):
+        o = out[r]
+        x0, x1, y0, y1 = o["block"]
+        assert o["steps"] == ref_steps and o["t"] == ref.t, (r, o["steps"], ref_steps)
+        if dims == [1, 2]:
+            np.testing.assert_array_equal(o["q"], want[:, x0:x1, y0:y1])
+        else:
+            np.testing.assert_allclose(o["q"], want[:, x0:x1, y0:y1], rtol=1e-5, atol=1e-6)
 
 
 CNX, CNY, CDX, C_T_END = 72, 90, 3.0, 900.0
@@ -157,4 +217,91 @@ def test_split_compressed_run_equals_single_domain(dims):
         x0, x1, y0, y1 = o["block"]
         assert o["sent"] > 0 and o["exchanges"] >= ref_steps
         assert o["steps"] == ref_steps and o["t"] == ref.t, (r, o["steps"], ref_steps, o["t"], ref.t)
+        np.testing.assert_array_equal(o["depth"], want[x0:x1, y0:y1])
+
+
+def _forced_compressed(z, mask, cls_pad, table, block, ckpt=None, max_steps=10 ** 9, resume=False, **kw):
+    """The compressed rain run of `block` with a ring stage, infiltration, a sponge band and
+    a discharge inlet, each given by global coordinates and restricted to the block (a
+    rank lists what lies in its own block; the inlet is listed, possibly empty, on every
+    rank)."""
+    from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
+    from geoswe_b200.compressed import CompressedSolver
+    x0, x1, y0, y1 = block
+    s = Solver2D(Mesh2D(nx=x1 - x0, ny=y1 - y0, dx=CDX, dy=CDX, ngh=2),
+                 Config(bc_x="fall", bc_y="fall", friction="manning"),
+                 np.zeros((3, x1 - x0, y1 - y0), np.float32), z[x0:x1, y0:y1].copy(), **kw)
+    s.set_inside_mask(mask[x0:x1, y0:y1])
+    s.set_manning_table(cls_pad[x0:x1 + 4, y0:y1 + 4].copy(), table)
+    cs = CompressedSolver.from_dense(s)
+    cs.set_rain(RainfallForcing(time_s=[0.0, 300.0, 1e9], rate_mm_h=[60.0, 25.0, 25.0]))
+    ij = cs.ij_active
+    gi, gj = ij[:, 0] + x0, ij[:, 1] + y0                   # global padded indices
+    own = (ij[:, 0] >= 2) & (ij[:, 0] < 2 + x1 - x0) & (ij[:, 1] >= 2) & (ij[:, 1] < 2 + y1 - y0)
+    # ring stage on the ring cells of global rows < 30 (owned by this block)
+    ring = np.nonzero((cs.is_active == 0) & own & (gi < 30))[0]
+    bed = cs._b[cs._slot].cpu().numpy()[ring].astype(np.float32)
+    t_c = np.array([0.0, 450.0, 900.0])
+    cs.set_ring(dict(i=ij[ring, 0], j=ij[ring, 1], bed=bed, wg=np.ones((ring.size, 1), np.float32), NG=1,
+                     n=int(ring.size), t_common=t_c, stage_all=np.array([[14.0, 16.0, 15.0]], np.float32)))
+    cs.set_infil({"tab": np.array([1e-6, 2e-6, 5e-7, 0.0], np.float32)})
+    keep = np.ones((cs.nxp, cs.nyp), np.float32)
+    band = (np.arange(cs.nxp)[:, None] + x0 >= 40) & (np.arange(cs.nxp)[:, None] + x0 < 44)
+    keep[np.broadcast_to(band, keep.shape)] = 0.995
+    cs.set_sponge({"keep": keep, "amb": np.zeros_like(keep)})
+    g, a = cs.ghost_boundary_pairs()
+    pick = (ij[a, 0] == ij[g, 0]) & (ij[a, 1] == ij[g, 1] + 1) & (gi[g] >= 20) & (gi[g] < 28) & own[g]
+    cs.add_inflow(g[pick], a[pick], (0.0, 1.0), CDX, [0.0, 400.0, 900.0], [0.0, 3.0, 0.5])
+    steps = cs.run(t_end=C_T_END, window=8, max_steps=max_steps, checkpoint_every_s=200.0 if ckpt else 0.0,
+                   ckpt_dir=ckpt, resume=resume)
+    return cs, steps, int(pick.sum())
+
+
+def _forced_rank(rank, world, port, out, dims, ckpt, m):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        torch.cuda.set_device(0)
+        from geoswe_b200.partition import block_of
+        z, mask, cls_pad, table = _compressed_inputs()
+        block = block_of(CNX, CNY, dims, (rank // dims[1], rank % dims[1]))
+        # a run stopped by a step cap (no clipped step) with checkpoints on the way, then
+        # fresh solvers resuming from them
+        cs, steps, n_inlet = _forced_compressed(z, mask, cls_pad, table, block, ckpt=ckpt, max_steps=m,
+                                                comm=dist.group.WORLD, dims=dims)
+        cs2, steps2, _ = _forced_compressed(z, mask, cls_pad, table, block, ckpt=ckpt, resume=True,
+                                            comm=dist.group.WORLD, dims=dims)
+        out[rank] = dict(block=block, steps=steps + steps2, t=cs2.t, nsteps=cs2.nsteps, depth=cs2.depth(),
+                         n_inlet=n_inlet)
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_split_compressed_run_with_forcings_and_checkpoints(tmp_path):
+    """A split compressed run with a ring stage, infiltration, a sponge band, a discharge
+    inlet and checkpoints (per-rank state files, meta written by rank 0), stopped by a
+    step cap half-way and resumed from its checkpoint by fresh solvers: equals the single-domain
+    run bit for bit (the inlet lies in one rank's block; the other ranks list it empty)."""
+    import json
+    z, mask, cls_pad, table = _compressed_inputs()
+    ref, ref_steps, n_inlet = _forced_compressed(z, mask, cls_pad, table, (0, CNX, 0, CNY))
+    want = ref.depth()
+    torch.cuda.synchronize()
+    dims = [2, 1]
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_forced_rank, args=(2, _free_port(), out, dims, str(tmp_path), ref_steps // 2), nprocs=2,
+                           start_method="spawn", join=True)
+        out = dict(out)
+    meta = json.load(open(tmp_path / "ckpt_meta.json"))
+    assert ref_steps > 20 and n_inlet > 0
+    assert meta["nranks"] == 2 and meta["steps"] == ref_steps
+    assert (tmp_path / "ckpt_r00.npz").exists() and (tmp_path / "ckpt_r01.npz").exists()
+    assert sum(out[r]["n_inlet"] for r in range(2)) == n_inlet
+    for r in range(2):
+        o = out[r]
+        x0, x1, y0, y1 = o["block"]
+        assert o["nsteps"] == ref_steps and o["t"] == ref.t, (r, o["nsteps"], ref_steps, o["t"], ref.t)
         np.testing.assert_array_equal(o["depth"], want[x0:x1, y0:y1])
