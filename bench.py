@@ -772,7 +772,7 @@ def run_compressed(args):
     import warnings
     with warnings.catch_warnings():
         warnings.simplefilter("ignore")
-        cs = CompressedSolver.from_dense(s)
+        cs = CompressedSolver.from_dense(s, brick_h=args.brick_h)
     del s
     torch.cuda.empty_cache()
     from geoswe_b200 import RainfallForcing
@@ -812,7 +812,8 @@ def run_compressed(args):
             "higher_is_better": True, "dtype": "f32", "arith": args.arith, "data": "synthetic",
             "config": {"workload": f"rain-on-terrain {n}x{n} on the compressed mesh, active z < p60 dilated 8 "
                                    f"cells, 50 mm/h, CFL 0.5, fp32",
-                       "active_cells": cells, "stored_slots": int(cs.nslots), "bricks": int(cs.n_bricks)},
+                       "active_cells": cells, "stored_slots": int(cs.nslots), "bricks": int(cs.n_bricks),
+                       "brick_h": cs.brick_h},
             "residual_bit_identical_to_dense": identical, "residual_nonzero_fraction": wet,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "kernel_ms": kern_ms, "bytes_per_cell": 38,
@@ -863,7 +864,7 @@ def run_tidal(args):
     rbed = s._b[:ngh, : s.nyp].reshape(-1).cpu().numpy().astype(np.float32)
     with warnings.catch_warnings():
         warnings.simplefilter("ignore")
-        cs = CompressedSolver.from_dense(s, track_max_depth=False)
+        cs = CompressedSolver.from_dense(s, track_max_depth=False, brick_h=args.brick_h)
     del s
     torch.cuda.empty_cache()
     t_c = np.arange(0.0, 3600.0 + 60.0, 60.0)
@@ -904,7 +905,7 @@ def run_tidal(args):
             "config": {"workload": f"tidal everywhere-wet compressed {nx}x{ny}, dx=1 m, sinusoidal bed, "
                                    f"n=0.03, tidal stage on the x- ring, CFL 0.5, fp32",
                        "active_cells": cells, "stored_slots": int(cs.nslots), "bricks": int(cs.n_bricks),
-                       "l2": "inputs larger than L2 (no flush)"},
+                       "brick_h": cs.brick_h, "l2": "inputs larger than L2 (no flush)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": _traffic("flat_tidal", cells)[0],
                          "traffic_from": _traffic("flat_tidal", cells)[1],
@@ -1004,6 +1005,7 @@ def main():
     ap.add_argument("--db-n", type=int, default=512)
     ap.add_argument("--db-steps", type=int, default=500)
     ap.add_argument("--db-t-end", type=float, default=50.0, help="simulated time of the fp64 comparison")
+    ap.add_argument("--brick-h", type=int, default=16, help="rows per brick of the compressed and tidal cases")
     ap.add_argument("--tidal-nx", type=int, default=32000)
     ap.add_argument("--tidal-ny", type=int, default=20000)
     ap.add_argument("--adj-n", type=int, default=2048)

@@ -87,7 +87,7 @@ class GswFlatArgs(C.Structure):
                 ("linf", i32), ("rain_kind", i32), ("state", vp), ("lam_target", vp), ("rain", vp),
                 ("ngh", i32), ("nx", i32), ("ny", i32), ("n_tab_len", i32), ("n_cls", vp), ("n_tab", vp),
                 ("vcap", f64), ("quadratic", i32), ("keep_h", i32), ("max_h", vp), ("rain_lookup", vp),
-                ("rain_ncol", i32), ("segments", i32)]
+                ("rain_ncol", i32), ("segments", i32), ("brick_lo", C.c_int64), ("brick_hi", C.c_int64)]
 
 
 class GswFlatInflowArgs(C.Structure):

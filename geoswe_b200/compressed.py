@@ -163,7 +163,8 @@ class CompressedSolver:
             # seed, so every cell an active stencil here reads is stored on both ranks
             ext = inside.to(torch.float32)
             halo.exchange(ext)
-            sl, lin, ii, jj = self._build_layout((ext > 0.5).to(torch.uint8), active=inside)
+            sl, lin, ii, jj = self._build_layout((ext > 0.5).to(torch.uint8), active=inside,
+                                                 seams=[f for f in ("x-", "x+", "y-", "y+") if halo.has_neighbor(f)])
         pidx_of_slot = ii * s.pitch + jj
 
         def pack_dense(field2d_pitched, dtype=torch.float32):
@@ -313,12 +314,16 @@ class CompressedSolver:
         self.dt_max_user = dt_max
         self._dense_had_rain = False
 
-    def _build_layout(self, inside, active=None):
+    def _build_layout(self, inside, active=None, seams=()):
         """Stored set (the inside mask dilated twice with the 4-neighbour cross,
         compressed_rhs.py:256), Hilbert bricks, the canonical id -> slot map and the slot
         flags. `inside` is a device uint8 (nxp, nyp) mask; `active` (default `inside`)
         marks the cells this solver updates -- on a split run `inside` also holds the
         neighbours' inside cells in the seam ghost rows, stored but not updated here.
+        `seams` names the faces ("x-", "x+", "y-", "y+") whose ghost strips another rank
+        refreshes: the bricks that read a cell of those strips are moved to the end of
+        the brick order (Hilbert order kept within each part), and `n_bricks_inner`
+        counts the others, which the step updates while the seam exchange is in flight.
         Returns (slots, padded linear index, i, j) of every stored cell."""
         dev = self.device
         self._inside = inside
@@ -339,6 +344,9 @@ class CompressedSolver:
             raise ValueError(_DEGENERATE)
         bij, bnbr = build_bricks(st.to(torch.uint8).cpu().numpy(), self.brick_h)
         self.n_bricks = int(len(bij))
+        self.n_bricks_inner = self.n_bricks
+        if seams:
+            bij, bnbr = self._seam_bricks_last(bij, bnbr, seams)
         BS = self.brick_h * BRICK_PITCH
         self.nslots = (self.n_bricks + 1) * BS
         self._bij = torch.from_numpy(bij).to(dev)
@@ -367,6 +375,34 @@ class CompressedSolver:
         self._slot_cells = sl
         self._lin_of_slot = lin
         return sl, lin, ii, jj
+
+    def _seam_bricks_last(self, bij, bnbr, seams):
+        """Stable reorder of the bricks: those with a cell within 3 cells (rows or
+        columns) of a seam ghost strip last. A brick's step reads its own cells and at
+        most 2 rows and 2 columns beyond them (the x-face gradients' bed two rows out,
+        the edge lanes' y-gradients one column beyond the neighbour brick's edge), so
+        the bricks kept first read no seam ghost cell, and the copy of unchanged stored
+        cells into the new state (seam ghosts included) is made by the bricks moved last."""
+        g, reach, bh = self.ngh, 3, self.brick_h
+        r0 = bij[:, 0].astype(np.int64) * bh
+        c0 = bij[:, 1].astype(np.int64) * BRICK_W
+        late = np.zeros(len(bij), bool)
+        if "x-" in seams:
+            late |= r0 < g + reach
+        if "x+" in seams:
+            late |= r0 + bh - 1 >= self.nxp - g - reach
+        if "y-" in seams:
+            late |= c0 < g + reach
+        if "y+" in seams:
+            late |= c0 + BRICK_W - 1 >= self.nyp - g - reach
+        nb = len(bij)
+        order = np.concatenate([np.nonzero(~late)[0], np.nonzero(late)[0]])
+        new_of_old = np.empty(nb + 1, np.int64)
+        new_of_old[order] = np.arange(nb)
+        new_of_old[nb] = nb                                  # the all-zero brick stays last
+        self.n_bricks_inner = int((~late).sum())
+        return (np.ascontiguousarray(bij[order]),
+                np.ascontiguousarray(new_of_old[bnbr[order].astype(np.int64)].astype(np.int32)))
 
     def _init_runtime(self, track_max_depth):
         dev = self.device
@@ -478,6 +514,14 @@ class CompressedSolver:
                 raise ValueError("add_inflow: index out of range of the stored cells")
             if act[g].any() or not act[a].all():
                 raise ValueError("add_inflow: ghost_idx must be ring cells and nbr_idx active cells")
+            if self.flat_halo is not None:
+                gi, gj = self.ij_active[g, 0], self.ij_active[g, 1]
+                h, w = self.ngh, self.halo
+                seam = ((w.has_neighbor("x-") & (gi < h)) | (w.has_neighbor("x+") & (gi >= self.nxp - h)) |
+                        (w.has_neighbor("y-") & (gj < h)) | (w.has_neighbor("y+") & (gj >= self.nyp - h)))
+                if seam.any():
+                    raise ValueError("add_inflow: a ghost cell lies in a seam ghost strip, which the neighbouring "
+                                     "rank owns; list the inlet cells of this rank's own block")
         dev = self.device
         slot = self._slot
         self._inflows.append(dict(
@@ -846,6 +890,9 @@ class CompressedSolver:
         per_step = 2 + len(self._inflows) + (self._ring is not None) + 3 * forced
         if split:
             per_step += self.flat_halo.launches_per_exchange + (len(self._inflows) if inlet_sums is not None else 0)
+        nb_in = self.n_bricks_inner
+        if split:                               # the step in two brick ranges
+            per_step += int(nb_in > 0) + int(self.n_bricks > nb_in) - 1
 
         def one_step(k_parity):
             s = _stream()
@@ -853,8 +900,6 @@ class CompressedSolver:
                 self.halo.allreduce_max_(self._lam_view)
             L.call("gsw_dt_finalize_dev", _ptr(self._dtp_dev), _ptr(self._state), s)
             src, dst = self._q[k_parity], self._q[1 - k_parity]
-            if split:                           # seam ghosts from the neighbours, before the step
-                self.flat_halo.exchange(src)
             sums = [None] * len(self._inflows)
             if inlet_sums is not None:          # an inlet may span ranks: one batched sum of
                 base = inlet_sums.data_ptr()    # every inlet's depth over the ranks (:2145-2153)
@@ -867,7 +912,19 @@ class CompressedSolver:
             a = self._args(src, dst)
             if forced:                          # the wave speed is taken after the forcings
                 a.lam_target = None
-            L.call("gsw_flat_step", C.byref(a), s)
+            if split:
+                # seam ghosts from the neighbours (the reference posts them before its
+                # interior step, compressed_solver.py:2185-2190, 2209-2222): the bricks
+                # that read no seam ghost cell step while the transfer is in flight, the
+                # rest after the ghosts are in place
+                hnd = self.flat_halo.start(src)
+                a.brick_lo, a.brick_hi = 0, nb_in
+                if nb_in:
+                    L.call("gsw_flat_step", C.byref(a), s)
+                self.flat_halo.finish(hnd)
+                a.brick_lo, a.brick_hi = nb_in, self.n_bricks
+            if not split or self.n_bricks > nb_in:
+                L.call("gsw_flat_step", C.byref(a), s)
             if forced:
                 L.call("gsw_flat_forcings", C.byref(self._forcing_args(dst, 0)), s)
             if self._ring is not None:          # ring stage at t_n, after the step

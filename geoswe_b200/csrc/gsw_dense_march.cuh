@@ -85,7 +85,7 @@ __device__ __forceinline__ Face<T> shfl_face_up(const Face<T>& f) {
     r.Ft = __shfl_up_sync(0xffffffffu, f.Ft, 1);
     r.srcR = __shfl_up_sync(0xffffffffu, f.srcR, 1);
     r.srcL = r.srcR;
-    r.wet = __shfl_up_sync(0xffffffffu, (int)f.wet, 1) != 0;
+    r.wet = true;   // unused: the residual adds a dry face's zeros
     return r;
 }
 
@@ -169,18 +169,23 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
             Face<T> Ef;
             srm_face<T, true>(cur, nx, p.half_dx, p.inv_dx, p.g, p.h_min, Ef, p.g_recip);
             // the residual in the reference's order (E, W, N, S per component; accumulate() in
-            // gsw_core.cuh), the E and W parts before the y-face so that W is released early
+            // gsw_core.cuh), the E and W parts before the y-face so that W is released early.
+            // A dry face (skipped by the reference) holds +0 in every field, and adding or
+            // subtracting +0 leaves these sums unchanged: they start at +0 and are never -0
+            // (an IEEE sum or difference is -0 only from a -0 left operand; the fast
+            // compilation's flush to zero can make one, whose sign may then differ), so no test of
+            // the wet flag is needed.
             T rh = (T)0, rhu = (T)0, rhv = (T)0;
-            if (Ef.wet) { rh = rh - Ef.Fh; rhu = rhu - Ef.Fn; rhv = rhv - Ef.Ft; rhu = rhu - Ef.srcL; }
-            if (Wf.wet) { rh = rh + Wf.Fh; rhu = rhu + Wf.Fn; rhv = rhv + Wf.Ft; rhu = rhu + Wf.srcR; }
+            rh = rh - Ef.Fh; rhu = rhu - Ef.Fn; rhv = rhv - Ef.Ft; rhu = rhu - Ef.srcL;
+            rh = rh + Wf.Fh; rhu = rhu + Wf.Fn; rhv = rhv + Wf.Ft; rhu = rhu + Wf.srcR;
             Wf = Ef;
             const Cell<T> rn = shfl_cell_down(cur);
             {
                 Face<T> Nf;
                 srm_face<T, false>(cur, rn, p.half_dy, p.inv_dy, p.g, p.h_min, Nf, p.g_recip);
                 const Face<T> Sf = shfl_face_up(Nf);
-                if (Nf.wet) { rh = rh - Nf.Fh; rhu = rhu - Nf.Ft; rhv = rhv - Nf.Fn; rhv = rhv - Nf.srcL; }
-                if (Sf.wet) { rh = rh + Sf.Fh; rhu = rhu + Sf.Ft; rhv = rhv + Sf.Fn; rhv = rhv + Sf.srcR; }
+                rh = rh - Nf.Fh; rhu = rhu - Nf.Ft; rhv = rhv - Nf.Fn; rhv = rhv - Nf.srcL;
+                rh = rh + Sf.Fh; rhu = rhu + Sf.Ft; rhv = rhv + Sf.Fn; rhv = rhv + Sf.srcR;
             }
 
             if (out_lane) {

@@ -44,7 +44,10 @@ __host__ __device__ __forceinline__ int auto_segments(int64_t bricks, int64_t wa
 
 // For the flat kernels' argument struct
 template <typename T>
-struct FlatK { FlatMesh<T> m; FlatPhys<T> ph; const GswLoopState* st; unsigned long long* lam; int segs; };
+struct FlatK {
+    FlatMesh<T> m; FlatPhys<T> ph; const GswLoopState* st; unsigned long long* lam; int segs;
+    int64_t b0, b1;    // bricks [b0, b1) are stepped
+};
 
 // Slot of brick-relative (row, lane). Lanes 0/31 of the rows above/below the brick are
 // never used by an output cell; they read the zero brick.
@@ -100,7 +103,7 @@ __device__ __forceinline__ Face<T> shfl_up_face(const Face<T>& f) {
     r.Ft = __shfl_up_sync(0xffffffffu, f.Ft, 1);
     r.srcR = __shfl_up_sync(0xffffffffu, f.srcR, 1);
     r.srcL = r.srcR;
-    r.wet = __shfl_up_sync(0xffffffffu, (int)f.wet, 1) != 0;
+    r.wet = true;   // unused: the residual adds a dry face's zeros
     return r;
 }
 
@@ -160,18 +163,23 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
         Face<T> Ef;
         srm_face<T, true>(cur, nx, ph.half_dx, ph.inv_dx, ph.g, ph.h_min, Ef, ph.g_recip);
         // the residual in the reference's order (E, W, N, S per component; accumulate() in
-        // gsw_core.cuh), the E and W parts before the y-face so that W is released early
+        // gsw_core.cuh), the E and W parts before the y-face so that W is released early.
+        // A dry face (skipped by the reference) holds +0 in every field, and adding or
+        // subtracting +0 leaves these sums unchanged: they start at +0 and are never -0
+        // (an IEEE sum or difference is -0 only from a -0 left operand; the fast
+        // compilation's flush to zero can make one, whose sign may then differ), so no test of
+        // the wet flag is needed.
         T rh = (T)0, rhu = (T)0, rhv = (T)0;
-        if (Ef.wet) { rh = rh - Ef.Fh; rhu = rhu - Ef.Fn; rhv = rhv - Ef.Ft; rhu = rhu - Ef.srcL; }
-        if (Wf.wet) { rh = rh + Wf.Fh; rhu = rhu + Wf.Fn; rhv = rhv + Wf.Ft; rhu = rhu + Wf.srcR; }
+        rh = rh - Ef.Fh; rhu = rhu - Ef.Fn; rhv = rhv - Ef.Ft; rhu = rhu - Ef.srcL;
+        rh = rh + Wf.Fh; rhu = rhu + Wf.Fn; rhv = rhv + Wf.Ft; rhu = rhu + Wf.srcR;
         Wf = Ef;
         const Cell<T> rn = shfl_down_cell<T>(cur);
         {
             Face<T> Nf;
             srm_face<T, false>(cur, rn, ph.half_dy, ph.inv_dy, ph.g, ph.h_min, Nf, ph.g_recip);
             const Face<T> Sf = shfl_up_face<T>(Nf);
-            if (Nf.wet) { rh = rh - Nf.Fh; rhu = rhu - Nf.Ft; rhv = rhv - Nf.Fn; rhv = rhv - Nf.srcL; }
-            if (Sf.wet) { rh = rh + Sf.Fh; rhu = rhu + Sf.Ft; rhv = rhv + Sf.Fn; rhv = rhv + Sf.srcR; }
+            rh = rh - Nf.Fh; rhu = rhu - Nf.Ft; rhv = rhv - Nf.Fn; rhv = rhv - Nf.srcL;
+            rh = rh + Sf.Fh; rhu = rhu + Sf.Ft; rhv = rhv + Sf.Fn; rhv = rhv + Sf.srcR;
         }
         if (lane >= 1 && lane <= 30) {
             const int64_t o = bidx * v.BS + (int64_t)r * GSW_BRICK_PITCH + (lane - 1);

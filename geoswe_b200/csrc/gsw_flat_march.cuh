@@ -18,8 +18,9 @@ template <typename T, bool STEP, int MINB, bool REFPOW, bool LEAN>
 __global__ void __launch_bounds__(256, MINB) flat_march_kernel(FlatK<T> p) {
     if (STEP && p.st->done) return;
     const int64_t item = (int64_t)blockIdx.x * blockDim.y + threadIdx.y;   // (brick, row segment)
-    const int64_t bidx = item / p.segs;
-    const int seg = (int)(item - bidx * p.segs);
+    const int64_t rel = item / p.segs;
+    const int seg = (int)(item - rel * p.segs);
+    const int64_t bidx = p.b0 + rel;
     unsigned long long lam_local = 0ull;
     T dt = (T)0, rate = (T)0;
     const T* frame = nullptr;
@@ -29,7 +30,7 @@ __global__ void __launch_bounds__(256, MINB) flat_march_kernel(FlatK<T> p) {
         if (p.ph.rain_kind == GSW_RAIN_GRIDDED) frame = p.ph.rain + (int64_t)p.st->rain_idx * p.ph.nx * p.ph.ny;
         if (p.ph.rain_kind == GSW_RAIN_LOOKUP) frame = p.ph.rain + (int64_t)p.st->rain_idx * p.ph.ncol;
     }
-    if (bidx < p.m.nb)
+    if (bidx < p.b1)
         lam_local = flat_brick<T, STEP, REFPOW, LEAN>(p.m, p.ph, bidx, seg * p.m.bh / p.segs, (seg + 1) * p.m.bh / p.segs,
                                         dt, rate, frame);
     if (STEP && p.lam != nullptr) block_max_to(lam_local, p.lam);
@@ -59,6 +60,12 @@ inline int fill_flat(const GswFlatArgs* a, FlatK<T>& k, bool step) {
     k.segs = a->segments > 0 ? a->segments : auto_segments(a->n_bricks, (int64_t)sm_count() * 24, a->brick_h);
     if (k.segs != 1 && k.segs != 2 && k.segs != 4) return set_error(GSW_ERR_INVALID, "flat: segments must be 0, 1, 2 or 4");
     if (a->brick_h % k.segs != 0) return set_error(GSW_ERR_INVALID, "flat: brick_h must be a multiple of segments");
+    const bool all = a->brick_lo == 0 && a->brick_hi == 0;
+    k.b0 = all ? 0 : a->brick_lo;
+    k.b1 = all ? a->n_bricks : a->brick_hi;
+    if (k.b0 < 0 || k.b1 < k.b0 || k.b1 > a->n_bricks)
+        return set_error(GSW_ERR_INVALID, "flat: brick range [%lld, %lld) outside [0, %lld)", (long long)a->brick_lo,
+                         (long long)a->brick_hi, (long long)a->n_bricks);
     if (step) {
         if (!a->state) return set_error(GSW_ERR_INVALID, "flat step: state is required");
         if (!a->n_tab || a->n_tab_len < 1) return set_error(GSW_ERR_INVALID, "flat step: n_tab is required");
@@ -97,10 +104,10 @@ inline int launch_flat(const GswFlatArgs* a, cudaStream_t s) {
     FlatK<T> k;
     int rc = fill_flat<T>(a, k, STEP);
     if (rc) return rc;
-    if (k.m.nb == 0) return GSW_OK;
+    if (k.b1 == k.b0) return GSW_OK;
     const int W = a->warps > 0 ? a->warps : 4;
     if (W < 1 || W > 8) return set_error(GSW_ERR_INVALID, "flat: warps must be in [1, 8]");
-    const int64_t blocks = (k.m.nb * k.segs + W - 1) / W;
+    const int64_t blocks = ((k.b1 - k.b0) * k.segs + W - 1) / W;
     if (blocks > 0x7fffffffLL) return set_error(GSW_ERR_INVALID, "flat: too many bricks");
     const int mb = a->min_blocks;
     if (mb != 0 && (mb < 3 || mb > 5)) return set_error(GSW_ERR_INVALID, "flat: min_blocks must be 0, 3, 4 or 5");

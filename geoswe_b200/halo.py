@@ -367,6 +367,13 @@ class FlatHalo:
 
     def exchange(self, planes):
         """Refresh the stored seam ghost cells of the three flat planes in place."""
+        self.finish(self.start(planes))
+
+    def start(self, planes):
+        """Pack the seam cells of the three flat planes and post the sends and receives;
+        returns the handle for ``finish``. Work that reads and writes no seam ghost cell
+        of ``planes`` may run in between (over NCCL, on the device while the transfer is
+        in flight)."""
         device = planes[0].device.type != "cpu"
         if any(p.dtype != torch.float32 for p in planes):
             raise ValueError("FlatHalo: the compressed state is float32")
@@ -382,7 +389,13 @@ class FlatHalo:
                 sends[side], recvs[side] = f["shost"], f["rhost"]
             else:
                 sends[side], recvs[side] = f["sdense"], f["rdense"]
-        for w in self.halo.post(sends, recvs):
+        return {"planes": planes, "device": device, "works": self.halo.post(sends, recvs)}
+
+    def finish(self, handle):
+        """Wait for the transfers of ``start`` and scatter the received seam cells into
+        the stored ghost slots."""
+        planes, device = handle["planes"], handle["device"]
+        for w in handle["works"]:
             w.wait()
         for side, f in self.faces.items():
             if self.staged:

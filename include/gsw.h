@@ -314,6 +314,9 @@ typedef struct GswFlatArgs {
     int32_t  segments;         /* warps per brick: 1 (one warp walks the brick's rows), 2 or 4 (each walks
                                   brick_h / segments rows: shorter per-warp latency for small meshes),
                                   0 (chosen from the brick count against the warps the GPU runs at once) */
+    int64_t  brick_lo, brick_hi; /* step: update bricks [brick_lo, brick_hi) only (a split run steps the
+                                  bricks that read no seam ghost cell while the seam exchange is in flight,
+                                  then the rest); 0, 0: every brick. Ignored by the wave-speed pass. */
 } GswFlatArgs;
 
 /* Discharge inlet of the compressed mesh: one ghost (ring) slot per inlet cell, next to

@@ -41,7 +41,8 @@ def test_struct_layouts_match_c(tmp_path):
               "GswInflowArgs": ["pitch", "step_off", "nx_n", "t_knots", "state", "hsum"],
               "GswFlatInflowArgs": ["n_knots", "nx_n", "t_knots", "state", "hsum"],
               "GswFlatArgs": ["n_bricks", "flags", "bed", "inv_dx", "h_min_cfl", "linf", "state", "rain",
-                              "ny", "n_tab_len", "vcap", "keep_h", "max_h", "warps"],
+                              "ny", "n_tab_len", "vcap", "keep_h", "max_h", "warps", "segments", "brick_lo",
+                              "brick_hi"],
               "GswMember": ["dt", "inv_dx", "vcap", "linf", "rain_kind", "rain", "n_tab"],
               "GswEnsembleArgs": ["n_bricks", "n_members", "grid", "brick_ij", "flags", "q0", "bed",
                                   "members", "states", "scratch", "all_done"],

@@ -491,3 +491,55 @@ def test_split_flat_oracle_run_equals_single_domain(world, dims):
         seen += len(out[r]["h"])
     assert seen == int(tab["is_active"].sum())
     assert float(o.q[0][tab["is_active"] != 0].max()) > 0.1
+
+
+@pytest.mark.parametrize("seams", [("x-",), ("x+", "y-"), ("x-", "x+", "y-", "y+")])
+def test_seam_bricks_ordered_last(seams):
+    """A split compressed run orders the bricks that read a seam ghost strip last: the
+    bricks before them have no cell within 3 rows or columns of a seam strip (the step
+    reads 2), the brick set and the neighbour links are those of the unsplit layout, and
+    Hilbert order is kept within each part."""
+    from geoswe_b200.compressed import BRICK_W, CompressedSolver
+    rng = np.random.default_rng(3)
+    nxp, nyp, g = 83, 131, 2
+    inside = torch.from_numpy((rng.random((nxp, nyp)) < 0.7).astype(np.uint8))
+    inside[:g], inside[-g:], inside[:, :g], inside[:, -g:] = 0, 0, 0, 0
+
+    def layout(seams):
+        cs = CompressedSolver()
+        cs._init_physics(device="cpu", nxp=nxp, nyp=nyp, ngh=g, nx=nxp - 2 * g, ny=nyp - 2 * g, dx=1.0, g=9.81,
+                         cfl=0.5, h_min=1e-6, cfl_linf=False, vcap=1.0, quad=True, keep_h=True, dt_max=None,
+                         brick_h=8)
+        cs._build_layout(inside, seams=seams)
+        return cs, cs._bij.numpy().astype(np.int64), cs._bnbr.numpy().astype(np.int64)
+
+    plain, pij, pnbr = layout(())
+    cs, bij, bnbr = layout(seams)
+    nb, ni, bh = cs.n_bricks, cs.n_bricks_inner, cs.brick_h
+    assert nb == plain.n_bricks and plain.n_bricks_inner == nb and 0 < ni < nb
+    key = lambda ij: [tuple(x) for x in ij]
+    assert sorted(key(bij)) == sorted(key(pij))
+    pos = {k: n for n, k in enumerate(key(pij))}
+    # each part keeps the unsplit (Hilbert) order
+    for part in (bij[:ni], bij[ni:]):
+        order = [pos[k] for k in key(part)]
+        assert order == sorted(order)
+    # neighbour links point at the same bricks; missing neighbours stay the zero brick
+    for b in range(nb):
+        pb = pos[tuple(bij[b])]
+        for d in range(4):
+            want = pnbr[pb, d]
+            got = bnbr[b, d]
+            assert (got == nb) == (want == nb)
+            if got != nb:
+                assert tuple(bij[got]) == tuple(pij[want])
+    # inner bricks are at least 3 cells from every seam strip
+    r0, c0 = bij[:ni, 0] * bh, bij[:ni, 1] * BRICK_W
+    if "x-" in seams:
+        assert (r0 >= g + 3).all()
+    if "x+" in seams:
+        assert (r0 + bh - 1 < nxp - g - 3).all()
+    if "y-" in seams:
+        assert (c0 >= g + 3).all()
+    if "y+" in seams:
+        assert (c0 + BRICK_W - 1 < nyp - g - 3).all()

@@ -192,7 +192,7 @@ def _compressed_rank(rank, world, port, out, dims):
         cs, steps = _compressed_run(z, mask, cls_pad, table, block, comm=dist.group.WORLD, dims=dims)
         out[rank] = dict(block=block, steps=steps, t=cs.t, depth=cs.depth(), n_active=cs.n_active,
                          sent=sum(cs.flat_halo.send_cells(s) for s in ("x-", "x+", "y-", "y+")),
-                         exchanges=cs.flat_halo.exchanges)
+                         exchanges=cs.flat_halo.exchanges, inner=cs.n_bricks_inner, nb=cs.n_bricks)
         torch.cuda.synchronize()
     finally:
         dist.destroy_process_group()
@@ -216,6 +216,7 @@ def test_split_compressed_run_equals_single_domain(dims):
         o = out[r]
         x0, x1, y0, y1 = o["block"]
         assert o["sent"] > 0 and o["exchanges"] >= ref_steps
+        assert 0 < o["inner"] < o["nb"]          # the step overlaps the seam exchange
         assert o["steps"] == ref_steps and o["t"] == ref.t, (r, o["steps"], ref_steps, o["t"], ref.t)
         np.testing.assert_array_equal(o["depth"], want[x0:x1, y0:y1])
 
