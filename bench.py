@@ -540,6 +540,7 @@ def run_ensemble(args):
     t0 = time.perf_counter()
     members = [build_member(sp, arith=args.arith) for sp in specs]
     ens = Ensemble(members, warps=args.ens_warps, grid=args.ens_grid)      # copies the initial states
+    ens.min_blocks, ens.segments = args.ens_min_blocks, args.ens_segments
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
     loop_shape = None
@@ -1017,6 +1018,8 @@ def main():
     ap.add_argument("--ens-window", type=int, default=32)
     ap.add_argument("--ens-warps", type=int, default=0)
     ap.add_argument("--ens-grid", type=int, default=0)
+    ap.add_argument("--ens-min-blocks", type=int, default=0, help="ensemble register cap (with --ens-warps/--ens-grid)")
+    ap.add_argument("--ens-segments", type=int, default=0, help="ensemble warps per brick (0: automatic)")
     ap.add_argument("--split", action="store_true",
                     help="one domain cut into row strips over the ranks (strong scaling) instead of replicas")
     ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],

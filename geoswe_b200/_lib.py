@@ -146,7 +146,7 @@ class GswEnsembleArgs(C.Structure):
                 ("brick_ij", vp), ("brick_nbr", vp),
                 ("brick_member", vp), ("flags", vp), ("n_cls", vp), ("q0", vp), ("q1", vp), ("q2", vp),
                 ("qn0", vp), ("qn1", vp), ("qn2", vp), ("bed", vp), ("max_h", vp), ("members", vp),
-                ("states", vp), ("scratch", vp), ("all_done", vp), ("member_brick_off", vp), ("run", vp)]
+                ("states", vp), ("scratch", vp), ("all_done", vp), ("member_brick_off", vp), ("run", vp), ("lean", i32)]
 
 
 # entry point -> argtypes

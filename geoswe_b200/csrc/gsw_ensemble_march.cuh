@@ -73,7 +73,9 @@ __device__ __forceinline__ void build_run_list(const GswEnsembleArgs& a, int tid
         }
 }
 
-template <int MINB, bool REFPOW>
+// LEAN: every member in the production configuration (quadratic friction, keep-h, the L2
+// norm; members take rain none or uniform), compiled in as in the stand-alone flat step.
+template <int MINB, bool REFPOW, bool LEAN>
 __global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArgs a, FlatMesh<float> m) {
     if (*a.all_done) return;
     const int lane = threadIdx.x;
@@ -111,11 +113,18 @@ __global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArg
         const GswLoopState* st = a.states + mi;
         if (st->done) continue;                                   // warp-uniform
         const GswMember& mb = a.members[mi];
+        if (LEAN && !(mb.quadratic != 0 && mb.keep_h != 0 && mb.linf == 0)) {   // warp-uniform
+            if (lane == 0) {            // not what this step was compiled for: the member stops
+                a.states[mi].error = GSW_ERR_INVALID;
+                a.states[mi].done = 1;
+            }
+            continue;
+        }
         const FlatPhys<float> ph = member_phys(mb, REFPOW ? 1 : 0);
         const float dt = st->dt_f32;
         const float rate = (mb.rain_kind == GSW_RAIN_UNIFORM) ? mb.rain[st->rain_idx] : 0.0f;
-        unsigned long long lam = flat_brick<float, true, REFPOW>(m, ph, b, seg * m.bh / S, (seg + 1) * m.bh / S, dt, rate,
-                                                         nullptr);
+        unsigned long long lam = flat_brick<float, true, REFPOW, LEAN>(m, ph, b, seg * m.bh / S, (seg + 1) * m.bh / S,
+                                                               dt, rate, nullptr);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const unsigned long long w = __shfl_xor_sync(0xffffffffu, lam, o);
@@ -156,12 +165,18 @@ __global__ void __launch_bounds__(256, MINB) ensemble_step_kernel(GswEnsembleArg
     }
 }
 
+template <bool REFPOW, bool LEAN>
+inline void launch_ensemble_caps(const GswEnsembleArgs* a, const FlatMesh<float>& m, int grid, int W, cudaStream_t st) {
+    if (a->min_blocks == 3) ensemble_step_kernel<3, REFPOW, LEAN><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else if (a->min_blocks == 4) ensemble_step_kernel<4, REFPOW, LEAN><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else if (a->min_blocks == 5) ensemble_step_kernel<5, REFPOW, LEAN><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    else ensemble_step_kernel<1, REFPOW, LEAN><<<grid, dim3(32, W), 0, st>>>(*a, m);
+}
+
 template <bool REFPOW>
 inline void launch_ensemble_shape(const GswEnsembleArgs* a, const FlatMesh<float>& m, int grid, int W, cudaStream_t st) {
-    if (a->min_blocks == 3) ensemble_step_kernel<3, REFPOW><<<grid, dim3(32, W), 0, st>>>(*a, m);
-    else if (a->min_blocks == 4) ensemble_step_kernel<4, REFPOW><<<grid, dim3(32, W), 0, st>>>(*a, m);
-    else if (a->min_blocks == 5) ensemble_step_kernel<5, REFPOW><<<grid, dim3(32, W), 0, st>>>(*a, m);
-    else ensemble_step_kernel<1, REFPOW><<<grid, dim3(32, W), 0, st>>>(*a, m);
+    if (a->lean) launch_ensemble_caps<REFPOW, true>(a, m, grid, W, st);
+    else launch_ensemble_caps<REFPOW, false>(a, m, grid, W, st);
 }
 
 // Launch of the step over checked arguments (outputs non-null).

@@ -92,6 +92,8 @@ class Ensemble:
         self._run = torch.zeros(2 * M + 2, dtype=torch.int64, device=dev)
         self._parity = np.zeros(M, np.int64)       # buffer of each member's current state
         self.warps, self.grid, self.min_blocks, self.segments = int(warps), int(grid), 0, 0
+        # every member in the production configuration: the step compiles it in
+        self.lean = all(m.quad and m.keep_h and not m.cfl_linf for m in members)
         self.kernel_launches = 0
         self._graph_cache = {}
 
@@ -135,6 +137,7 @@ class Ensemble:
         a.members, a.states = _ptr(self._members_dev), _ptr(self._states)
         a.scratch, a.all_done = _ptr(self._scratch), _ptr(self._all_done)
         a.member_brick_off, a.run = _ptr(self._brick_off_dev), _ptr(self._run)
+        a.lean = int(self.lean)
         return a
 
     def _build_members(self, t_end, max_steps, dt_max):
@@ -228,7 +231,7 @@ class Ensemble:
                 L.call("gsw_ensemble_step", C.byref(self._args(src, dst)), st)
             return K
 
-        key = (K, p0, self.warps, self.grid, self.min_blocks, self.segments)
+        key = (K, p0, self.warps, self.grid, self.min_blocks, self.segments, self.lean)
         if key not in self._graph_cache:
             self._graph_cache.clear()
             side = torch.cuda.Stream(device=self.device)
@@ -257,4 +260,7 @@ class Ensemble:
             m.nsteps += n
             if sts[k].error == L.ERR_NONFINITE:
                 raise FloatingPointError(f"ensemble member {k}: non-finite max wave speed at t={m.t:.3f}s")
+            if sts[k].error == L.ERR_INVALID:
+                raise RuntimeError(f"ensemble member {k} was stopped at t={m.t:.3f}s: the step ran compiled for "
+                                   f"the production configuration (Ensemble.lean), which this member does not have")
         return steps

@@ -534,6 +534,10 @@ typedef struct GswEnsembleArgs {
        = the i-th running member. A launch then visits running members' bricks only. */
     const int64_t* member_brick_off;
     int64_t* run;
+    int32_t  lean;               /* 1: every member has quadratic = 1, keep_h = 1 and linf = 0 (the production
+                                    configuration), which the step then compiles in (bit-identical results); a
+                                    member that has not is stopped with states[m].error = GSW_ERR_INVALID.
+                                    0: the general step. */
 } GswEnsembleArgs;
 
 /* Wave speed of every member's current state into states[m].lam_bits (atomicMax). */

@@ -45,7 +45,7 @@ def test_struct_layouts_match_c(tmp_path):
                               "brick_hi"],
               "GswMember": ["dt", "inv_dx", "vcap", "linf", "rain_kind", "rain", "n_tab"],
               "GswEnsembleArgs": ["n_bricks", "n_members", "grid", "brick_ij", "flags", "q0", "bed",
-                                  "members", "states", "scratch", "all_done"],
+                                  "members", "states", "scratch", "all_done", "run", "lean"],
               "GswSeamArgs": ["q0", "nslots", "slot", "pos", "n", "dense", "stride", "scatter", "reserved"]}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{ROOT}/include/gsw.h"', "int main(){"]
     for s, fs in checks.items():
@@ -75,3 +75,25 @@ def test_solver_refuses_without_cuda():
     from geoswe_b200 import Config, Mesh2D, Solver2D
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         Solver2D(Mesh2D(8, 8, 1.0, 1.0, ngh=2), Config(), np.zeros((3, 8, 8)), np.zeros((8, 8)))
+
+
+@pytest.mark.parametrize("lo,hi", [(5, 11), (-1, 3), (6, 4)])
+def test_flat_step_refuses_a_brick_range_outside_the_bricks(lo, hi):
+    """The argument checks of gsw_flat_step run before any device call: a brick range
+    outside [0, n_bricks) is refused with GSW_ERR_INVALID and a message."""
+    from geoswe_b200 import _lib as L
+    a = L.GswFlatArgs()
+    a.abi_version = L.ABI_VERSION
+    a.dtype = L.F32
+    a.brick_h, a.n_bricks, a.warps, a.segments = 16, 10, 4, 1
+    fake = C.c_void_p(0x1000)                 # never dereferenced: the call returns first
+    a.brick_ij = a.brick_nbr = a.flags = fake
+    a.q0 = a.q1 = a.q2 = a.qn0 = a.qn1 = a.qn2 = a.bed = fake
+    a.inv_dx = a.inv_dy = 1.0
+    a.g, a.h_min, a.h_min_cfl = 9.81, 1e-6, 1e-6
+    a.state, a.n_tab, a.n_tab_len = fake, fake, 1
+    a.brick_lo, a.brick_hi = lo, hi
+    lib = L.lib()
+    rc = lib.gsw_flat_step(C.byref(a), None)
+    assert rc == L.ERR_INVALID
+    assert b"brick range" in lib.gsw_last_error()

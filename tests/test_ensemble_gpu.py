@@ -65,3 +65,25 @@ def test_second_run_continues():
     for k, cs in enumerate(alone):
         assert ens.members[k].t == cs.t
         assert same(ens.flat(k, 0).cpu().numpy(), cs.flat(0).cpu().numpy())
+
+
+def test_lean_step_equals_general_step_and_guards_its_premise():
+    """Members in the production configuration take the compiled-in (lean) step; it
+    equals the general step bit for bit. A member outside that configuration in a step
+    forced lean is stopped with an error the host raises, not advanced wrongly."""
+    from geoswe_b200.ensemble import Ensemble
+    lean = Ensemble([_member(*sp) for sp in SPECS[:2]])
+    general = Ensemble([_member(*sp) for sp in SPECS[:2]])
+    assert lean.lean
+    general.lean = False
+    assert lean.run(t_end=400.0, window=8) == general.run(t_end=400.0, window=8)
+    for k in range(2):
+        for c in range(3):
+            assert same(lean.flat(k, c).cpu().numpy(), general.flat(k, c).cpu().numpy()), (k, c)
+    odd = _member(*SPECS[1])
+    odd.cfl_linf = True
+    mixed = Ensemble([_member(*SPECS[0]), odd])
+    assert not mixed.lean
+    mixed.lean = True
+    with pytest.raises(RuntimeError, match="member 1 was stopped"):
+        mixed.run(t_end=100.0, window=8)
