@@ -10,6 +10,9 @@
 //   u = hu / h    -> only where h > h_min (else u = 0, a constant)
 // h^(-4/3) (powf or pow_m43, as the forward step) is differentiated as the exact power,
 // -4/3 h^(-7/3).
+// The forward values are recomputed with the forward step's own operations (so every
+// branch matches); the adjoint arithmetic itself divides once per denominator and
+// multiplies by that reciprocal (a derivative, not a value the forward pass compares).
 #pragma once
 #include "gsw_core.cuh"
 
@@ -66,6 +69,7 @@ __device__ __forceinline__ void hllc_bwd(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
         const T huNK = hK * uNK, huTK = hK * uTK;
         const T D = S - SM + (T)1.0e-30;
         const T fac = (S - uNK) / D;
+        const T rD = (T)1.0 / D;
         const T hKs = hK * fac;
         const T huNKs = hKs * SM;
         const T huTKs = hKs * uTK;
@@ -78,9 +82,10 @@ __device__ __forceinline__ void hllc_bwd(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
         hKs_b += huNKs_b * SM;  SM_b += huNKs_b * hKs;
         hK_b += hKs_b * fac;
         const T fac_b = hKs_b * hK;
-        S_b += fac_b * ((T)1.0 - fac) / D;
-        uNK_b -= fac_b / D;
-        SM_b += fac_b * fac / D;
+        const T facD_b = fac_b * rD;
+        S_b += facD_b * ((T)1.0 - fac);
+        uNK_b -= facD_b;
+        SM_b += facD_b * fac;
         flux_bwd(hK, uNK, uTK, g, Fh_b, FN_b, FT_b, hK_b, uNK_b, uTK_b);   // the K-side flux
         hK_b += huNK_b * uNK + huTK_b * uTK;
         uNK_b += huNK_b * hK;
@@ -93,7 +98,7 @@ __device__ __forceinline__ void hllc_bwd(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
     if (SM_b != z) {
         if (big) {
             const T num_b = SM_b / denom;
-            const T den_b = -(SM_b * SM / denom);
+            const T den_b = -(num_b * SM);
             T dR_b = num_b * SL * hR, dL_b = -(num_b * SR * hL);
             SL_b += num_b * hR * dR;
             hR_b += num_b * SL * dR;
@@ -118,7 +123,7 @@ __device__ __forceinline__ void hllc_bwd(T hL, T uNL, T uTL, T hR, T uNR, T uTR,
         else               { u_st_b += SR_b; a_st_b += SR_b; }
     }
     const T h_st_b = (h_st > z && a_st > z) ? a_st_b * g / (two * a_st) : z;
-    const T h_rt_b = (h_rt > z) ? h_st_b * two * h_rt / g : z;
+    const T h_rt_b = (h_rt > z) ? h_st_b * two * h_rt * ((T)1.0 / g) : z;   // 1/g: loop-invariant
     aL_b += half * h_rt_b; aR_b += half * h_rt_b;
     uNL_b += quarter * h_rt_b; uNR_b -= quarter * h_rt_b;
     uNL_b += half * u_st_b; uNR_b += half * u_st_b;
@@ -195,12 +200,14 @@ __device__ __forceinline__ void srm_face_bwd(const Cell<T>& L, const Cell<T>& R,
     const T Lu_b = XAXIS ? uNL_b : uTL_b, Lv_b = XAXIS ? uTL_b : uNL_b;
     const T Ru_b = XAXIS ? uNR_b : uTR_b, Rv_b = XAXIS ? uTR_b : uNR_b;
     if (L.h > h_min) {
-        Lb.hu += Lu_b / L.h; Lb.hv += Lv_b / L.h;
-        Lh_b -= (Lu_b * L.u + Lv_b * L.v) / L.h;
+        const T r = (T)1.0 / L.h;
+        Lb.hu += Lu_b * r; Lb.hv += Lv_b * r;
+        Lh_b -= (Lu_b * L.u + Lv_b * L.v) * r;
     }
     if (R.h > h_min) {
-        Rb.hu += Ru_b / R.h; Rb.hv += Rv_b / R.h;
-        Rh_b -= (Ru_b * R.u + Rv_b * R.v) / R.h;
+        const T r = (T)1.0 / R.h;
+        Rb.hu += Ru_b * r; Rb.hv += Rv_b * r;
+        Rh_b -= (Ru_b * R.u + Rv_b * R.v) * r;
     }
     Lb.h += Lh_b + Leta_b;
     Rb.h += Rh_b + Reta_b;
@@ -273,12 +280,14 @@ __device__ __forceinline__ void wetdry_friction_bwd(T h1, T hu1, T hv1, T n, T d
     } else {
         n_b = ne_b;
     }
-    T hs_b = h43_b * (-(T)4.0 / (T)3.0) * h43 / hs;
+    const T rhs = (T)1.0 / hs;
+    T hs_b = h43_b * (-(T)4.0 / (T)3.0) * h43 * rhs;
     if (modU > z) {
-        const T u_b = modU_b * u / modU, v_b = modU_b * v / modU;
-        in_b.hu += u_b / hs;
-        in_b.hv += v_b / hs;
-        hs_b -= (u_b * u + v_b * v) / hs;
+        const T rU = modU_b / modU;
+        const T u_b = rU * u, v_b = rU * v;
+        in_b.hu += u_b * rhs;
+        in_b.hv += v_b * rhs;
+        hs_b -= (u_b * u + v_b * v) * rhs;
     }
     if (pass) in_b.h += hs_b;
 }
