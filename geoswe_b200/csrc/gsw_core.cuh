@@ -399,6 +399,23 @@ __device__ __forceinline__ unsigned long long lam_dense_bits(float h, float hu, 
     const bool fin = (hu == hu) && (hv == hv) && (lam <= 3.0e38f) && (aw <= 3.0e38f);
     return fin ? (unsigned long long)__double_as_longlong((double)lam) : 0x7ff0000000000000ull;
 }
+// The same rule as the bits of the binary32 wave speed: unsigned order of the bits of
+// non-negative floats is their order, with +inf (the non-finite case) above every finite
+// value, and widening to binary64 is monotonic, so the maximum of these bits, widened
+// once, equals the maximum of lam_dense_bits over the same cells. A march keeps one
+// 32-bit maximum per thread instead of converting and comparing 64-bit values per cell.
+__device__ __forceinline__ uint32_t lam_dense_bits32(float h, float hu, float hv, float g, float h_cfl) {
+    if (h < h_cfl) return 0u;
+    const float ahu = fabsf(hu), ahv = fabsf(hv);
+    const float aw = div_z(ahu > ahv ? ahu : ahv, h);
+    const float lam = aw + gsqrt(g * h);
+    const bool fin = (hu == hu) && (hv == hv) && (lam <= 3.0e38f) && (aw <= 3.0e38f);
+    return fin ? __float_as_uint(lam) : 0x7f800000u;
+}
+__device__ __forceinline__ unsigned long long lam_bits_of32(uint32_t b) {
+    return (unsigned long long)__double_as_longlong((double)__uint_as_float(b));
+}
+
 // Dense loop, fp64 (the generic path, solver.py:2668-2693 with swe.max_wave_speed_2d):
 // every cell counts, u = 0 where h <= h_cfl else hu/max(h, h_cfl), c = sqrt(g max(h,0)).
 // The all-dry floor sqrt(g h_cfl) is applied by gsw_dt_finalize, so whether cells below

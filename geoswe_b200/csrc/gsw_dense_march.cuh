@@ -114,6 +114,7 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
     const int i0 = p.row_lo + blockIdx.y * p.tile_rows;
     const int i1 = min(i0 + p.tile_rows, p.row_hi);
     unsigned long long lam_local = 0ull;
+    uint32_t lam32 = 0u;        // binary32: the bits of the largest wave speed (lam_dense_bits32)
 
     T dt = (T)0;
     T rate = (T)0;
@@ -217,8 +218,12 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
                         const bool skip = !LEAN && (p.cfl_skip != nullptr) &&
                             p.cfl_skip[(int64_t)(r - p.ngh) * (p.nyp - 2 * p.ngh) + (c - p.ngh)] != 0;
                         if (!skip) {
-                            const unsigned long long lb = lam_dense_bits(h, hu, hv, p.g, p.h_cfl);
-                            lam_local = lb > lam_local ? lb : lam_local;
+                            if constexpr (sizeof(T) == 4) {
+                                lam32 = max(lam32, lam_dense_bits32(h, hu, hv, p.g, p.h_cfl));
+                            } else {
+                                const unsigned long long lb = lam_dense_bits(h, hu, hv, p.g, p.h_cfl);
+                                lam_local = lb > lam_local ? lb : lam_local;
+                            }
                         }
                     }
                 }
@@ -227,6 +232,7 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
             b_next = b_p2;
         }
     }
+    if constexpr (sizeof(T) == 4) lam_local = lam_bits_of32(lam32);
     if (STEP && (LEAN || p.lam != nullptr)) block_max_to(lam_local, p.lam);
 }
 
