@@ -93,7 +93,8 @@ class GswFlatArgs(C.Structure):
 class GswFlatInflowArgs(C.Structure):
     _fields_ = [("abi_version", u32), ("dtype", i32), ("q0", vp), ("q1", vp), ("q2", vp), ("bed", vp),
                 ("ghost_slot", vp), ("nbr_slot", vp), ("n", i32), ("n_knots", i32), ("nx_n", f64),
-                ("ny_n", f64), ("ds", f64), ("t_knots", vp), ("q_knots", vp), ("state", vp), ("hsum", vp)]
+                ("ny_n", f64), ("ds", f64), ("t_knots", vp), ("q_knots", vp), ("state", vp), ("hsum", vp),
+                ("dry", vp)]
 
 
 class GswFlatAdjArgs(C.Structure):

@@ -89,6 +89,34 @@ def build_bricks(stored_pad: np.ndarray, brick_h: int):
     return bij, bnbr
 
 
+def inlet_dry_reductions(zb, halo, device):
+    """The dry-inlet seed's reductions over the ranks of a split run, as the reference
+    makes them once (compressed_solver.py:1559-1594): for each inlet (zb[k], this rank's
+    float32 bed values of its cells, possibly none), the bed minimum and maximum over
+    every rank (one MIN all-reduce of (zmin, -zmax)), then the cells at that minimum (a
+    SUM) and the largest seed depth max(seed - z, 0) with seed = float32(zmin + 0.10
+    (zmax - zmin)) (a MAX). Returns one (zmin, zmax, nlow, hmax) per inlet; a rank
+    without cells of an inlet contributes the neutral values."""
+    n = len(zb)
+    ext = torch.tensor([[float(z.min()), -float(z.max())] if z.size else [np.inf, np.inf] for z in zb],
+                       dtype=torch.float64, device=device).reshape(n, 2)
+    halo.allreduce_min_(ext)                              # NCCL reduces device tensors
+    ext = ext.cpu()
+    agg_n = torch.zeros(n, dtype=torch.float64)
+    agg_h = torch.full((n,), -np.inf, dtype=torch.float64)
+    for k, z in enumerate(zb):
+        zmin, zmax = float(ext[k, 0]), -float(ext[k, 1])
+        seed = np.float32(zmin + 0.10 * (zmax - zmin))        # the kernel's double arithmetic
+        if z.size:
+            agg_n[k] = float(np.count_nonzero(z <= np.float32(zmin)))
+            agg_h[k] = float(np.maximum(seed - z, np.float32(0.0)).max())
+    agg_n, agg_h = agg_n.to(device), agg_h.to(device)
+    halo.allreduce_sum_(agg_n)
+    halo.allreduce_max_(agg_h)
+    agg_n, agg_h = agg_n.cpu(), agg_h.cpu()
+    return [(float(ext[k, 0]), -float(ext[k, 1]), float(agg_n[k]), float(agg_h[k])) for k in range(n)]
+
+
 class CompressedSolver:
     """Shallow-water solver on the compressed active-cell mesh (GPU, float32).
 
@@ -695,6 +723,16 @@ class CompressedSolver:
         a.state = _ptr(self._state)
         return a
 
+    def _inlet_dry_seeds(self):
+        """Each inlet's dry-seed reductions over the ranks (inlet_dry_reductions), once per
+        inlet list (the bed does not change), kept with the inlet as `dry` for the apply
+        kernel."""
+        if all("dry" in f for f in self._inflows):
+            return
+        zb = [self._b[f["nbr"]].cpu().numpy().astype(np.float32) for f in self._inflows]
+        for f, d in zip(self._inflows, inlet_dry_reductions(zb, self.halo, self.device)):
+            f["dry"] = torch.tensor(d, dtype=torch.float64, device=self.device)
+
     def _inflow_args(self, f, q, hsum=None):
         a = L.GswFlatInflowArgs()
         a.abi_version = L.ABI_VERSION
@@ -705,6 +743,7 @@ class CompressedSolver:
         a.t_knots, a.q_knots, a.n_knots = _ptr(f["t"]), _ptr(f["q"]), int(f["t"].numel())
         a.state = _ptr(self._state)
         a.hsum = hsum
+        a.dry = _ptr(f["dry"]) if "dry" in f else None
         return a
 
     # ---------------------------------------------------------------- views
@@ -869,6 +908,7 @@ class CompressedSolver:
             self.halo.check_same(len(self._inflows), "CompressedSolver: discharge inlets")
             if self._inflows:
                 inlet_sums = torch.zeros(len(self._inflows), dtype=torch.float64, device=self.device)
+                self._inlet_dry_seeds()
         K = int(window) if window else self._window_size()
         if split and not window:
             K = min(K, 32)     # launched eagerly: poll often, so few no-op steps follow the end

@@ -75,6 +75,14 @@ __device__ __forceinline__ T div_z(T a, T b) {
     const T q = one_if(zr, a) / b;
     return zr ? a * b : q;
 }
+// a / b where b is never zero (a wet/dry floor h_min > 0 or a depth above it): only the
+// dividend needs the zero test, and b's finiteness (0 / inf is 0, 0 * inf is not).
+template <typename T>
+__device__ __forceinline__ T div_znz(T a, T b) {
+    const bool zr = (a == (T)0) && (gabs(b) < (T)INFINITY);
+    const T q = one_if(zr, a) / b;
+    return zr ? a * b : q;
+}
 // Binary32, the whole guard in one asm block: the zero test feeds both selects as a
 // predicate, where the forms above pass it through an integer register (a select and
 // an integer compare more per guard, 14 guards per cell). sqrt.rn and div.rn are the
@@ -105,6 +113,20 @@ __device__ __forceinline__ float div_z<float>(float a, float b) {
         : "=f"(r) : "f"(a), "f"(b));
     return r;
 }
+template <>
+__device__ __forceinline__ float div_znz<float>(float a, float b) {
+    float r;
+    asm("{\n\t.reg .pred p;\n\t.reg .f32 t, m;\n\t"
+        "abs.f32 m, %2;\n\t"
+        "setp.eq.f32 p, %1, 0f00000000;\n\t"
+        "setp.lt.and.f32 p, m, 0f7F800000, p;\n\t"
+        "selp.f32 t, 0f3F800000, %1, p;\n\t"
+        "div.rn.f32 t, t, %2;\n\t"
+        "mul.rn.f32 m, %1, %2;\n\t"
+        "selp.f32 %0, m, t, p;\n\t}"
+        : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
 #else
 // Fast arithmetic (gsw_fast.cu, compiled with FMA contraction and flush-to-zero):
 // binary32 square root and division by the hardware approximations, sqrt.approx
@@ -122,8 +144,10 @@ __device__ __forceinline__ float gdiv(float a, float b) {
 }
 __device__ __forceinline__ float  sqrt_z(float x) { return gsqrt(x); }
 __device__ __forceinline__ float  div_z(float a, float b) { return gdiv(a, b); }
+__device__ __forceinline__ float  div_znz(float a, float b) { return gdiv(a, b); }
 __device__ __forceinline__ double sqrt_z(double x) { return x == 0.0 ? x : sqrt(x); }
 __device__ __forceinline__ double div_z(double a, double b) { return a / b; }
+__device__ __forceinline__ double div_znz(double a, double b) { return a / b; }
 #endif
 
 // q = h / g for the HLLC star depth, by the constant's reciprocal when the library has
@@ -161,8 +185,8 @@ struct Cell {
 template <typename T>
 __device__ __forceinline__ void make_prims(Cell<T>& c, T h_min) {
     const T hs = (c.h > h_min) ? c.h : h_min;
-    c.u = (c.h > h_min) ? div_z(c.hu, hs) : Real<T>::zero();
-    c.v = (c.h > h_min) ? div_z(c.hv, hs) : Real<T>::zero();
+    c.u = (c.h > h_min) ? div_znz(c.hu, hs) : Real<T>::zero();   // hs = h > h_min >= 0 where used
+    c.v = (c.h > h_min) ? div_znz(c.hv, hs) : Real<T>::zero();
     c.eta = c.h + c.b;
 }
 
@@ -361,8 +385,8 @@ __device__ __forceinline__ void wetdry_friction(T& h, T& hu, T& hv, bool frictio
     }
     if (!friction) return;
     const T hs = (h > h_min) ? h : h_min;
-    const T u = div_z(hu, hs);
-    const T v = div_z(hv, hs);
+    const T u = div_znz(hu, hs);      // hs >= h_min > 0
+    const T v = div_znz(hv, hs);
     const T modU = sqrt_z(u * u + v * v);
     const T h43 = ref_pow ? pow_m43_ref(hs) : pow_m43(hs);
     if (modU > vcap) {
@@ -394,7 +418,7 @@ __device__ __forceinline__ unsigned long long lam_dense_bits(float h, float hu, 
     // monotonic and symmetric, so it equals max(|hu|, |hv|) / h to the bit (NaN momentum
     // is tested on its own; a NaN or infinite h leaves the quotient non-finite)
     const float ahu = fabsf(hu), ahv = fabsf(hv);
-    const float aw = div_z(ahu > ahv ? ahu : ahv, h);
+    const float aw = div_znz(ahu > ahv ? ahu : ahv, h);       // h >= h_cfl > 0, or NaN
     const float lam = aw + gsqrt(g * h);
     const bool fin = (hu == hu) && (hv == hv) && (lam <= 3.0e38f) && (aw <= 3.0e38f);
     return fin ? (unsigned long long)__double_as_longlong((double)lam) : 0x7ff0000000000000ull;
@@ -407,7 +431,7 @@ __device__ __forceinline__ unsigned long long lam_dense_bits(float h, float hu, 
 __device__ __forceinline__ uint32_t lam_dense_bits32(float h, float hu, float hv, float g, float h_cfl) {
     if (h < h_cfl) return 0u;
     const float ahu = fabsf(hu), ahv = fabsf(hv);
-    const float aw = div_z(ahu > ahv ? ahu : ahv, h);
+    const float aw = div_znz(ahu > ahv ? ahu : ahv, h);       // h >= h_cfl > 0, or NaN
     const float lam = aw + gsqrt(g * h);
     const bool fin = (hu == hu) && (hv == hv) && (lam <= 3.0e38f) && (aw <= 3.0e38f);
     return fin ? __float_as_uint(lam) : 0x7f800000u;
@@ -446,10 +470,10 @@ __device__ __forceinline__ unsigned long long lam_flat_bits(float h, float hu, f
     float speed;
     if (linf) {   // one division, as in lam_dense_bits (fmaxf ignores a NaN operand, as before)
         const float ahu = (hu == hu) ? fabsf(hu) : 0.0f, ahv = (hv == hv) ? fabsf(hv) : 0.0f;
-        speed = div_z(ahu > ahv ? ahu : ahv, hs);
+        speed = div_znz(ahu > ahv ? ahu : ahv, hs);             // hs >= h_min_cfl > 0
         if (hu != hu && hv != hv) speed = __int_as_float(0x7fffffff);
     } else {
-        const float u = div_z(hu, hs), v = div_z(hv, hs);
+        const float u = div_znz(hu, hs), v = div_znz(hv, hs);
         speed = sqrt_z(u * u + v * v);
     }
     const float l = speed + c;

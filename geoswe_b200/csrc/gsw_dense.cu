@@ -243,6 +243,8 @@ extern "C" int gsw_stage_apply(const GswStageArgs* a, void* stream) {
     if (a->n_cells <= 0) return GSW_OK;
     if (!a->cell_off || !a->bed64 || !a->time_s || !a->stage_m || a->n_knots < 1 || !a->state)
         return set_error(GSW_ERR_INVALID, "stage: null table or state");
+    if (a->lam_target && !(a->h_cfl > 0.0))
+        return set_error(GSW_ERR_INVALID, "stage: h_cfl (%g) must be > 0 (the wave speed's divisor floor)", a->h_cfl);
     cudaStream_t s = (cudaStream_t)stream;
     const int grid = std::min(sm_count() * 4, (a->n_cells + 255) / 256);
     if (a->dtype == GSW_F32) stage_kernel<float><<<grid, 256, 0, s>>>(*a);

@@ -154,6 +154,14 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
                       // flat march with either arithmetic, slow down)
 #endif
         for (int r = i0; r < i1; ++r) {
+            // the update's class id and running maximum, loaded before the faces so that
+            // their latency is hidden (the production kernel; the general one loads late)
+            uint8_t cls_r = 0;
+            T mh_r = (T)0;
+            if (LEAN && STEP && out_lane) {
+                cls_r = p.ncls[(int64_t)r * p.cpitch + c];
+                if (p.max_h != nullptr) mh_r = p.max_h[(int64_t)r * p.pitch + c];
+            }
             nx.h = pf_h; nx.hu = pf_hu; nx.hv = pf_hv;
             nx.b = b_next;
             const T b_p2 = pf_b;
@@ -206,14 +214,15 @@ __global__ void __launch_bounds__(256, MINB) dense_march_kernel(DenseK<T> p) {
                     T hu = ldg_at(p.q1, p.pitch, r, c) + dt * rhu;     // reloaded: not carried down the march
                     T hv = ldg_at(p.q2, p.pitch, r, c) + dt * rhv;
                     T n = (T)0;
-                    if (LEAN) n = p.ntab[p.ncls[(int64_t)r * p.cpitch + c]];
+                    if (LEAN) n = p.ntab[cls_r];
                     else if (p.friction_kind == GSW_FRICTION_TABLE)
                         n = p.ncls ? p.ntab[p.ncls[(int64_t)r * p.cpitch + c]] : p.ntab[0];
                     else if (p.friction_kind == GSW_FRICTION_FIELD) n = p.nfield[o];
                     wetdry_friction<T>(h, hu, hv, LEAN || p.friction_kind != GSW_FRICTION_NONE, n, dt, p.g,
                                        p.h_min, p.vcap, LEAN || p.quad != 0, LEAN || p.keep_h != 0, REFPOW);
                     p.o0[o] = h; p.o1[o] = hu; p.o2[o] = hv;
-                    if (p.max_h != nullptr && h > p.max_h[o]) p.max_h[o] = h;
+                    if (LEAN) { if (p.max_h != nullptr && h > mh_r) p.max_h[o] = h; }
+                    else if (p.max_h != nullptr && h > p.max_h[o]) p.max_h[o] = h;
                     if (LEAN || p.lam != nullptr) {
                         const bool skip = !LEAN && (p.cfl_skip != nullptr) &&
                             p.cfl_skip[(int64_t)(r - p.ngh) * (p.nyp - 2 * p.ngh) + (c - p.ngh)] != 0;
@@ -266,6 +275,8 @@ inline int fill_dense(const GswDenseArgs* a, DenseK<T>& k, bool step) {
         const T dx = (T)1 / k.inv_dx, dy = (T)1 / k.inv_dy;
         k.half_dx = (T)0.5 * dx; k.half_dy = (T)0.5 * dy;
     }
+    if (!(a->h_min > 0.0) || !(a->h_cfl > 0.0))     // both are divisor floors of the step
+        return set_error(GSW_ERR_INVALID, "dense: h_min (%g) and h_cfl (%g) must be > 0", a->h_min, a->h_cfl);
     k.g = (T)a->g; k.h_min = (T)a->h_min;
     k.g_recip = sizeof(T) == 4 ? (T)div_const_recip((float)a->g) : (T)0;
     k.st = a->state; k.lam = (unsigned long long*)a->lam_target;

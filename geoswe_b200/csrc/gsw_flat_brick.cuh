@@ -149,6 +149,16 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
     srm_face<T, true>(cur, nx, ph.half_dx, ph.inv_dx, ph.g, ph.h_min, Wf, ph.g_recip);
     cur = nx;
     for (int r = r0; r < r1; ++r) {
+        // the update's slot flag, class id and running maximum, loaded before the faces so
+        // that their latency is hidden (the production kernel; the general one loads late)
+        uint8_t f_r = 0, cls_r = 0;
+        T mh_r = (T)0;
+        if (LEAN && STEP && lane >= 1 && lane <= 30) {
+            const int64_t o = bidx * v.BS + (int64_t)r * GSW_BRICK_PITCH + (lane - 1);
+            f_r = m.flags[o];
+            if (m.ncls) cls_r = m.ncls[o];
+            if (m.max_h != nullptr) mh_r = m.max_h[o];
+        }
         nx.h = pf_h; nx.hu = pf_hu; nx.hv = pf_hv;
         nx.b = b_next;
         const T b_p2 = pf_b;
@@ -183,7 +193,7 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
         }
         if (lane >= 1 && lane <= 30) {
             const int64_t o = bidx * v.BS + (int64_t)r * GSW_BRICK_PITCH + (lane - 1);
-            const uint8_t f = m.flags[o];
+            const uint8_t f = (LEAN && STEP) ? f_r : m.flags[o];
             if (f & GSW_SLOT_STORED) {
                 const bool active = (f & GSW_SLOT_ACTIVE) != 0;
                 if (!STEP) {
@@ -191,7 +201,7 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
                     m.o0[o] = rh; m.o1[o] = rhu; m.o2[o] = rhv;
                 } else if (!active) {
                     m.o0[o] = cur.h; m.o1[o] = __ldg(m.q1 + o); m.o2[o] = __ldg(m.q2 + o);
-                    if (m.max_h != nullptr && cur.h > m.max_h[o]) m.max_h[o] = cur.h;
+                    if (m.max_h != nullptr && cur.h > (LEAN ? mh_r : m.max_h[o])) m.max_h[o] = cur.h;
                 } else {
                     T rr0 = rh;
                     if (ph.rain_kind == GSW_RAIN_UNIFORM) rr0 = rr0 + rate;
@@ -204,11 +214,11 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
                     T h = cur.h + dt * rr0;
                     T hu = __ldg(m.q1 + o) + dt * rhu;       // reloaded: not carried down the march
                     T hv = __ldg(m.q2 + o) + dt * rhv;
-                    const T n = m.ncls ? ph.ntab[m.ncls[o]] : ph.ntab[0];
+                    const T n = m.ncls ? ph.ntab[LEAN ? cls_r : m.ncls[o]] : ph.ntab[0];
                     wetdry_friction<T>(h, hu, hv, true, n, dt, ph.g, ph.h_min, ph.vcap,
                                        LEAN || ph.quad != 0, LEAN || ph.keep_h != 0, REFPOW);
                     m.o0[o] = h; m.o1[o] = hu; m.o2[o] = hv;
-                    if (m.max_h != nullptr && h > m.max_h[o]) m.max_h[o] = h;
+                    if (m.max_h != nullptr && h > (LEAN ? mh_r : m.max_h[o])) m.max_h[o] = h;
                     const unsigned long long lb = lam_flat_bits(h, hu, hv, ph.g, ph.h_min, ph.h_min_cfl,
                                                                 !LEAN && ph.linf != 0);
                     lam_local = lb > lam_local ? lb : lam_local;

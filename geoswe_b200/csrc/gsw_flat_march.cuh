@@ -49,6 +49,8 @@ inline int fill_flat(const GswFlatArgs* a, FlatK<T>& k, bool step) {
     FlatPhys<T>& ph = k.ph;
     ph.inv_dx = (T)a->inv_dx; ph.inv_dy = (T)a->inv_dy;
     ph.half_dx = (T)0.5 * ((T)1 / ph.inv_dx); ph.half_dy = (T)0.5 * ((T)1 / ph.inv_dy);
+    if (!(a->h_min > 0.0) || !(a->h_min_cfl > 0.0))  // both are divisor floors of the step
+        return set_error(GSW_ERR_INVALID, "flat: h_min (%g) and h_min_cfl (%g) must be > 0", a->h_min, a->h_min_cfl);
     ph.g = (T)a->g; ph.h_min = (T)a->h_min; ph.h_min_cfl = (T)a->h_min_cfl; ph.vcap = (T)a->vcap;
     ph.linf = a->linf; ph.quad = a->quadratic; ph.keep_h = a->keep_h;
     ph.rain_kind = a->rain_kind; ph.rain = (const T*)a->rain; ph.ngh = a->ngh; ph.nx = a->nx; ph.ny = a->ny;

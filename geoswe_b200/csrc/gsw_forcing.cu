@@ -108,7 +108,13 @@ __global__ void flat_inflow_kernel(GswFlatInflowArgs a) {
         s_Q = np_interp(a.state->t, a.t_knots, a.q_knots, a.n_knots);
         s_sum = a.hsum != nullptr ? *a.hsum : (double)pairwise_sum<T>(q0, a.nbr_slot, 0, a.n);
         s_wet = s_sum > 0.0;
-        if (!s_wet) {
+        if (!s_wet && a.dry != nullptr) {       // the seed's reductions over every rank's cells
+            const double zlo = a.dry[0], zhi = a.dry[1];
+            s_seed = (T)__dadd_rn(zlo, __dmul_rn(0.10, __dsub_rn(zhi, zlo)));
+            s_zmin = zlo;
+            s_nlow = a.dry[2] > 0.0 ? a.dry[2] : 1.0;
+            s_flat = !(a.dry[3] > 0.0);
+        } else if (!s_wet) {
             T zmin = bed[a.nbr_slot[0]], zmax = zmin;
             for (int k = 1; k < a.n; ++k) {
                 const T z = bed[a.nbr_slot[k]];
@@ -130,6 +136,8 @@ __global__ void flat_inflow_kernel(GswFlatInflowArgs a) {
             s_zmin = zlo;
             s_nlow = nlow > 0 ? (double)nlow : 1.0;
             s_flat = !((double)hmax > 0.0);
+        }
+        if (!s_wet) {
             s_add = 0.0;
             if (s_flat) {
                 const double qc = __ddiv_rn(fabs(s_Q), __dmul_rn(s_nlow, a.ds));

@@ -172,7 +172,7 @@ typedef struct GswDenseArgs {
     int32_t  keep_h;           /* 1: dry cells keep max(h,0) (default), 0: h = 0 */
     void*    max_h;            /* running max depth, pitch = pitch, or NULL */
     const uint8_t* cfl_skip;   /* interior (nx, ny) C-order: 1 = excluded from the wave speed */
-    double   h_cfl;            /* wave-speed wet threshold (and divisor) */
+    double   h_cfl;            /* wave-speed wet threshold (and divisor), > 0; h_min > 0 too */
     int32_t  tile_rows;        /* rows per warp strip; 0: the largest of 32, 16, 8, 4 that gives at least
                                   twice the warps the GPU runs at once */
     int32_t  warps;            /* warps per block (0: default 4) */
@@ -295,7 +295,8 @@ typedef struct GswFlatArgs {
     const void* q0; const void* q1; const void* q2;   /* state in, slot-indexed */
     void* qn0; void* qn1; void* qn2;                  /* state out (step) / residual (rhs) */
     const void* bed;
-    double   inv_dx, inv_dy, g, h_min, h_min_cfl;     /* rounded to dtype by the kernels */
+    double   inv_dx, inv_dy, g, h_min, h_min_cfl;     /* rounded to dtype by the kernels; h_min and
+                                                         h_min_cfl (divisor floors) > 0 */
     int32_t  linf;             /* 1: CFL norm max(|u|,|v|); 0: sqrt(u^2+v^2) */
     /* step only */
     int32_t  rain_kind;        /* GSW_RAIN_NONE / UNIFORM / GRIDDED / LOOKUP */
@@ -345,6 +346,11 @@ typedef struct GswFlatInflowArgs {
                                      depth sum over every rank of a split run (the per-rank sums of
                                      gsw_flat_inflow_depth_sum added by an all-reduce), as the
                                      reference's split loop does (geoswe/compressed_solver.py:2145-2153) */
+    const double* dry;            /* device; NULL: the dry-inlet seed's bed range and counts come from the
+                                     cells above. Non-NULL: 4 doubles {zmin, zmax, nlow, hmax} over every
+                                     rank's cells of the inlet (bed minimum and maximum, cells at the
+                                     minimum, largest seed depth), as the reference reduces them once over
+                                     the ranks (geoswe/compressed_solver.py:1559-1594) */
 } GswFlatInflowArgs;
 GSW_API int gsw_flat_inflow_apply(const GswFlatInflowArgs* a, void* stream);
 /* *out = this rank's depth sum over the inlet's active neighbours (the pairwise float sum
@@ -491,7 +497,7 @@ GSW_API int gsw_gauge_adjoint(const GswGaugeArgs* a, void* stream);
 /* Physics and time-step rule of one member. */
 typedef struct GswMember {
     GswDtParams dt;          /* the member's flat time-step rule (rain limit folded into dt_max) */
-    float    inv_dx, g, h_min, h_min_cfl, vcap;
+    float    inv_dx, g, h_min, h_min_cfl, vcap;    /* h_min, h_min_cfl > 0 (divisor floors) */
     int32_t  linf, quadratic, keep_h;
     int32_t  rain_kind;      /* GSW_RAIN_NONE or GSW_RAIN_UNIFORM */
     float    g_recip;        /* gsw_div_const_recip(g), or 0 (the star depth's h / g divides) */

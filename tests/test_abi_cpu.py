@@ -39,7 +39,7 @@ def test_struct_layouts_match_c(tmp_path):
               "GswBcArgs": ["pitch", "kinds", "state"],
               "GswStageArgs": ["pitch", "bed_is_f32", "time_s", "lam_target", "g", "h_cfl"],
               "GswInflowArgs": ["pitch", "step_off", "nx_n", "t_knots", "state", "hsum"],
-              "GswFlatInflowArgs": ["n_knots", "nx_n", "t_knots", "state", "hsum"],
+              "GswFlatInflowArgs": ["n_knots", "nx_n", "t_knots", "state", "hsum", "dry"],
               "GswFlatArgs": ["n_bricks", "flags", "bed", "inv_dx", "h_min_cfl", "linf", "state", "rain",
                               "ny", "n_tab_len", "vcap", "keep_h", "max_h", "warps", "segments", "brick_lo",
                               "brick_hi"],
@@ -97,3 +97,31 @@ def test_flat_step_refuses_a_brick_range_outside_the_bricks(lo, hi):
     rc = lib.gsw_flat_step(C.byref(a), None)
     assert rc == L.ERR_INVALID
     assert b"brick range" in lib.gsw_last_error()
+
+
+@pytest.mark.parametrize("h_min,h_cfl", [(0.0, 1e-6), (1e-6, 0.0), (-1e-6, 1e-6), (float("nan"), 1e-6)])
+def test_step_refuses_a_divisor_floor_that_is_not_positive(h_min, h_cfl):
+    """h_min and the wave speed's h_cfl floor the step's divisors, so the dense and flat
+    steps refuse a value that is not > 0 (before any device call)."""
+    from geoswe_b200 import _lib as L
+    lib = L.lib()
+    fake = C.c_void_p(0x1000)                 # never dereferenced: the call returns first
+    d = L.GswDenseArgs()
+    d.abi_version, d.dtype = L.ABI_VERSION, L.F32
+    d.nxp = d.nyp = d.pitch = 16
+    d.ngh, d.tile_rows, d.warps = 2, 4, 4
+    d.q0 = d.q1 = d.q2 = d.qn0 = d.qn1 = d.qn2 = d.bed = d.state = fake
+    d.inv_dx = d.inv_dy = 1.0
+    d.g, d.h_min, d.h_cfl = 9.81, h_min, h_cfl
+    assert lib.gsw_dense_step(C.byref(d), None) == L.ERR_INVALID
+    assert b"must be > 0" in lib.gsw_last_error()
+    f = L.GswFlatArgs()
+    f.abi_version, f.dtype = L.ABI_VERSION, L.F32
+    f.brick_h, f.n_bricks, f.warps, f.segments = 16, 4, 4, 1
+    f.brick_ij = f.brick_nbr = f.flags = fake
+    f.q0 = f.q1 = f.q2 = f.qn0 = f.qn1 = f.qn2 = f.bed = f.state = f.n_tab = fake
+    f.n_tab_len = 1
+    f.inv_dx = f.inv_dy = 1.0
+    f.g, f.h_min, f.h_min_cfl = 9.81, h_min, h_cfl
+    assert lib.gsw_flat_step(C.byref(f), None) == L.ERR_INVALID
+    assert b"must be > 0" in lib.gsw_last_error()

@@ -226,6 +226,46 @@ def test_inlet_sums_and_counts_over_ranks():
         assert "differ across ranks" in out[r][2] and "between 2 and 3" in out[r][2]
 
 
+def _dry_bed(k, rank):
+    """Inlet k's bed values on `rank` (inlet 1 has no cells on rank 1; inlet 2 is flat)."""
+    rng = np.random.default_rng(100 * k + rank)
+    if k == 1 and rank == 1:
+        return np.zeros(0, np.float32)
+    if k == 2:
+        return np.full(3 + rank, 7.25, np.float32)
+    return (5.0 + rng.random(4 + 3 * rank) * 2.0).astype(np.float32)
+
+
+def _dry_seed_local(z):
+    """The single-domain kernel's dry seed reductions over all of an inlet's cells."""
+    zmin, zmax = float(z.min()), float(z.max())
+    seed = np.float32(zmin + 0.10 * (zmax - zmin))
+    return zmin, zmax, float(np.count_nonzero(z <= np.float32(zmin))), float(np.maximum(seed - z, 0).max())
+
+
+def _dry_seed_rank(rank, world, port, out):
+    _init(rank, world, port)
+    try:
+        from geoswe_b200.compressed import inlet_dry_reductions
+        h = Halo2D(None, 20, 10, G, dtype="float32", dims=[world, 1])
+        out[rank] = inlet_dry_reductions([_dry_bed(k, rank) for k in range(3)], h, torch.device("cpu"))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_inlet_dry_seed_reductions_over_ranks():
+    """A dry inlet's seed (bed range, cells at the minimum, largest seed depth) is reduced
+    over every rank's cells, as the reference does once at setup: two ranks give the
+    values the single-domain kernel computes from all the cells, including an inlet
+    with no cells on one rank and a flat one."""
+    out = _spawn(_dry_seed_rank, 2)
+    for k in range(3):
+        want = _dry_seed_local(np.concatenate([_dry_bed(k, r) for r in range(2)]))
+        for r in range(2):
+            assert out[r][k] == want, (k, r, out[r][k], want)
+    assert out[0][2][3] == 0.0                     # the flat inlet: no seed depth anywhere
+
+
 # ------------------------------------------------------------------ split oracle run
 NSTEPS = 25
 

@@ -306,3 +306,75 @@ def test_split_compressed_run_with_forcings_and_checkpoints(tmp_path):
         x0, x1, y0, y1 = o["block"]
         assert o["nsteps"] == ref_steps and o["t"] == ref.t, (r, o["nsteps"], ref_steps, o["t"], ref.t)
         np.testing.assert_array_equal(o["depth"], want[x0:x1, y0:y1])
+
+
+def _seam_inlet_compressed(z, mask, cls_pad, table, block, **kw):
+    """The compressed rain run of `block` with one discharge inlet along the top edge of
+    the active set, global padded columns [30, 64): across the y seam of a [1, 2] split."""
+    from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
+    from geoswe_b200.compressed import CompressedSolver
+    x0, x1, y0, y1 = block
+    s = Solver2D(Mesh2D(nx=x1 - x0, ny=y1 - y0, dx=CDX, dy=CDX, ngh=2),
+                 Config(bc_x="fall", bc_y="fall", friction="manning"),
+                 np.zeros((3, x1 - x0, y1 - y0), np.float32), z[x0:x1, y0:y1].copy(), **kw)
+    s.set_inside_mask(mask[x0:x1, y0:y1])
+    s.set_manning_table(cls_pad[x0:x1 + 4, y0:y1 + 4].copy(), table)
+    cs = CompressedSolver.from_dense(s)
+    cs.set_rain(RainfallForcing(time_s=[0.0, 300.0, 1e9], rate_mm_h=[60.0, 25.0, 25.0]))
+    ij = cs.ij_active
+    gi, gj = ij[:, 0] + x0, ij[:, 1] + y0
+    own = (ij[:, 0] >= 2) & (ij[:, 0] < 2 + x1 - x0) & (ij[:, 1] >= 2) & (ij[:, 1] < 2 + y1 - y0)
+    g, a = cs.ghost_boundary_pairs()
+    pick = ((ij[a, 0] == ij[g, 0] + 1) & (ij[a, 1] == ij[g, 1]) & own[g] & (gi[g] < 20)
+            & (gj[g] >= 30) & (gj[g] < 64))
+    cs.add_inflow(g[pick], a[pick], (1.0, 0.0), CDX, [0.0, 300.0, 900.0], [0.0, 4.0, 1.0])
+    steps = cs.run(t_end=C_T_END)
+    return cs, steps, int(pick.sum())
+
+
+def _seam_inlet_rank(rank, world, port, out, dims):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        torch.cuda.set_device(0)
+        from geoswe_b200.partition import block_of
+        z, mask, cls_pad, table = _compressed_inputs()
+        block = block_of(CNX, CNY, dims, (rank // dims[1], rank % dims[1]))
+        cs, steps, n = _seam_inlet_compressed(z, mask, cls_pad, table, block, comm=dist.group.WORLD, dims=dims)
+        out[rank] = dict(block=block, steps=steps, t=cs.t, depth=cs.depth(), n=n)
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_split_compressed_inlet_across_the_seam():
+    """A compressed inlet with cells on both ranks, starting dry: its dry seed (bed range,
+    cells at the minimum, largest seed depth) is reduced over the ranks once, as the
+    reference does, so the dry phase equals the single-domain run; once wet, each rank
+    sums its cells' depths and one all-reduce adds the two partial sums in double, while
+    the single-domain run sums all cells in float (as the reference's split and single
+    runs do), so the inlet weights differ in the last bit and the difference grows over
+    the run's ~7500 wet/dry steps: the run is held to the same steps, the same volume
+    to 1e-4, and depths within 1 cm (RMSE 1 mm). An inlet inside one rank is bitwise
+    (the test above)."""
+    z, mask, cls_pad, table = _compressed_inputs()
+    ref, ref_steps, n = _seam_inlet_compressed(z, mask, cls_pad, table, (0, CNX, 0, CNY))
+    want = ref.depth()
+    torch.cuda.synchronize()
+    dims = [1, 2]
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_seam_inlet_rank, args=(2, _free_port(), out, dims), nprocs=2,
+                           start_method="spawn", join=True)
+        out = dict(out)
+    assert ref_steps > 20 and n > 0
+    assert out[0]["n"] > 0 and out[1]["n"] > 0 and out[0]["n"] + out[1]["n"] == n
+    for r in range(2):
+        o = out[r]
+        x0, x1, y0, y1 = o["block"]
+        assert o["steps"] == ref_steps and o["t"] == ref.t, (r, o["steps"], ref_steps)
+        d = o["depth"].astype(np.float64) - want[x0:x1, y0:y1]
+        assert np.abs(d).max() <= 1e-2 and np.sqrt(np.mean(d * d)) <= 1e-3, (r, np.abs(d).max())
+    vol = sum(float(out[r]["depth"].astype(np.float64).sum()) for r in range(2))
+    assert abs(vol - float(want.astype(np.float64).sum())) <= 1e-4 * float(want.astype(np.float64).sum())
