@@ -24,6 +24,8 @@ from .solver import Solver2D, _cached_graph, _ptr, _stream
 
 BRICK_W, BRICK_PITCH = L.BRICK_W, L.BRICK_PITCH
 SLOT_STORED, SLOT_ACTIVE = 1, 2
+# The order of a split cache's halo faces (CompressedHalo, compressed_solver.py:1127-1132)
+HALO_FACE_ORDER = ("y-", "y+", "x-", "x+")
 
 
 GswFlatArgs = L.GswFlatArgs
@@ -237,21 +239,36 @@ class CompressedSolver:
     @classmethod
     def from_cache(cls, cache_dir, *, cfl: float = 0.5, h_min: float = 1e-6, g: float = 9.81, dt_max=None,
                    cfl_linf: bool = False, brick_h: Optional[int] = None, track_max_depth: bool = True,
-                   device=None, say=None, arith: str = "exact"):
+                   device=None, say=None, arith: str = "exact", comm=None, dims=None):
         """Load a flat-mesh cache in the reference's format (save_cache /
         run_cached, compressed_solver.py:2504-2560, 2616-2780): meta.json plus .npy files
         (nbr int16 deltas, is_active, ij_active, q0..q2, bed_f, mcls_f, m_tab, and the
         ring and rain bundles), straight to the GPU without a dense domain. Physics
         scalars are the cached loop's (CFL, h_min, g as given; quadratic Manning, keep-h,
-        15 m/s velocity cap). Multi-rank caches, porosity (Sigma), sponge and drain bundles
-        are refused with an error."""
+        15 m/s velocity cap). Porosity (Sigma), sponge and drain bundles are refused with
+        an error.
+
+        A cache of a run split over N ranks (one ``r##`` directory per rank, as the
+        reference's save_cache writes under MPI) loads with ``comm`` (a process group of
+        N ranks) and ``dims`` (the split, as for ``Solver2D``): each rank reads its own
+        directory, keeps its stored cells and its active set as cached, and rebuilds the
+        seam exchange, which is checked against the cached halo faces
+        (compressed_solver.py:1127-1161, 2550-2557)."""
         import json
         import os
         t0 = time.perf_counter()
+        rank, size = 0, 1
+        if comm is not None:
+            import torch.distributed as dist
+            rank, size = dist.get_rank(comm), dist.get_world_size(comm)
+        if size > 1:
+            cache_dir = os.path.join(cache_dir, f"r{rank:02d}")
         path = lambda n: os.path.join(cache_dir, n)
         meta = json.load(open(path("meta.json")))
-        if meta.get("mpi") or int(meta.get("nranks", 1)) != 1:
-            raise NotImplementedError("from_cache: multi-rank caches are not supported (one GPU per solver)")
+        split = bool(meta.get("mpi")) or int(meta.get("nranks", 1)) != 1
+        if split != (size > 1) or int(meta.get("nranks", 1)) != size:
+            raise ValueError(f"from_cache: the cache was written by {int(meta.get('nranks', 1))} rank(s); load it "
+                             f"with comm= of as many ranks (got {size})")
         for key, what in (("has_sponge", "sponge"), ("has_drain", "drain")):
             if meta.get(key):
                 raise NotImplementedError(f"from_cache: the cache holds a {what} bundle, which this solver "
@@ -276,7 +293,21 @@ class CompressedSolver:
         inside = np.zeros((nxp, nyp), np.uint8)
         act = is_active != 0
         inside[ij[act, 0], ij[act, 1]] = 1
-        self._build_layout(torch.from_numpy(inside).to(dev))
+        halo = None
+        if split:
+            # the stored set is the cached one (own inside cells and the neighbours' in the
+            # seam ghost rows, dilated); only the cached active cells are updated here
+            from .halo import Halo2D
+            halo = Halo2D(comm, nxp, nyp, ngh, dtype="float32", dims=dims)
+            stored_mask = np.zeros((nxp, nyp), bool)
+            stored_mask[ij[:, 0], ij[:, 1]] = True
+            self._build_layout(torch.from_numpy(inside).to(dev), seams=[f for f in ("x-", "x+", "y-", "y+")
+                                                                        if halo.has_neighbor(f)],
+                               stored=torch.from_numpy(stored_mask).to(dev))
+            self._tables_cache = dict(ij=ij.astype(np.int32), nbr=nbr, is_active=is_active, N=N,
+                                      fully_covered=None)
+        else:
+            self._build_layout(torch.from_numpy(inside).to(dev))
         stored = self._stored.cpu().numpy()
         canon_ij = np.argwhere(stored)
         if self.N_stored != N or not np.array_equal(canon_ij, ij):
@@ -318,6 +349,25 @@ class CompressedSolver:
                               t=torch.from_numpy(ld("ring_t_common").astype(np.float64).reshape(-1)).to(dev),
                               stage=torch.from_numpy(np.ascontiguousarray(
                                   ld("ring_stage_all").astype(np.float32).reshape(NG, -1))).to(dev))
+        if split:
+            from .halo import FlatHalo
+            slot_pad = torch.full((nxp * nyp,), -1, dtype=torch.int64, device=dev)
+            slot_pad[self._lin_of_slot] = self._slot_cells
+            self.halo = halo
+            self.flat_halo = FlatHalo(halo, slot_pad.reshape(nxp, nyp), nslots=self.nslots)
+            faces = [s for s in HALO_FACE_ORDER if halo.has_neighbor(s)]
+            cached = meta.get("halo_faces", [])
+            if len(cached) != len(faces):
+                raise RuntimeError(f"cache {cache_dir}: {len(cached)} halo faces cached, this split has {len(faces)}")
+            for fi, (side, fm) in enumerate(zip(faces, cached)):
+                n_send = np.load(path(f"halo_f{fi}_sfi.npy")).size
+                n_recv = np.load(path(f"halo_f{fi}_rfi.npy")).size
+                if (int(fm["nbr"]) != halo._neighbor(side) or n_send != self.flat_halo.send_cells(side)
+                        or n_recv != int(self.flat_halo.faces[side]["rslot"].numel())):
+                    raise RuntimeError(f"cache {cache_dir}: halo face {side} differs from this split's (neighbour "
+                                       f"{fm['nbr']} vs {halo._neighbor(side)}, {n_send} vs "
+                                       f"{self.flat_halo.send_cells(side)} cells sent); load with the dims it "
+                                       f"was written with")
         self.build_seconds = time.perf_counter() - t0
         if say:
             say(f"[compressed] loaded {cache_dir}: N_active={self.N_active} N_stored={self.N_stored} "
@@ -342,7 +392,7 @@ class CompressedSolver:
         self.dt_max_user = dt_max
         self._dense_had_rain = False
 
-    def _build_layout(self, inside, active=None, seams=()):
+    def _build_layout(self, inside, active=None, seams=(), stored=None):
         """Stored set (the inside mask dilated twice with the 4-neighbour cross,
         compressed_rhs.py:256), Hilbert bricks, the canonical id -> slot map and the slot
         flags. `inside` is a device uint8 (nxp, nyp) mask; `active` (default `inside`)
@@ -352,19 +402,23 @@ class CompressedSolver:
         refreshes: the bricks that read a cell of those strips are moved to the end of
         the brick order (Hilbert order kept within each part), and `n_bricks_inner`
         counts the others, which the step updates while the seam exchange is in flight.
+        `stored` (a device bool (nxp, nyp) mask) gives the stored set directly (a cache
+        of a split run), instead of the dilation of `inside`.
         Returns (slots, padded linear index, i, j) of every stored cell."""
         dev = self.device
         self._inside = inside
         if active is None:
             active = inside
         st = inside.bool()
-        for _ in range(2):
+        for _ in range(2 if stored is None else 0):
             d = st.clone()
             d[1:, :] |= st[:-1, :]
             d[:-1, :] |= st[1:, :]
             d[:, 1:] |= st[:, :-1]
             d[:, :-1] |= st[:, 1:]
             st = d
+        if stored is not None:
+            st = stored.bool()
         self._stored = st
         self.N_stored = int(st.sum())
         self.N_active = int(active.sum())
@@ -751,8 +805,12 @@ class CompressedSolver:
         """The reference's CompressedSWE tables of this mesh (host, bit-exact), built on
         first use: ij_active (N, 2), nbr (N, 4) int16 deltas, is_active (N)."""
         if self._tables_cache is None:
-            self._tables_cache = build_tables(self._inside.cpu().numpy(), ring=2)
-            assert self._tables_cache["N"] == self.N_stored
+            t = build_tables(self._inside.cpu().numpy(), ring=2)
+            assert t["N"] == self.N_stored
+            # the cells this solver updates: on a split run its own inside cells, not the
+            # neighbours' inside cells stored in its seam ghost rows
+            t["is_active"] = ((self._flags[self._slot] & SLOT_ACTIVE) != 0).cpu().numpy().astype(np.uint8)
+            self._tables_cache = t
         return self._tables_cache
 
     @property
@@ -1054,6 +1112,23 @@ class CompressedSolver:
         if nranks > 1:
             self._barrier()
 
+    def _placement(self):
+        """This block's place in the global grid, from every rank's block extents (one
+        all-gather): ({i0, j0, nx_loc, ny_loc}, (nx_glob, ny_glob))."""
+        import torch.distributed as dist
+        h = self.halo
+        dev = h.device if h.device_direct else torch.device("cpu")
+        mine = torch.tensor([h.coords[0], h.coords[1], self.nx, self.ny], dtype=torch.int64, device=dev)
+        every = [torch.zeros_like(mine) for _ in range(h.size)]
+        dist.all_gather(every, mine, group=h.group)
+        blocks = [tuple(int(v) for v in t.cpu()) for t in every]
+        cx, cy = h.coords
+        i0 = sum(b[2] for b in blocks if b[1] == cy and b[0] < cx)
+        j0 = sum(b[3] for b in blocks if b[0] == cx and b[1] < cy)
+        nxg = sum(b[2] for b in blocks if b[1] == cy)
+        nyg = sum(b[3] for b in blocks if b[0] == cx)
+        return dict(i0=int(i0), j0=int(j0), nx_loc=int(self.nx), ny_loc=int(self.ny)), (int(nxg), int(nyg))
+
     def _rank_and_size(self):
         if self.flat_halo is None:
             return 0, 1
@@ -1108,11 +1183,26 @@ class CompressedSolver:
         """Write the mesh, state, Manning table and the rain / ring bundles in the
         reference's cache format (save_cache, compressed_solver.py:2504-2560), which its
         run_cached and from_cache here both read. Inlets are not part of the format (the
-        reference passes them to run_cached)."""
-        if self.flat_halo is not None:
-            raise NotImplementedError("save_cache: caches of a run split over ranks are not supported")
+        reference passes them to run_cached).
+
+        A run split over ranks writes one ``r##`` directory per rank (every rank calls
+        this), as the reference does under MPI (compressed_solver.py:3342-3356,
+        2550-2557): its own cells (`is_active` marks the cells this rank updates), the
+        block's placement in the global grid, and each seam face's neighbour, width and
+        send / receive cells (canonical ids, row offset, position along the face), in the
+        reference's face order."""
         import json
         import os
+        split = self.flat_halo is not None
+        placement = None
+        if split:
+            rank, nranks = self._rank_and_size()
+            placement, glob = self._placement()
+            cache_dir = os.path.join(cache_dir, f"r{rank:02d}")
+            if nx_glob is None:
+                nx_glob = glob[0]
+            if ny_glob is None:
+                ny_glob = glob[1]
         os.makedirs(cache_dir, exist_ok=True)
         sv = lambda n, a: np.save(os.path.join(cache_dir, n + ".npy"), np.asarray(a))
         tab = self._canonical()
@@ -1129,8 +1219,21 @@ class CompressedSolver:
         meta = dict(nxp=self.nxp, nyp=self.nyp, ngh=self.ngh, dx=self.dx, x0=float(x0), y0=float(y0),
                     crs_wkt=str(crs_wkt), nx_glob=int(nx_glob if nx_glob is not None else self.nx),
                     ny_glob=int(ny_glob if ny_glob is not None else self.ny), has_ring=self._ring is not None,
-                    has_sponge=False, has_rain=self._rain is not None, no_sigma=True, N=int(N), nranks=1,
-                    mpi=False)
+                    has_sponge=False, has_rain=self._rain is not None, no_sigma=True, N=int(N),
+                    nranks=int(self._rank_and_size()[1]), mpi=split)
+        if split:
+            meta["placement"] = placement
+            meta["halo_faces"] = []
+            canon = self._canonical_of_slot()
+            for fi, side in enumerate(s for s in HALO_FACE_ORDER if self.halo.has_neighbor(s)):
+                f = self.flat_halo.faces[side]
+                P = int(f["P"])
+                for k in ("s", "r"):
+                    pos = f[k + "pos"]
+                    sv(f"halo_f{fi}_{k}fi", canon[f[k + "slot"]].cpu().numpy().astype(np.int32))
+                    sv(f"halo_f{fi}_{k}off", (pos // P).cpu().numpy().astype(np.int32))
+                    sv(f"halo_f{fi}_{k}perp", (pos % P).cpu().numpy().astype(np.int32))
+                meta["halo_faces"].append(dict(nbr=int(self.halo._neighbor(side)), P=P))
         if self._rain is not None:
             table = self._rain.cpu().numpy().astype(np.float32)
             if self._rain_kind == L.RAIN_UNIFORM:

@@ -479,6 +479,20 @@ __device__ __forceinline__ unsigned long long lam_flat_bits(float h, float hu, f
     const float l = speed + c;
     return (unsigned long long)__double_as_longlong((double)l);
 }
+// The L2 rule as the bits of the binary32 speed (see lam_dense_bits32): NaN depth gives the
+// quiet NaN 0x7fc00000, which widens to the 0x7ff8000000000000 above, and widening keeps
+// the unsigned order of these bits (positive values, +inf, then NaNs), so the maximum of
+// the 32-bit keys, widened once, is the maximum of lam_flat_bits over the same cells.
+__device__ __forceinline__ uint32_t lam_flat_bits32(float h, float hu, float hv, float g, float h_min,
+                                                    float h_min_cfl) {
+    if (h != h) return 0x7fc00000u;
+    if (h < h_min) return 0u;
+    const float hs = h > h_min_cfl ? h : h_min_cfl;
+    const float c = gsqrt(g * (h > 0.0f ? h : 0.0f));
+    const float u = div_znz(hu, hs), v = div_znz(hv, hs);
+    const float speed = sqrt_z(u * u + v * v);
+    return __float_as_uint(speed + c);
+}
 // The same rule in double (the flat tier is fp32 in the reference; fp64 runs exist for
 // the adjoint's finite-difference and autograd checks).
 __device__ __forceinline__ unsigned long long lam_flat_bits(double h, double hu, double hv, double g,

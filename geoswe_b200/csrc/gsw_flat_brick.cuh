@@ -121,6 +121,7 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
                                                          int r0, int r1, T dt, T rate, const T* frame) {
     const int lane = threadIdx.x;
     unsigned long long lam_local = 0ull;
+    uint32_t lam32 = 0u;        // the production kernel's binary32 key (lam_flat_bits32)
     BrickView v;
     v.BS = (int64_t)m.bh * GSW_BRICK_PITCH;
     v.bh = m.bh;
@@ -219,15 +220,20 @@ __device__ __forceinline__ unsigned long long flat_brick(const FlatMesh<T>& m, c
                                        LEAN || ph.quad != 0, LEAN || ph.keep_h != 0, REFPOW);
                     m.o0[o] = h; m.o1[o] = hu; m.o2[o] = hv;
                     if (m.max_h != nullptr && h > (LEAN ? mh_r : m.max_h[o])) m.max_h[o] = h;
-                    const unsigned long long lb = lam_flat_bits(h, hu, hv, ph.g, ph.h_min, ph.h_min_cfl,
-                                                                !LEAN && ph.linf != 0);
-                    lam_local = lb > lam_local ? lb : lam_local;
+                    if constexpr (LEAN && sizeof(T) == 4) {
+                        lam32 = max(lam32, lam_flat_bits32(h, hu, hv, ph.g, ph.h_min, ph.h_min_cfl));
+                    } else {
+                        const unsigned long long lb = lam_flat_bits(h, hu, hv, ph.g, ph.h_min, ph.h_min_cfl,
+                                                                    !LEAN && ph.linf != 0);
+                        lam_local = lb > lam_local ? lb : lam_local;
+                    }
                 }
             }
         }
         cur = nx;
         b_next = b_p2;
     }
+    if constexpr (LEAN && sizeof(T) == 4) lam_local = lam_bits_of32(lam32);
     return lam_local;
 }
 

@@ -378,3 +378,75 @@ def test_split_compressed_inlet_across_the_seam():
         assert np.abs(d).max() <= 1e-2 and np.sqrt(np.mean(d * d)) <= 1e-3, (r, np.abs(d).max())
     vol = sum(float(out[r]["depth"].astype(np.float64).sum()) for r in range(2))
     assert abs(vol - float(want.astype(np.float64).sum())) <= 1e-4 * float(want.astype(np.float64).sum())
+
+
+def _plain_compressed(z, mask, cls_pad, table, block, **kw):
+    from geoswe_b200 import Config, Mesh2D, RainfallForcing, Solver2D
+    from geoswe_b200.compressed import CompressedSolver
+    x0, x1, y0, y1 = block
+    s = Solver2D(Mesh2D(nx=x1 - x0, ny=y1 - y0, dx=CDX, dy=CDX, ngh=2),
+                 Config(bc_x="fall", bc_y="fall", friction="manning"),
+                 np.zeros((3, x1 - x0, y1 - y0), np.float32), z[x0:x1, y0:y1].copy(), **kw)
+    s.set_inside_mask(mask[x0:x1, y0:y1])
+    s.set_manning_table(cls_pad[x0:x1 + 4, y0:y1 + 4].copy(), table)
+    cs = CompressedSolver.from_dense(s)
+    cs.set_rain(RainfallForcing(time_s=[0.0, 300.0, 1e9], rate_mm_h=[60.0, 25.0, 25.0]))
+    return cs
+
+
+def _split_cache_rank(rank, world, port, out, dims, cdir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        torch.cuda.set_device(0)
+        from geoswe_b200.compressed import CompressedSolver
+        from geoswe_b200.partition import block_of
+        z, mask, cls_pad, table = _compressed_inputs()
+        block = block_of(CNX, CNY, dims, (rank // dims[1], rank % dims[1]))
+        cs = _plain_compressed(z, mask, cls_pad, table, block, comm=dist.group.WORLD, dims=dims)
+        cs.run(t_end=300.0)
+        cs.save_cache(cdir)
+        dist.barrier()
+        ld = CompressedSolver.from_cache(cdir, comm=dist.group.WORLD, dims=dims)
+        steps = ld.run(t_end=C_T_END)
+        out[rank] = dict(block=block, steps=steps, t=ld.t, depth=ld.depth(), inner=ld.n_bricks_inner,
+                         nb=ld.n_bricks, n_active=ld.n_active)
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_split_cache_saves_per_rank_and_reloads(tmp_path):
+    """A split compressed run saves one cache directory per rank (the reference's r##
+    layout: own cells active, placement, seam faces) and fresh solvers load it on the
+    same ranks and continue: equal bit for bit to the single-domain run saved and
+    reloaded at the same time."""
+    import json
+    from geoswe_b200.compressed import CompressedSolver
+    z, mask, cls_pad, table = _compressed_inputs()
+    one = _plain_compressed(z, mask, cls_pad, table, (0, CNX, 0, CNY))
+    one.run(t_end=300.0)
+    one.save_cache(tmp_path / "one")
+    ref = CompressedSolver.from_cache(tmp_path / "one")
+    ref_steps = ref.run(t_end=C_T_END)
+    want = ref.depth()
+    torch.cuda.synchronize()
+    dims = [2, 1]
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_split_cache_rank, args=(2, _free_port(), out, dims, str(tmp_path / "split")),
+                           nprocs=2, start_method="spawn", join=True)
+        out = dict(out)
+    for r in range(2):
+        meta = json.load(open(tmp_path / "split" / f"r{r:02d}" / "meta.json"))
+        assert meta["mpi"] and meta["nranks"] == 2 and len(meta["halo_faces"]) == 1
+        assert meta["placement"]["i0"] == out[r]["block"][0] and meta["nx_glob"] == CNX
+        assert (tmp_path / "split" / f"r{r:02d}" / "halo_f0_sfi.npy").exists()
+    assert ref_steps > 20 and sum(out[r]["n_active"] for r in range(2)) == ref.n_active
+    for r in range(2):
+        o = out[r]
+        x0, x1, y0, y1 = o["block"]
+        assert 0 < o["inner"] < o["nb"]
+        assert o["steps"] == ref_steps and o["t"] == ref.t, (r, o["steps"], ref_steps)
+        np.testing.assert_array_equal(o["depth"], want[x0:x1, y0:y1])
