@@ -301,8 +301,8 @@ class CompressedSolver:
             halo = Halo2D(comm, nxp, nyp, ngh, dtype="float32", dims=dims)
             stored_mask = np.zeros((nxp, nyp), bool)
             stored_mask[ij[:, 0], ij[:, 1]] = True
-            self._build_layout(torch.from_numpy(inside).to(dev), seams=[f for f in ("x-", "x+", "y-", "y+")
-                                                                        if halo.has_neighbor(f)],
+            seams = [f for f in HALO_FACE_ORDER if halo.has_neighbor(f)]
+            self._build_layout(torch.from_numpy(inside).to(dev), seams=seams,
                                stored=torch.from_numpy(stored_mask).to(dev))
             self._tables_cache = dict(ij=ij.astype(np.int32), nbr=nbr, is_active=is_active, N=N,
                                       fully_covered=None)
@@ -1041,8 +1041,8 @@ class CompressedSolver:
             # one step outside the window, so every captured window starts on buffer 0
             one_step(1)
             self.kernel_launches += per_step
-        key = (K, self._rain_kind, len(self._inflows), self._ring is not None, self.warps, self.min_blocks, self.segments,
-               tuple(sorted(self._forcing)))
+        key = (K, self._rain_kind, len(self._inflows), self._ring is not None, self.warps, self.min_blocks,
+               self.segments, tuple(sorted(self._forcing)))
         if split:                               # the step sequence holds collectives: eager
             g, per = None, 0
         else:
