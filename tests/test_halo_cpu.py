@@ -266,6 +266,29 @@ def test_inlet_dry_seed_reductions_over_ranks():
     assert out[0][2][3] == 0.0                     # the flat inlet: no seed depth anywhere
 
 
+def _placement_rank(rank, world, port, out, dims, nx, ny):
+    _init(rank, world, port)
+    try:
+        from geoswe_b200.compressed import CompressedSolver
+        x0, x1, y0, y1 = block_of(nx, ny, dims, (rank // dims[1], rank % dims[1]))
+        cs = CompressedSolver()
+        cs.halo = Halo2D(None, x1 - x0 + 4, y1 - y0 + 4, 2, dtype="float32", dims=dims)
+        cs.nx, cs.ny = x1 - x0, y1 - y0
+        out[rank] = (cs._placement(), (x0, y0))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_split_cache_placement():
+    """A split cache records each block's place in the global grid (the reference's
+    `placement` and global extents), gathered from every rank's block extents: uneven
+    blocks of a 2 x 2 split land at the offsets `partition.block_of` gave them."""
+    out = _spawn(_placement_rank, 4, [2, 2], 37, 53)
+    for r in range(4):
+        (pl, glob), (x0, y0) = out[r]
+        assert (pl["i0"], pl["j0"]) == (x0, y0) and glob == (37, 53), (r, pl, glob)
+
+
 # ------------------------------------------------------------------ split oracle run
 NSTEPS = 25
 
