@@ -243,3 +243,24 @@ def test_library_slot_map_equals_the_solvers():
     assert lib.gsw_bricks_slot_of(ij.ctypes.data, len(ij), bij.ctypes.data, len(bij), cs.brick_h, cs.nxp, cs.nyp,
                                   slot.ctypes.data) == 0
     assert np.array_equal(slot, cs._slot.cpu().numpy())
+
+
+@pytest.mark.parametrize("where", ["depth", "bed"])
+def test_nonfinite_state_raises(where):
+    """A NaN depth (caught by the initial wave speed) or a NaN bed (the step makes the
+    NaN, the step's own wave-speed key carries it) stops the flat loop with
+    FloatingPointError, as the reference's dt_from_lam does."""
+    from geoswe_b200 import RainfallForcing
+    from geoswe_b200.compressed import CompressedSolver
+    q0, bed = flowing(40, 50, seed=4, dtype=np.float32)
+    s = _dense(q0, bed, _blob_mask(40, 50), friction="manning", manning_n=0.03)
+    cs = CompressedSolver.from_dense(s)
+    cs.set_rain(RainfallForcing(time_s=[0.0, 1e9], rate_mm_h=[20.0, 20.0]))
+    k = int(np.nonzero(cs.is_active)[0][len(np.nonzero(cs.is_active)[0]) // 2])
+    slot = int(cs.slot_of[k])
+    if where == "depth":
+        cs._q[cs._cur][0][slot] = float("nan")
+    else:
+        cs._b[slot] = float("nan")
+    with pytest.raises(FloatingPointError):
+        cs.run(t_end=60.0)
