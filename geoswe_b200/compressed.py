@@ -20,7 +20,7 @@ import numpy as np
 import torch
 
 from . import _lib as L
-from .solver import Solver2D, _cached_graph, _ptr, _stream
+from .solver import Solver2D, _cached_graph, _loop_finished, _ptr, _stream
 
 BRICK_W, BRICK_PITCH = L.BRICK_W, L.BRICK_PITCH
 SLOT_STORED, SLOT_ACTIVE = 1, 2
@@ -1055,7 +1055,7 @@ class CompressedSolver:
                 g.replay()
             self.kernel_launches += per
             st = self._read_state()
-            if st.done:
+            if st.done or _loop_finished(st, p):
                 break
             if every > 0.0:
                 executed = int(st.steps) + int(st.pending)

@@ -57,6 +57,16 @@ def _to_device(x, device, dtype):
     return x.to(device, non_blocking=pinned).to(dtype)
 
 
+def _loop_finished(st, p) -> bool:
+    """True when the next evaluation of the dt rule (dt_finalize_one) would only commit the
+    last step and stop the loop: the time has reached t_end - eps_end or the step count
+    max_steps. The host then ends the loop itself (the caller commits the pending step)
+    instead of launching one more window whose steps all find the loop done."""
+    t_now = float(st.t_new) if st.pending else float(st.t)
+    executed = int(st.steps) + int(st.pending)
+    return not (t_now < p.t_end - p.eps_end) or (p.max_steps > 0 and executed >= p.max_steps)
+
+
 def _cached_graph(cache, key, capture, device, keep=4):
     """The CUDA graph of `capture()` for `key`, captured on first use on a side stream
     (the captured kernels read the loop's `done` flag first, so a replay after the loop
@@ -863,7 +873,7 @@ class Solver2D:
         while True:
             self.kernel_launches += run_window()
             st = self._read_state()
-            if st.done:
+            if st.done or _loop_finished(st, p):
                 break
         L.call("gsw_loop_commit", _ptr(self._state), _stream())
         self.kernel_launches += 1
